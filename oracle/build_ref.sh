@@ -1,0 +1,92 @@
+#!/bin/bash
+# build_ref.sh -- TEST INFRASTRUCTURE ONLY.
+#
+# Compiles the CPS reference (RBC-UKQCD/CPS_public, cps_pp v5.3.1) noarch
+# sources directly with g++ -- without running CPS's configure/make -- and
+# links them with oracle/ref_harness.C into oracle/_ref/cpsref, the executable
+# that runs the reference's own Dslash / MatPcDagMatPc / InvCg / MInvCG.
+#
+# Usage: oracle/build_ref.sh [path-to-cps_pp]   (default /root/reference/cps_pp)
+# Output goes only to oracle/_ref/ (git-ignored).  Nothing is written into the
+# reference tree and no reference source is copied into this repository.
+#
+# Build notes (both are upstream defects, worked around without editing sources):
+#  * d_op_wilson/noarch/wilson_dslash.C lacks the closing brace of
+#    wilson_dslash() after line 515; it is compiled through a one-line wrapper
+#    translation unit that includes it and supplies the missing brace at the end.
+#  * The 4-argument DiracOp::InvCg (d_op_base/comsrc/inv_cg.C:449-454) falls off
+#    the end without returning; the harness calls InvCgShift directly.
+set -euo pipefail
+REF=${1:-/root/reference/cps_pp}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT=$HERE/_ref
+OBJ=$OUT/obj
+if [ ! -d "$REF/src" ]; then
+  echo "build_ref.sh: reference tree $REF not found" >&2
+  exit 3
+fi
+mkdir -p "$OBJ"
+CXXFLAGS="-O2 -fopenmp -DUSE_OMP -w -std=gnu++11"
+INC="-I$HERE/ref_config -I$REF/include"
+
+# Every noarch/comsrc source; other-architecture ports and external-library
+# bridges are excluded (they need headers that are not on this machine).
+find "$REF/src" \( -name '*.C' -o -name '*.c' \) \
+  | grep -v -E '/(bgl|bgp|bgq|qcdoc|qcdsp|qmp|mpi|sse|bfm|bg_bagel|bg_bagel_spi|noarch_pv|quda|grid|cuda|bgl_qmp)/' \
+  | grep -v -E '/d_op_wilson/noarch/wilson_dslash\.C$' \
+  | sort > "$OUT/sources.txt"
+# gjp has no noarch directory: its qmp/start_end.C holds the non-QMP Start()/End().
+echo "$REF/src/util/gjp/qmp/start_end.C" >> "$OUT/sources.txt"
+
+compile_one() {
+  local f=$1
+  local rel=${f#$REF/src/}
+  local o=$OBJ/$(echo "$rel" | tr '/' '_').o
+  if [ -f "$o" ] && [ "$o" -nt "$f" ]; then return 0; fi
+  if [[ $f == *.c ]]; then
+    gcc -x c -O2 -fopenmp -DUSE_OMP -w $INC -c "$f" -o "$o" 2> "$o.log" || { rm -f "$o"; echo "skip $rel" >> "$OUT/skipped.txt"; return 0; }
+  else
+    g++ -x c++ $CXXFLAGS $INC -c "$f" -o "$o" 2> "$o.log" || { rm -f "$o"; echo "skip $rel" >> "$OUT/skipped.txt"; return 0; }
+  fi
+  rm -f "$o.log"
+}
+export -f compile_one
+export REF OBJ OUT CXXFLAGS INC
+rm -f "$OUT/skipped.txt"
+xargs -P "$(nproc)" -I{} bash -c 'compile_one "$@"' _ {} < "$OUT/sources.txt"
+
+# wilson_dslash.C through the brace-supplying wrapper.
+WRAP=$OUT/wilson_dslash_wrap.C
+printf '#include "%s"\n}\n' "$REF/src/util/dirac_op/d_op_wilson/noarch/wilson_dslash.C" > "$WRAP"
+g++ $CXXFLAGS $INC -c "$WRAP" -o "$OBJ/wilson_dslash_wrap.o"
+
+rm -f "$OUT/libcps.a"
+ar rcs "$OUT/libcps.a" "$OBJ"/*.o
+
+# Symbols referenced from objects that did not compile here (MPI / FFTW users)
+# or that CPS declares but never defines for noarch; none is reached by the
+# fermion-matrix path.
+cat > "$OUT/stubs.C" <<'EOF'
+#include <config.h>
+#include <util/dirac_op.h>
+#include <util/error.h>
+CPS_START_NAMESPACE
+int DiracOp::InvLowModeApprox(std::vector<Vector *> &, std::vector<Vector *> &, char *, int) {
+  ERR.General("stub", "InvLowModeApprox", "not available in the oracle build");
+  return 0;
+}
+void DiracOpMobiusEOFA::Mat(Vector *, Vector *) {
+  ERR.General("stub", "DiracOpMobiusEOFA::Mat", "not available in the oracle build");
+}
+void DiracOpMobiusEOFA::MatHerm(Vector *, Vector *) {
+  ERR.General("stub", "DiracOpMobiusEOFA::MatHerm", "not available in the oracle build");
+}
+CPS_END_NAMESPACE
+EOF
+g++ $CXXFLAGS $INC -c "$OUT/stubs.C" -o "$OUT/stubs.o" || true
+
+STUBOBJ=""
+[ -f "$OUT/stubs.o" ] && STUBOBJ="$OUT/stubs.o"
+g++ $CXXFLAGS $INC "$HERE/ref_harness.C" $STUBOBJ "$OUT/libcps.a" -o "$OUT/cpsref" -lm -fopenmp \
+  2> "$OUT/link.log" || { cat "$OUT/link.log" >&2; exit 1; }
+echo "built $OUT/cpsref"
