@@ -1,0 +1,108 @@
+"""Generates the golden fixtures in tests/golden/ by running the compiled CPS
+reference (oracle/_ref/cpsref, built by oracle/build_ref.sh from the reference
+sources).  Run from the repository root:  python tests/golden/make_golden.py
+
+Inputs are re-created from seeds by cps_public_b200.fields (a SHA-256 of each
+input is stored so a drifting generator is caught); outputs are stored in full.
+OMP_NUM_THREADS=1 makes the reference's reductions sequential.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from cps_public_b200 import fields  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# (name, action, dims, ls, eps, seed, mass, extra parameters)
+CASES = [
+    ("wilson_4x4x4x4", "wilson", (4, 4, 4, 4), 1, 0.3, 11, 0.1, {}),
+    ("wilson_aprd_4x4x4x4", "wilson", (4, 4, 4, 4), 1, 0.3, 12, 0.1, {"bc_t": 1}),
+    ("dwf_4x4x4x4_ls4", "dwf", (4, 4, 4, 4), 4, 0.2, 21, 0.05, {"m5": 1.8}),
+    ("mobius_4x4x4x4_ls4", "mobius", (4, 4, 4, 4), 4, 0.2, 31, 0.05, {"m5": 1.8, "b": 1.5, "c": 0.5}),
+]
+
+SHIFTS = [0.0, 0.01, 0.1]
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, np.float64).tobytes()).hexdigest()
+
+
+def gen_case(name, action, dims, ls, eps, seed, mass, extra):
+    u = fields.random_gauge(dims, eps, seed)
+    nsites = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(nsites, seed)
+    kw = dict(ls=ls, mass=mass, threads=1, **extra)
+    rec = {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps,
+           "seed": seed, "mass": mass}
+    for k, v in extra.items():
+        rec[k] = v
+    full = action == "wilson"
+    dsl = [(0, 0), (0, 1), (1, 0), (1, 1)] if full else [(1, 0), (0, 1)]
+    for cb, dag in dsl:
+        _, _, r = refrun.run(refrun.OP_DSLASH, action, dims, u, [src], cb=cb, dag=dag, **kw)
+        rec[f"dslash_cb{cb}_dag{dag}"] = r
+    if "bc_t" in extra:
+        return rec
+    for dag in (0, 1):
+        _, _, r = refrun.run(refrun.OP_MATPC, action, dims, u, [src], dag=dag, **kw)
+        rec[f"matpc_dag{dag}"] = r
+    _, rp, r = refrun.run(refrun.OP_MDAGM, action, dims, u, [src], **kw)
+    rec["mdagm"] = r
+    rec["mdagm_dot"] = rp[0]
+    it, rp, r = refrun.run(refrun.OP_INVCG, action, dims, u, [src, np.zeros_like(src)],
+                           stop_rsd=1e-10, max_iter=5000, **kw)
+    rec["cg_sol"] = r
+    rec["cg_iters"] = it
+    rec["cg_true_res"] = rp[0]
+    ns = len(SHIFTS) if full else 2
+    it, rp, r = refrun.run(refrun.OP_MINVCG, action, dims, u, [src], shifts=SHIFTS[:ns],
+                           extra=[np.full(ns, 1e-9), np.ones(ns)], max_iter=5000, **kw)
+    rec["minvcg_shifts"] = np.array(SHIFTS[:ns])
+    rec["minvcg_sol"] = r.reshape(ns, -1)
+    rec["minvcg_iters"] = it
+    rec["minvcg_rsd"] = rp[:ns].copy()
+    if action == "mobius":
+        for dag in (0, 1):
+            _, _, r = refrun.run(refrun.OP_M5INV, action, dims, u, [src], dag=dag, **kw)
+            rec[f"m5inv_dag{dag}"] = r
+        for cb, dag in [(1, 0), (0, 1)]:
+            _, _, r = refrun.run(refrun.OP_MOBIUS_D4, action, dims, u, [src], cb=cb, dag=dag, **kw)
+            rec[f"d4_cb{cb}_dag{dag}"] = r
+    return rec
+
+
+def gen_baseline_config0():
+    """The reference's own CPU-runnable benchmark case: Wilson 8^4, eps 0.3,
+    mass 0.1, Gaussian source on the odd checkerboard, stop_rsd 1e-10."""
+    dims = (8, 8, 8, 8)
+    u = fields.random_gauge(dims, 0.3, 100)
+    src = fields.random_source(int(np.prod(dims)) // 2, 100)
+    it, rp, r = refrun.run(refrun.OP_INVCG, "wilson", dims, u, [src, np.zeros_like(src)],
+                           mass=0.1, stop_rsd=1e-10, max_iter=5000, threads=1)
+    return {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "eps": 0.3,
+            "seed": 100, "mass": 0.1, "cg_sol": r, "cg_iters": it, "cg_true_res": rp[0]}
+
+
+def main():
+    if not refrun.available():
+        sys.exit("oracle/_ref/cpsref missing: run oracle/build_ref.sh first")
+    for case in CASES:
+        rec = gen_case(*case)
+        np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **rec)
+        print("wrote", case[0])
+    np.savez_compressed(os.path.join(OUT, "wilson_8x8x8x8_cg.npz"), **gen_baseline_config0())
+    print("wrote wilson_8x8x8x8_cg")
+
+
+if __name__ == "__main__":
+    main()

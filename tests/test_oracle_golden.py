@@ -1,0 +1,81 @@
+"""Pins the C oracle (oracle/cps_oracle.c) against golden vectors produced by
+the compiled CPS reference (tests/golden/make_golden.py).  Agreement is bit for
+bit: the oracle issues the reference's floating-point operations in order."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.golden_util import load
+
+CASES = ["wilson_4x4x4x4", "dwf_4x4x4x4_ls4", "mobius_4x4x4x4_ls4"]
+
+
+def make_op(rec, u, action):
+    kw = dict(ls=int(rec["ls"]), mass=float(rec["mass"]))
+    for k in ("m5", "b", "c", "bc_t"):
+        if k in rec:
+            kw[k] = float(rec[k]) if k != "bc_t" else int(rec[k])
+    return oracle.Op(action, tuple(rec["dims"]), u, **kw)
+
+
+@pytest.mark.parametrize("name", CASES + ["wilson_aprd_4x4x4x4"])
+def test_dslash_bitexact(name):
+    rec, u, src = load(name)
+    op = make_op(rec, u, name.split("_")[0])
+    keys = [k for k in rec if k.startswith("dslash_")]
+    assert keys
+    for k in keys:
+        cb, dag = int(k[9]), int(k[-1])
+        np.testing.assert_array_equal(op.dslash(src, cb, dag), rec[k], err_msg=k)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_matpc_mdagm_bitexact(name):
+    rec, u, src = load(name)
+    op = make_op(rec, u, name.split("_")[0])
+    for dag in (0, 1):
+        np.testing.assert_array_equal(op.matpc(src, dag), rec[f"matpc_dag{dag}"])
+    out, dot = op.mdagm(src)
+    np.testing.assert_array_equal(out, rec["mdagm"])
+    assert dot == float(rec["mdagm_dot"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_invcg_bitexact(name):
+    rec, u, src = load(name)
+    op = make_op(rec, u, name.split("_")[0])
+    sol, it, tr = op.invcg(src, 1e-10, 5000)
+    assert it == int(rec["cg_iters"])
+    assert tr == float(rec["cg_true_res"])
+    np.testing.assert_array_equal(sol, rec["cg_sol"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_minvcg_bitexact(name):
+    rec, u, src = load(name)
+    op = make_op(rec, u, name.split("_")[0])
+    shifts = list(rec["minvcg_shifts"])
+    sols, it, rsd = op.minvcg(src, shifts, [1e-9] * len(shifts))
+    assert it == int(rec["minvcg_iters"])
+    np.testing.assert_array_equal(rsd, rec["minvcg_rsd"])
+    for i in range(len(shifts)):
+        np.testing.assert_array_equal(sols[i], rec["minvcg_sol"][i])
+
+
+def test_mobius_m5inv_d4_bitexact():
+    rec, u, src = load("mobius_4x4x4x4_ls4")
+    op = make_op(rec, u, "mobius")
+    for dag in (0, 1):
+        np.testing.assert_array_equal(op.m5inv(src, dag), rec[f"m5inv_dag{dag}"])
+    for cb, dag in [(1, 0), (0, 1)]:
+        np.testing.assert_array_equal(op.mobius_d4(src, cb, dag), rec[f"d4_cb{cb}_dag{dag}"])
+
+
+def test_wilson_8x8x8x8_cg_config():
+    """The reference's CPU-runnable benchmark case (Wilson 8^4 CG to 1e-10)."""
+    rec, u, src = load("wilson_8x8x8x8_cg")
+    op = oracle.Op("wilson", (8, 8, 8, 8), u, mass=0.1)
+    sol, it, tr = op.invcg(src, 1e-10, 5000)
+    assert it == int(rec["cg_iters"])
+    assert tr == float(rec["cg_true_res"]) and tr <= 1e-10
+    np.testing.assert_array_equal(sol, rec["cg_sol"])
