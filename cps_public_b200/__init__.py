@@ -1,0 +1,175 @@
+"""cps_public_b200 -- B200-native CPS fermion-matrix hot path.
+
+Python front end of libcpsb200.so, mirroring the CPS interfaces it replaces:
+
+* ``Gauge``        resident gauge field (the gauge half of the DiracOp constructor)
+* ``DiracOp``      Dslash / MatPc / MatPcDag / MatPcDagMatPc / InvCg / MInvCG for the
+                   Wilson, DWF and Mobius actions (cps_pp/include/util/dirac_op.h)
+* ``fmat_evl_inv`` / ``fmat_evl_minv``  the Lattice::FmatEvlInv / FmatEvlMInv entry
+                   points (cps_pp/include/util/lattice.h:942,976)
+
+All compute runs in the CUDA library; this module only marshals numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DWF, F16, F32, F64, MOBIUS, MULTI, ORDER_CANONICAL, ORDER_WILSON, SINGLE,  # noqa: F401
+                   WILSON, CgArg, CpsbError, DiracParams, SolveResult, check, ptr)
+
+_initialised = None
+
+
+def init(device: int = 0) -> None:
+    global _initialised
+    lib = _lib.load()
+    check(lib.cpsb_init(device), "cpsb_init")
+    _initialised = device
+
+
+def mem_info():
+    lib = _lib.load()
+    f, t = C.c_ulonglong(), C.c_ulonglong()
+    check(lib.cpsb_mem_info(C.byref(f), C.byref(t)), "cpsb_mem_info")
+    return f.value, t.value
+
+
+class Gauge:
+    """A gauge field resident on the device (CANONICAL or WILSON order input)."""
+
+    def __init__(self, u: np.ndarray, dims, order: int = ORDER_CANONICAL, bc_t: int = 0):
+        if _initialised is None:
+            init(0)
+        lib = _lib.load()
+        self.dims = tuple(int(d) for d in dims)
+        u = np.ascontiguousarray(u, np.float64)
+        vol = int(np.prod(self.dims))
+        if u.size != vol * 72:
+            raise ValueError(f"gauge field has {u.size} reals, expected {vol * 72}")
+        h = C.c_void_p()
+        d = (C.c_int * 4)(*self.dims)
+        check(lib.cpsb_gauge_load(C.byref(h), ptr(u), d, order, bc_t), "cpsb_gauge_load")
+        self.h = h
+        self.n4cb = vol // 2
+
+    def free(self):
+        if self.h:
+            _lib.load().cpsb_gauge_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+ACTION_NAMES = {"wilson": WILSON, "dwf": DWF, "mobius": MOBIUS}
+
+
+class DiracOp:
+    """Device fermion operator with the CPS DiracOp interface.
+
+    ``DiracOp(gauge, 'dwf', mass=0.01, ls=16, m5=1.8)``; vectors are float64 numpy
+    arrays in CPS checkerboard order (sites x 24).
+    """
+
+    def __init__(self, gauge: Gauge, action="wilson", mass=0.1, ls=1, m5=1.8, a5_inv=1.0, b=1.5, c=0.5,
+                 pc_type=2):
+        self.gauge = gauge
+        self.p = DiracParams()
+        self.p.action = ACTION_NAMES[action] if isinstance(action, str) else int(action)
+        self.p.ls = 1 if self.p.action == WILSON else int(ls)
+        self.p.mass = mass
+        self.p.m5 = m5
+        self.p.a5_inv = a5_inv
+        self.p.mobius_b = b
+        self.p.mobius_c = c
+        self.p.pc_type = pc_type
+        self.n = gauge.n4cb * self.p.ls * 24
+
+    def _v(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        if x.size != self.n:
+            raise ValueError(f"vector has {x.size} reals, expected {self.n}")
+        return x
+
+    def Dslash(self, x, cb, dag):
+        out = np.empty(self.n)
+        check(_lib.load().cpsb_dslash(self.gauge.h, C.byref(self.p), ptr(out), ptr(self._v(x)), cb, dag),
+              "cpsb_dslash")
+        return out
+
+    def MatPc(self, x):
+        out = np.empty(self.n)
+        check(_lib.load().cpsb_matpc(self.gauge.h, C.byref(self.p), ptr(out), ptr(self._v(x)), 0), "cpsb_matpc")
+        return out
+
+    def MatPcDag(self, x):
+        out = np.empty(self.n)
+        check(_lib.load().cpsb_matpc(self.gauge.h, C.byref(self.p), ptr(out), ptr(self._v(x)), 1), "cpsb_matpc")
+        return out
+
+    def MatPcDagMatPc(self, x):
+        """Returns (M^dag M x, |M x|^2)."""
+        out = np.empty(self.n)
+        dot = C.c_double()
+        check(_lib.load().cpsb_mdagm(self.gauge.h, C.byref(self.p), ptr(out), ptr(self._v(x)), C.byref(dot)),
+              "cpsb_mdagm")
+        return out, dot.value
+
+    def InvCg(self, src, stop_rsd=1e-10, max_num_iter=5000, precision=F64, guess=None, reliable_delta=0.1,
+              batch=0):
+        """Solves M^dag M x = src; returns (x, SolveResult)."""
+        x = np.zeros(self.n) if guess is None else self._v(guess).copy()
+        a = CgArg(stop_rsd, max_num_iter, precision, reliable_delta, batch)
+        r = SolveResult()
+        rc = check(_lib.load().cpsb_invcg(self.gauge.h, C.byref(self.p), C.byref(a), ptr(x),
+                                          ptr(self._v(src)), C.byref(r)), "cpsb_invcg")
+        r.rc = rc
+        return x, r
+
+    def InvCgMulti(self, srcs, stop_rsd=1e-10, max_num_iter=5000, precision=F64, reliable_delta=0.1, batch=0):
+        n = len(srcs)
+        xs = [np.zeros(self.n) for _ in range(n)]
+        bs = [self._v(s) for s in srcs]
+        xp = (_lib._dp * n)(*[ptr(x) for x in xs])
+        bp = (_lib._dp * n)(*[ptr(b) for b in bs])
+        a = CgArg(stop_rsd, max_num_iter, precision, reliable_delta, batch)
+        res = (SolveResult * n)()
+        check(_lib.load().cpsb_invcg_multi(self.gauge.h, C.byref(self.p), C.byref(a), n, xp, bp, res),
+              "cpsb_invcg_multi")
+        return xs, list(res)
+
+    def MInvCG(self, src, shifts, rsd, ms_type=MULTI, alpha=None, max_num_iter=5000, precision=F64):
+        ns = len(shifts)
+        nvec = 1 if ms_type == SINGLE else ns
+        xs = [np.zeros(self.n) for _ in range(nvec)]
+        xp = (_lib._dp * nvec)(*[ptr(x) for x in xs])
+        rs = np.array(rsd, np.float64)
+        sh = np.array(shifts, np.float64)
+        al = np.ones(ns) if alpha is None else np.array(alpha, np.float64)
+        a = CgArg(float(np.min(rs)), max_num_iter, precision, 0.1, 0)
+        r = SolveResult()
+        rc = check(_lib.load().cpsb_minvcg(self.gauge.h, C.byref(self.p), C.byref(a), xp, ptr(self._v(src)),
+                                           ptr(sh), ns, ptr(rs), ms_type, ptr(al), C.byref(r)), "cpsb_minvcg")
+        r.rc = rc
+        return xs, r, rs
+
+
+def fmat_evl_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
+    """Lattice::FmatEvlInv: returns (iterations, f_out, true_res)."""
+    x, r = op.InvCg(f_in, cg_arg.get("stop_rsd", 1e-10), cg_arg.get("max_num_iter", 5000),
+                    cg_arg.get("precision", F64), guess=f_out)
+    return r.iters, x, r.true_rsd
+
+
+def fmat_evl_minv(op: DiracOp, f_in, shifts, cg_args, ms_type=MULTI, alpha=None):
+    """Lattice::FmatEvlMInv: returns (iterations, solutions, per-shift residuals)."""
+    rsd = [a.get("stop_rsd", 1e-10) for a in cg_args]
+    xs, r, rs = op.MInvCG(f_in, shifts, rsd, ms_type, alpha, cg_args[0].get("max_num_iter", 5000),
+                          cg_args[0].get("precision", F64))
+    return r.iters, xs, rs

@@ -1,0 +1,35 @@
+// blas.h -- launchers of the streaming kernels in blas.cu and m5.cu.
+#pragma once
+#include "cg_state.h"
+#include "cpsb_kernels.h"
+
+namespace cpsb {
+
+struct Scal2 {
+  double a[MAX_RHS];
+  double b[MAX_RHS];
+};
+
+cudaError_t launch_unitarity(const double *u, long nlinks, const int dims[4], int bc_t, unsigned long long *out,
+                             cudaStream_t st);
+cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr Ap, CgState *S, Reduce red,
+                               cudaStream_t st);
+cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, SpinorPtr p, SpinorPtr r, CgState *S,
+                                unsigned *ticket, cudaStream_t st);
+cudaError_t launch_axpby(int po, SpinorPtr out, int px, SpinorPtr X, int py, SpinorPtr Y, const Geom &g, Scal2 sc,
+                         const int *skip, Reduce red, int norm, cudaStream_t st);
+cudaError_t launch_redot(int prec, const Geom &g, SpinorPtr X, SpinorPtr Y, Reduce red, cudaStream_t st);
+
+// Mobius 5th-direction kernels (m5.cu).
+struct M5Coef {
+  double K;            // kappa_b/kappa_c (the M5 hopping coefficient ratio)
+  double invd;         // 1/(1 + m_f prod(-K)) (dag 0) or its dag-1 form
+  double f1[64];       // per-step wall factors of the forward sweep
+  double f2[64];       // per-step wall factors of the backward sweep
+  double b, c, mass;   // mixing b + c*H5, walls -m_f
+  double scale;        // output scale
+};
+cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                      int xpay, int norm, Reduce red, const int *skip, cudaStream_t st);
+
+}  // namespace cpsb

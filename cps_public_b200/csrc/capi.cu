@@ -1,0 +1,413 @@
+// capi.cu -- the extern "C" boundary (include/cpsb200.h).  Validates arguments,
+// moves host vectors in CPS order through pinned staging buffers, packs them
+// into the device layout and converts every library error into a status code.
+#include <stdio.h>
+#include <string.h>
+
+#include <chrono>
+
+#include "host.h"
+
+using namespace cpsb;
+
+namespace cpsb {
+void drop_solvers(Gauge *G);
+}
+
+struct cpsb_gauge_s {
+  Gauge g;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const Error &e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return CPSB_ERR_OOM;
+  } catch (...) {
+    g_last_error = "unexpected exception";
+    return CPSB_ERR_CUDA;
+  }
+}
+
+void need_init() {
+  if (ctx().device < 0) throw Error{CPSB_ERR_NO_DEVICE, "cpsb_init has not been called"};
+  CK(cudaSetDevice(ctx().device));
+}
+
+void check_params(cpsb_gauge h, const cpsb_dirac_params *p) {
+  if (!h || !p) throw Error{CPSB_ERR_ARG, "null gauge handle or parameters"};
+  if (p->action < CPSB_WILSON || p->action > CPSB_MOBIUS) throw Error{CPSB_ERR_ARG, "unknown action"};
+  if (p->action != CPSB_WILSON && (p->ls < 2 || p->ls > 64)) throw Error{CPSB_ERR_ARG, "ls must be in [2, 64]"};
+}
+
+long cb_sites(cpsb_gauge h, const cpsb_dirac_params *p) {
+  return h->g.n4cb * (p->action == CPSB_WILSON ? 1 : p->ls);
+}
+
+// Pinned staging buffer reused across calls (grown on demand).
+struct Staging {
+  void *p = nullptr;
+  size_t bytes = 0;
+  std::mutex mu;
+  void *get(size_t n) {
+    if (n > bytes) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      bytes = 0;
+      CK(cudaMallocHost(&p, n));
+      bytes = n;
+    }
+    return p;
+  }
+};
+Staging &staging() {
+  static Staging s;
+  return s;
+}
+
+void h2d_vec(Field &f, const double *host, long nsites, long offset_sites, cudaStream_t st, DevBuf &tmp) {
+  const size_t bytes = (size_t)nsites * 24 * sizeof(double);
+  if (tmp.bytes < bytes) tmp.alloc(bytes);
+  Staging &sg = staging();
+  std::lock_guard<std::mutex> lk(sg.mu);
+  void *pin = sg.get(bytes);
+  memcpy(pin, host, bytes);
+  CK(cudaMemcpyAsync(tmp.p, pin, bytes, cudaMemcpyHostToDevice, st));
+  SpinorPtr dst = f.ptr();
+  if (f.prec == P64) dst.data = (char *)dst.data + 0;  // whole-field packing below uses offsets
+  CK(cudaStreamSynchronize(st));
+  (void)offset_sites;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cpsb_error_string(int code) {
+  switch (code) {
+    case CPSB_OK: return "ok";
+    case CPSB_NOT_CONVERGED: return "not converged within max_num_iter";
+    case CPSB_ERR_ARG: return "invalid argument";
+    case CPSB_ERR_CUDA: return "CUDA error";
+    case CPSB_ERR_OOM: return "out of device memory";
+    case CPSB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case CPSB_ERR_BREAKDOWN: return "solver breakdown (p.Ap = 0)";
+    case CPSB_ERR_NO_DEVICE: return "no CUDA device / cpsb_init not called";
+    case CPSB_ERR_BUSY: return "resource busy";
+  }
+  return "unknown status";
+}
+
+const char *cpsb_last_error(void) { return g_last_error.c_str(); }
+
+int cpsb_init(int device) {
+  return guarded([&] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error{CPSB_ERR_NO_DEVICE, "no CUDA device"};
+    if (device < 0 || device >= n) throw Error{CPSB_ERR_ARG, "device index out of range"};
+    Context &c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.device == device) return CPSB_OK;
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    c.nsm = prop.multiProcessorCount;
+    if (!c.stream) CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.device = device;
+    return CPSB_OK;
+  });
+}
+
+int cpsb_mem_info(unsigned long long *free_b, unsigned long long *total_b) {
+  return guarded([&] {
+    need_init();
+    size_t f = 0, t = 0;
+    CK(cudaMemGetInfo(&f, &t));
+    if (free_b) *free_b = f;
+    if (total_b) *total_b = t;
+    return CPSB_OK;
+  });
+}
+
+int cpsb_gauge_load(cpsb_gauge *out, const double *u, const int dims[4], int order, int bc_t) {
+  return guarded([&] {
+    need_init();
+    if (!out || !u || !dims) throw Error{CPSB_ERR_ARG, "null argument"};
+    for (int i = 0; i < 4; i++)
+      if (dims[i] < 2 || dims[i] % 2) throw Error{CPSB_ERR_ARG, "lattice extents must be even and >= 2"};
+    if (order != CPSB_ORDER_CANONICAL && order != CPSB_ORDER_WILSON) throw Error{CPSB_ERR_ARG, "bad gauge order"};
+    std::unique_ptr<cpsb_gauge_s> h(new cpsb_gauge_s);
+    Gauge &G = h->g;
+    for (int i = 0; i < 4; i++) G.dims[i] = dims[i];
+    G.bc_t = bc_t ? 1 : 0;
+    const long vol = (long)dims[0] * dims[1] * dims[2] * dims[3];
+    G.n4cb = vol / 2;
+    const size_t bytes = (size_t)vol * 72 * sizeof(double);
+    cudaStream_t st = ctx().stream;
+    G.canon.alloc(bytes);
+    std::vector<double> canon;
+    const double *src = u;
+    if (order == CPSB_ORDER_WILSON) {
+      // WILSON -> CANONICAL: even sites first, links transposed (convert_func.C:371-405)
+      canon.resize((size_t)vol * 72);
+      const int lx = dims[0], ly = dims[1], lz = dims[2], lt = dims[3];
+      for (int t = 0; t < lt; t++)
+        for (int z = 0; z < lz; z++)
+          for (int y = 0; y < ly; y++)
+            for (int x = 0; x < lx; x++) {
+              long cs = x + lx * (y + (long)ly * (z + (long)lz * t));
+              long ws = (x - x % 2 + lx * (y + (long)ly * (z + (long)lz * t)) + vol * ((x + y + z + t) % 2)) / 2;
+              for (int mu = 0; mu < 4; mu++)
+                for (int row = 0; row < 3; row++)
+                  for (int col = 0; col < 3; col++)
+                    for (int r = 0; r < 2; r++)
+                      canon[72 * cs + r + 2 * (col + 3 * (row + 3 * mu))] = u[72 * ws + r + 2 * (row + 3 * (col + 3 * mu))];
+            }
+      src = canon.data();
+    }
+    CK(cudaMemcpyAsync(G.canon.p, src, bytes, cudaMemcpyHostToDevice, st));
+    G.u64.alloc((size_t)vol * 4 * 144);
+    CK(launch_gauge_pack(P64, G.u64.p, (const double *)G.canon.p, G.dims, G.bc_t, st));
+    DevBuf flag(8);
+    CK(cudaMemsetAsync(flag.p, 0, 8, st));
+    CK(launch_unitarity((const double *)G.canon.p, vol * 4, G.dims, G.bc_t, (unsigned long long *)flag.p, st));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, flag.p, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double worst;
+    memcpy(&worst, &bits, 8);
+    G.recon_err = worst;
+    G.recon_ok = worst < 1e-6;
+    *out = h.release();
+    return CPSB_OK;
+  });
+}
+
+int cpsb_gauge_free(cpsb_gauge h) {
+  return guarded([&] {
+    if (!h) return CPSB_OK;
+    need_init();
+    CK(cudaStreamSynchronize(ctx().stream));
+    drop_solvers(&h->g);
+    delete h;
+    return CPSB_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Copies nvec host vectors (each nsites*24 doubles, CPS order) into one device
+// CPS-order buffer, packs it into f (precision f.prec).
+void upload(Field &f, const double *const *host, int nvec, long nsites_each, cudaStream_t st) {
+  static DevBuf tmp;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  const size_t each = (size_t)nsites_each * 24 * sizeof(double);
+  if (tmp.bytes < each * nvec) tmp.alloc(each * nvec);
+  Staging &sg = staging();
+  std::lock_guard<std::mutex> lk2(sg.mu);
+  void *pin = sg.get(each * nvec);
+  for (int i = 0; i < nvec; i++) memcpy((char *)pin + i * each, host[i], each);
+  CK(cudaMemcpyAsync(tmp.p, pin, each * nvec, cudaMemcpyHostToDevice, st));
+  CK(launch_pack(f.prec, f.ptr(), (const double *)tmp.p, f.nsites, st));
+  CK(cudaStreamSynchronize(st));
+}
+
+void download(double *const *host, int nvec, long nsites_each, const Field &f, cudaStream_t st) {
+  static DevBuf tmp;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  const size_t each = (size_t)nsites_each * 24 * sizeof(double);
+  if (tmp.bytes < each * nvec) tmp.alloc(each * nvec);
+  CK(launch_unpack(f.prec, (double *)tmp.p, f.ptr(), f.nsites, st));
+  Staging &sg = staging();
+  std::lock_guard<std::mutex> lk2(sg.mu);
+  void *pin = sg.get(each * nvec);
+  CK(cudaMemcpyAsync(pin, tmp.p, each * nvec, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < nvec; i++) memcpy(host[i], (char *)pin + i * each, each);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cpsb_dslash(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, int cb, int dag) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (!out || !in || (cb != 0 && cb != 1) || (dag != 0 && dag != 1)) throw Error{CPSB_ERR_ARG, "bad argument"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    Field fi(P64, op.nsites()), fo(P64, op.nsites());
+    upload(fi, &in, 1, op.nsites(), st);
+    op.dslash(fo, fi, cb, dag, st);
+    download(&out, 1, op.nsites(), fo, st);
+    return CPSB_OK;
+  });
+}
+
+int cpsb_matpc(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, int dag) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (!out || !in || (dag != 0 && dag != 1)) throw Error{CPSB_ERR_ARG, "bad argument"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    Field fi(P64, op.nsites()), fo(P64, op.nsites());
+    upload(fi, &in, 1, op.nsites(), st);
+    op.matpc(fo, fi, dag, nullptr, nullptr, st);
+    download(&out, 1, op.nsites(), fo, st);
+    return CPSB_OK;
+  });
+}
+
+int cpsb_mdagm(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    Field fi(P64, op.nsites()), fo(P64, op.nsites());
+    RedSlot rs;
+    DevBuf d(sizeof(double) * MAX_RHS);
+    Reduce r = rs.r((double *)d.p);
+    upload(fi, &in, 1, op.nsites(), st);
+    op.mdagm(fo, fi, &r, nullptr, st);
+    if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    download(&out, 1, op.nsites(), fo, st);
+    return CPSB_OK;
+  });
+}
+
+int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
+                   void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    Field fi(P64, op.nsites()), fo(P64, op.nsites());
+    RedSlot rs;
+    DevBuf d(sizeof(double) * MAX_RHS);
+    Reduce r = rs.r((double *)d.p);
+    CK(launch_pack(P64, fi.ptr(), in, op.nsites(), st));
+    op.mdagm(fo, fi, &r, nullptr, st);
+    CK(launch_unpack(P64, out, fo.ptr(), op.nsites(), st));
+    if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return CPSB_OK;
+  });
+}
+
+static int check_cg(const cpsb_cg_arg *a) {
+  if (!a) throw Error{CPSB_ERR_ARG, "null cg arguments"};
+  if (!(a->stop_rsd >= 0) || a->max_num_iter < 0) throw Error{CPSB_ERR_ARG, "bad stop_rsd / max_num_iter"};
+  if (a->precision < CPSB_PREC_F64 || a->precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+  return 0;
+}
+
+int cpsb_invcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs, double **x,
+                     const double *const *b, cpsb_solve_result *res) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (nrhs < 1 || nrhs > MAX_RHS || !x || !b || !res) throw Error{CPSB_ERR_ARG, "bad nrhs / vectors"};
+    for (int i = 0; i < nrhs; i++)
+      if (!x[i] || !b[i]) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = ctx().stream;
+    CgSolver *s = get_solver(&h->g, *p, a->precision, nrhs);
+    std::lock_guard<std::mutex> lk(s->busy);
+    const long n = cb_sites(h, p);
+    upload(s->x64, (const double *const *)x, nrhs, n, st);
+    upload(s->b64, b, nrhs, n, st);
+    int rc = s->solve(*a, res, st);
+    download(x, nrhs, n, s->x64, st);
+    return rc;
+  });
+}
+
+int cpsb_invcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *x, const double *b,
+               cpsb_solve_result *res) {
+  double *xs[1] = {x};
+  const double *bs[1] = {b};
+  return cpsb_invcg_multi(h, p, a, 1, xs, bs, res);
+}
+
+int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs, double *x,
+                         const double *b, cpsb_solve_result *res, void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (nrhs < 1 || nrhs > MAX_RHS || !x || !b || !res) throw Error{CPSB_ERR_ARG, "bad nrhs / vectors"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    CgSolver *s = get_solver(&h->g, *p, a->precision, nrhs);
+    std::lock_guard<std::mutex> lk(s->busy);
+    CK(launch_pack(P64, s->x64.ptr(), x, s->x64.nsites, st));
+    CK(launch_pack(P64, s->b64.ptr(), b, s->b64.nsites, st));
+    int rc = s->solve(*a, res, st);
+    CK(launch_unpack(P64, x, s->x64.ptr(), s->x64.nsites, st));
+    CK(cudaStreamSynchronize(st));
+    return rc;
+  });
+}
+
+int cpsb_invcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *x, const double *b,
+                   cpsb_solve_result *res, void *stream) {
+  return cpsb_invcg_multi_dev(h, p, a, 1, x, b, res, stream);
+}
+
+int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double **x, const double *b,
+                const double *shift, int nshift, double *rsd, int type, const double *alpha,
+                cpsb_solve_result *res) {
+  (void)h; (void)p; (void)a; (void)x; (void)b; (void)shift; (void)nshift; (void)rsd; (void)type; (void)alpha;
+  (void)res;
+  g_last_error = "multishift CG not built yet";
+  return CPSB_ERR_UNSUPPORTED;
+}
+
+int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
+                      double *bytes) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (reps < 1 || nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "bad reps / nrhs"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, precision, nrhs);
+    Field fi(precision, op.nsites()), fo(precision, op.nsites());
+    CK(cudaMemsetAsync(fi.data.p, 0, fi.data.bytes, st));
+    if (fi.norm.p) CK(cudaMemsetAsync(fi.norm.p, 0, fi.norm.bytes, st));
+    for (int i = 0; i < 3; i++) op.hop(fo, fi, 1, 0, 1.0, nullptr, nullptr, nullptr, st);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st));
+    for (int i = 0; i < reps; i++) op.hop(fo, fi, 1, 0, 1.0, nullptr, nullptr, nullptr, st);
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms) *ms = t / reps;
+    if (bytes) *bytes = op.hop_bytes();
+    return CPSB_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// cpsb_kernels.h -- host-visible launch interface of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "cpsb_device.cuh"
+
+namespace cpsb {
+
+// Reduction target: one partial per block (rhs-major), a ticket, and nrhs results.
+struct Reduce {
+  double *partial;
+  unsigned *ticket;
+  double *result;
+};
+
+struct DslashArgs {
+  Geom g;
+  GaugePtr U;
+  SpinorPtr in, out, x;   // x: the vector added by the xpay epilogue
+  int cb;                 // checkerboard of the input (output is 1-cb)
+  int dag;
+  int five_d;             // 1: DWF 5-D checkerboarding, 0: all slices share a 4-D parity
+  int hop5;               // 1: add the Shamir 5th-direction hop
+  double hop5_fact;       // 2*a5_inv
+  double hop5_wall;       // -2*m_f*a5_inv
+  double a;               // epilogue coefficient
+  double bc_t_sign;       // -1: reconstructed links need the antiperiodic sign at the t boundary
+  Reduce red;             // |out|^2 per RHS when requested
+  const int *skip;        // per-RHS: nonzero skips that RHS (device memory), may be null
+};
+
+// Grid: blockIdx.y = right-hand side, blockIdx.x strides over the sites of one RHS.
+int grid_blocks(long sites_per_rhs, int nt);
+
+cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int nt, cudaStream_t st);
+
+// ---------------------------------------------------------------- BLAS
+// All vectors share one Geom (nsites sites, nrhs right-hand sides).  Scalars
+// marked "dev" are read from device memory so the kernels can be captured in
+// CUDA graphs and need no host round trip.
+struct CgState;   // defined in cg_state.h
+
+cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, long nsites, cudaStream_t st);
+cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, long nsites, cudaStream_t st);
+cudaError_t launch_convert(int pdst, SpinorPtr dst, int psrc, SpinorPtr src, long nsites, cudaStream_t st);
+cudaError_t launch_gauge_pack(int prec, void *dst, const double *u_canonical, const int dims[4],
+                              int bc_t, cudaStream_t st);
+
+}  // namespace cpsb

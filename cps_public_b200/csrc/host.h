@@ -1,0 +1,143 @@
+// host.h -- host-side objects of libcpsb200: device context, resident gauge
+// fields, device spinor fields, the fermion operators and the solvers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cpsb200.h"
+#include "blas.h"
+#include "cg_state.h"
+#include "cpsb_kernels.h"
+
+namespace cpsb {
+
+// Thrown inside the library, converted to a status code at the C ABI.
+struct Error {
+  int code;
+  std::string msg;
+};
+void check_cuda(cudaError_t e, const char *what);
+#define CK(call) ::cpsb::check_cuda((call), #call)
+
+struct Context {
+  int device = -1;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+};
+Context &ctx();
+
+// Device allocation that remembers its size; freed on destruction.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t n);
+  ~DevBuf();
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  void alloc(size_t n);
+};
+
+struct Gauge {
+  int dims[4];
+  int bc_t = 0;
+  long n4cb = 0;
+  DevBuf u64;          // 18 reals per link, BondCond applied
+  DevBuf u32, u16;     // rows 0,1 per link (made on first use)
+  DevBuf canon;        // CANONICAL copy kept for building reduced precisions
+  bool recon_ok = false;
+  double recon_err = 0;
+  std::mutex mu;
+  GaugePtr ptr(int prec);
+};
+
+// A device spinor field in the chunked layout of cpsb_device.cuh.
+struct Field {
+  int prec = P64;
+  long nsites = 0;
+  DevBuf data, norm;
+  Field() = default;
+  Field(int prec, long nsites) { create(prec, nsites); }
+  void create(int prec, long nsites);
+  SpinorPtr ptr() const { return SpinorPtr{data.p, (float *)norm.p, nsites}; }
+  size_t bytes() const { return data.bytes + norm.bytes; }
+};
+size_t field_bytes(int prec, long nsites);
+
+// Reduction slot: partials for every block of a launch, a ticket and results.
+struct RedSlot {
+  DevBuf buf;
+  Reduce r(double *result);
+  RedSlot();
+};
+
+struct Operator {
+  Gauge *G;
+  cpsb_dirac_params p;
+  int prec;
+  int nrhs;
+  Geom geom;
+  double kappa = 0;        // Wilson / DWF
+  double kappa_b = 0;      // Mobius
+  M5Coef m5c[2];           // Mobius M5^-1 coefficient sets (dag 0, dag 1)
+  Field t1, t2, t3;
+  RedSlot red_inner;
+  int nt = 128;
+
+  Operator(Gauge *G, const cpsb_dirac_params &p, int prec, int nrhs);
+  long nsites() const { return geom.nsites; }
+  // out = a * D(cb, dag) in [+ x] with optional |out|^2 into red.
+  void hop(const Field &out, const Field &in, int cb, int dag, double a, const Field *x, const Reduce *red,
+           const int *skip, cudaStream_t st);
+  // DiracOp::Dslash front end
+  void dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st);
+  // out = MatPc in (dag 0) or MatPcDag in (dag 1); |out|^2 into red when given.
+  void matpc(const Field &out, const Field &in, int dag, const Reduce *red, const int *skip, cudaStream_t st);
+  // out = MatPcDagMatPc in; |MatPc in|^2 into red when given.
+  void mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st);
+  // Bytes one hop application must move (spinors in + out + links), for the roofline.
+  double hop_bytes() const;
+};
+
+// Workspace and state of one CG solve (reused across solves with the same shape).
+struct CgSolver {
+  Gauge *G;
+  cpsb_dirac_params p;
+  int sloppy;
+  int nrhs;
+  std::unique_ptr<Operator> op64, opS;
+  Field x64, b64, r64, Ap64;          // FP64 (x64/b64 are the caller's vectors packed)
+  Field rS, pS, ApS, xS;              // sloppy (xS is FP32 when sloppy is FP16)
+  DevBuf state;                       // CgState
+  CgState *hstate = nullptr;          // pinned mirror
+  DevBuf scal;                        // misc per-RHS scalars
+  RedSlot red_d, red_r, red_misc;
+  DevBuf tick;                        // ticket for the xp update
+  cudaGraphExec_t graph = nullptr;
+  int graph_batch = 0;
+  std::mutex busy;
+
+  CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
+  ~CgSolver();
+  // Solves with x64 (initial guess) and b64 already packed; fills res[nrhs].
+  int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st);
+
+ private:
+  void launch_batch(int k, cudaStream_t st);
+  void run_batches(int batch, cudaStream_t st, const bool *done, bool any);
+  void true_residual(double *rr_out, const double *bnorm, cudaStream_t st);
+};
+
+CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
+
+int multishift(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, Field &b64, std::vector<Field> &x,
+               const double *shift, int nshift, double *rsd, int type, const double *alpha, cpsb_solve_result *res,
+               cudaStream_t st);
+
+}  // namespace cpsb

@@ -1,0 +1,194 @@
+// m5.cu -- Mobius fifth-direction kernels: exact M5^-1 fused with the b/c
+// mixing of the 4-D hop.
+//
+// Restates, for real Mobius coefficients, zmobius_m5inv (cps_pp/src/util/
+// dirac_op/d_op_zmobius/noarch/zmobius_m5inv.C:247-400 dag 0, :534-686 dag 1):
+// a forward and a backward sweep along s per 4-D site and chirality with the
+// domain-wall wall correction, and the mixing  b*psi_s + c*(P+ psi_{s-1} +
+// P- psi_{s+1})  with -m_f walls of zmobius_kappa_dslash_5_plus_cmplx
+// (zmobius_dslash_5_plus.C:125-376).  The sweeps are independent for every
+// complex spinor component, so one thread owns one (site, storage chunk) column
+// of Ls values in registers and the pass reads and writes each value once.
+//
+//   dag 0:  out = scale * mix(M5^-1 in)                 (precedes D_W in MatPc)
+//   dag 1:  out = [x +] scale * M5^-dag(mix^dag(in))    (follows D_W^dag in MatPcDag)
+#include "blas.h"
+
+namespace cpsb {
+
+template <int P> struct ChunkT;
+template <> struct ChunkT<P64> { static const int NCH = 12, NC = 1; typedef double T; };
+template <> struct ChunkT<P32> { static const int NCH = 6, NC = 2; typedef float T; };
+
+template <int P>
+__device__ __forceinline__ void ld_chunk(const SpinorPtr &f, long i, int k, cplx<typename ChunkT<P>::T> *v);
+template <>
+__device__ __forceinline__ void ld_chunk<P64>(const SpinorPtr &f, long i, int k, cplx<double> *v) {
+  double2 a = __ldg((const double2 *)f.data + k * f.stride + i);
+  v[0] = mk(a.x, a.y);
+}
+template <>
+__device__ __forceinline__ void ld_chunk<P32>(const SpinorPtr &f, long i, int k, cplx<float> *v) {
+  float4 a = __ldg((const float4 *)f.data + k * f.stride + i);
+  v[0] = mk(a.x, a.y);
+  v[1] = mk(a.z, a.w);
+}
+template <int P>
+__device__ __forceinline__ void st_chunk(const SpinorPtr &f, long i, int k, const cplx<typename ChunkT<P>::T> *v);
+template <>
+__device__ __forceinline__ void st_chunk<P64>(const SpinorPtr &f, long i, int k, const cplx<double> *v) {
+  ((double2 *)f.data)[k * f.stride + i] = make_double2(v[0].re, v[0].im);
+}
+template <>
+__device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k, const cplx<float> *v) {
+  ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+}
+
+// v[s] += f * w[s] on one chunk
+#define AXPYC(dst, f, src)                                   \
+  _Pragma("unroll") for (int q = 0; q < NC; q++) {           \
+    (dst)[q].re += (f) * (src)[q].re;                        \
+    (dst)[q].im += (f) * (src)[q].im;                        \
+  }
+#define SCALC(dst, f)                                        \
+  _Pragma("unroll") for (int q = 0; q < NC; q++) {           \
+    (dst)[q].re *= (f);                                      \
+    (dst)[q].im *= (f);                                      \
+  }
+
+template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
+__global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
+                                                Reduce red, const int *skip) {
+  typedef typename ChunkT<P>::T T;
+  const int NCH = ChunkT<P>::NCH, NC = ChunkT<P>::NC;
+  __shared__ double sh[NT / 32];
+  const int rhs = blockIdx.y;
+  const long per = (long)g.n4cb * LS;
+  const long work = (long)g.n4cb * NCH;
+  double acc = 0;
+  const T K = (T)cf.K, b = (T)cf.b, c = (T)cf.c, mwall = (T)(-cf.mass * cf.c), sc = (T)cf.scale, invd = (T)cf.invd;
+  const bool sk = skip && skip[rhs];
+  for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
+    const int x = (int)(w % g.n4cb);
+    const int k = (int)(w / g.n4cb);
+    const bool upper = (k < NCH / 2);
+    const long base = rhs * per + x;
+    cplx<T> v[LS][NC], y[LS][NC];
+#pragma unroll
+    for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
+    if (DAG == 1) {
+      // mix^dag: upper from s+1, lower from s-1
+#pragma unroll
+      for (int s = 0; s < LS; s++) {
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
+        if (upper) {
+          if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
+        } else {
+          if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
+    }
+    // M5^-1 (DAG 0) or M5^-dag (DAG 1) sweeps.  The structure of the
+    // dag-0 lower sweep equals the dag-1 upper sweep and vice versa.
+    const bool walls_first = (DAG == 0) ? !upper : upper;
+    if (walls_first) {
+      SCALC(v[LS - 1], invd);
+#pragma unroll
+      for (int s = 0; s <= LS - 2; s++) { const T f = (T)cf.f1[s]; AXPYC(v[LS - 1], f, v[s]); }
+#pragma unroll
+      for (int s = LS - 2; s >= 0; s--) { AXPYC(v[s], -K, v[s + 1]); }
+    } else {
+#pragma unroll
+      for (int s = 0; s <= LS - 2; s++) { AXPYC(v[s + 1], -K, v[s]); }
+#pragma unroll
+      for (int s = LS - 2; s >= 0; s--) { const T f = (T)cf.f2[s]; AXPYC(v[s], f, v[LS - 1]); }
+      SCALC(v[LS - 1], invd);
+    }
+    if (DAG == 0) {
+      // mix: upper from s-1, lower from s+1
+#pragma unroll
+      for (int s = 0; s < LS; s++) {
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
+        if (upper) {
+          if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
+        } else {
+          if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
+    }
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      cplx<T> o[NC];
+      if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
+#pragma unroll
+      for (int q = 0; q < NC; q++) {
+        if (XPAY) o[q] = o[q] + cscale(sc, y[s][q]);
+        else o[q] = cscale(sc, y[s][q]);
+        if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
+      }
+      st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
+    }
+  }
+  if (NORM) {
+    double bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bs;
+    if (last_block(red.ticket, gridDim.x * gridDim.y)) {
+      for (int q = 0; q < g.nrhs; q++) {
+        double t = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
+        if (threadIdx.x == 0 && !(skip && skip[q])) red.result[q] = t;
+        __syncthreads();
+      }
+    }
+  }
+}
+
+template <int P, int LS>
+static cudaError_t m5_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                                int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  const int NT = 128;
+  dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
+#define M5L(D, XP, NR)                                                                              \
+  if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
+    m5_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
+    return cudaGetLastError();                                                                      \
+  }
+  M5L(0, false, false) M5L(0, true, false) M5L(0, true, true) M5L(0, false, true)
+  M5L(1, false, false) M5L(1, true, false) M5L(1, true, true) M5L(1, false, true)
+#undef M5L
+  return cudaErrorInvalidValue;
+}
+
+template <int P>
+static cudaError_t m5_launch_p(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                               int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  switch (g.ls) {
+    case 4: return m5_launch_ls<P, 4>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 8: return m5_launch_ls<P, 8>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 12: return m5_launch_ls<P, 12>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 16: return m5_launch_ls<P, 16>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 20: return m5_launch_ls<P, 20>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 24: return m5_launch_ls<P, 24>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    case 32: return m5_launch_ls<P, 32>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                      int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  if (prec == P64) return m5_launch_p<P64>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+  if (prec == P32) return m5_launch_p<P32>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+  return cudaErrorInvalidValue;  // FP16 Mobius storage is not supported by this kernel
+}
+
+}  // namespace cpsb

@@ -1,0 +1,267 @@
+// operator.cu -- device context, resident gauge fields, spinor fields and the
+// Wilson / DWF / Mobius preconditioned operators built from the kernels.
+//
+// Operator composition restates CPS:
+//  Wilson  MatPc = 1 - kappa^2 D_eo D_oe, kappa = 1/(2(m+4))
+//          (d_op_wilson/noarch/wilson_m.C:49-85, d_op_wilson.C:134-137)
+//  DWF     MatPc = 1 - kappa^2 D(cb=0) D(cb=1), kappa = 1/(2(4+a5_inv-M5)), D the
+//          5-D hop (dwf_m.C:31-63, dwf_init.C:97-98)
+//  Mobius  MatPc (SYM2) = 1 - kappa_b D4(0) M5^-1 kappa_b D4(1) M5^-1 with
+//          kappa_b = 1/(2(b(4-M5)+a5_inv)), kappa_c = 1/(2(c(4-M5)-a5_inv))
+//          (d_op_zmobius/noarch/zmobius_m-sym2.h:1-127, zmobius_mdag-sym2.h,
+//          d_op_mobius/d_op_mobius.C:106-109)
+//  MatPcDagMatPc = MatPcDag(MatPc in), |MatPc in|^2 fused into the MatPc pass
+//          (dwf_mdagm.C:32-62, mobius_mdagm.C:33-60, wilson_mdagm.C:83-160).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "host.h"
+
+namespace cpsb {
+
+void check_cuda(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  int code = (e == cudaErrorMemoryAllocation) ? CPSB_ERR_OOM : CPSB_ERR_CUDA;
+  cudaGetLastError();  // clear a non-sticky error
+  throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+Context &ctx() {
+  static Context c;
+  return c;
+}
+
+DevBuf::DevBuf(size_t n) { alloc(n); }
+void DevBuf::alloc(size_t n) {
+  if (p) {
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  if (n == 0) return;
+  CK(cudaMalloc(&p, n));
+  bytes = n;
+}
+DevBuf::~DevBuf() {
+  if (p) cudaFree(p);
+}
+
+size_t field_bytes(int prec, long nsites) {
+  if (prec == P64) return (size_t)nsites * 192;
+  if (prec == P32) return (size_t)nsites * 96;
+  return (size_t)nsites * 48 + (size_t)nsites * 4;
+}
+
+void Field::create(int pr, long n) {
+  prec = pr;
+  nsites = n;
+  data.alloc((size_t)n * (pr == P64 ? 192 : pr == P32 ? 96 : 48));
+  if (pr == P16) norm.alloc((size_t)n * 4);
+  else norm.alloc(0);
+}
+
+RedSlot::RedSlot() {
+  // partials: grid_blocks cap (148*16) * MAX_RHS; + ticket + padding
+  const size_t nparts = 148 * 16 * MAX_RHS;
+  buf.alloc(nparts * sizeof(double) + 256);
+  CK(cudaMemset(buf.p, 0, buf.bytes));
+}
+Reduce RedSlot::r(double *result) {
+  Reduce q;
+  q.partial = (double *)buf.p;
+  q.ticket = (unsigned *)((char *)buf.p + 148 * 16 * MAX_RHS * sizeof(double));
+  q.result = result;
+  return q;
+}
+
+GaugePtr Gauge::ptr(int prec) {
+  if (prec == P64) return GaugePtr{u64.p, n4cb};
+  std::lock_guard<std::mutex> lk(mu);
+  DevBuf &b = prec == P32 ? u32 : u16;
+  if (!b.p) {
+    if (!recon_ok)
+      throw Error{CPSB_ERR_UNSUPPORTED,
+                  "gauge field is not SU(3) to reduced-precision accuracy; recon-12 storage unavailable"};
+    b.alloc((size_t)n4cb * 2 * 4 * (prec == P32 ? 48 : 24));
+    CK(launch_gauge_pack(prec, b.p, (const double *)canon.p, dims, bc_t, ctx().stream));
+    CK(cudaStreamSynchronize(ctx().stream));
+  }
+  return GaugePtr{b.p, n4cb};
+}
+
+// ----------------------------------------------------------------- Operator
+static void m5_coefficients(double K, double mass, int ls, M5Coef *c0, M5Coef *c1) {
+  // dag 0 (zmobius_m5inv.C:247-400 with K[s] = K for all s)
+  memset(c0, 0, sizeof(M5Coef));
+  memset(c1, 0, sizeof(M5Coef));
+  double prod = 1.0;
+  for (int i = 0; i < ls; i++) prod *= -K;
+  prod *= mass;
+  const double invd0 = 1.0 / (1.0 + prod);
+  double fl = K * mass * invd0;
+  for (int s = 0; s <= ls - 2; s++) {
+    c0->f1[s] = fl;
+    fl *= -K;
+  }
+  double pr = 1.0;
+  for (int i = 0; i < ls - 1; i++) pr *= -K;
+  double fr = -pr * mass * invd0;
+  for (int s = ls - 2; s >= 0; s--) {
+    c0->f2[s] = fr;
+    fr /= -K;
+  }
+  c0->K = K;
+  c0->invd = invd0;
+  // dag 1 (zmobius_m5inv.C:534-686)
+  prod = 1.0;
+  for (int i = 0; i < ls; i++) prod *= K;
+  prod *= mass;
+  const double invd1 = 1.0 / (1.0 + prod);
+  double fr1 = K * mass * invd1;
+  for (int s = 0; s <= ls - 2; s++) {
+    c1->f1[s] = fr1;
+    fr1 *= -K;
+  }
+  pr = 1.0;
+  for (int i = 0; i < ls - 2; i++) pr *= -K;
+  pr *= -K;
+  double fl1 = -pr * mass * invd1;
+  for (int s = ls - 2; s >= 0; s--) {
+    c1->f2[s] = fl1;
+    if (s > 0) fl1 /= -K;
+  }
+  c1->K = K;
+  c1->invd = invd1;
+}
+
+Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g), p(pp), prec(pr), nrhs(nr) {
+  if (p.action < 0 || p.action > 2) throw Error{CPSB_ERR_ARG, "unknown action"};
+  const int ls = p.action == CPSB_WILSON ? 1 : p.ls;
+  if (ls < 1 || ls > 64) throw Error{CPSB_ERR_ARG, "ls out of range"};
+  if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
+  geom.lx = G->dims[0];
+  geom.ly = G->dims[1];
+  geom.lz = G->dims[2];
+  geom.lt = G->dims[3];
+  geom.lxh = geom.lx / 2;
+  geom.n4cb = (int)G->n4cb;
+  geom.ls = ls;
+  geom.nrhs = nrhs;
+  geom.nsites = (long)geom.n4cb * ls * nrhs;
+  if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
+  if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
+  if (p.action == CPSB_MOBIUS) {
+    if (p.pc_type != 2) throw Error{CPSB_ERR_UNSUPPORTED, "only the ZMOB_PC_SYM2 Mobius preconditioner is implemented"};
+    if (prec == P16) throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
+    const int ok[] = {4, 8, 12, 16, 20, 24, 32};
+    bool found = false;
+    for (int v : ok) found |= (v == ls);
+    if (!found) throw Error{CPSB_ERR_UNSUPPORTED, "Mobius Ls must be one of 4,8,12,16,20,24,32"};
+    kappa_b = 1.0 / (2 * (p.mobius_b * (4 - p.m5) + p.a5_inv));
+    const double kappa_c = 1.0 / (2 * (p.mobius_c * (4 - p.m5) - p.a5_inv));
+    m5_coefficients(kappa_b / kappa_c, p.mass, ls, &m5c[0], &m5c[1]);
+    for (int d = 0; d < 2; d++) {
+      m5c[d].b = p.mobius_b;
+      m5c[d].c = p.mobius_c;
+      m5c[d].mass = p.mass;
+      m5c[d].scale = 1.0;
+    }
+    t3.create(prec, geom.nsites);
+  }
+  t1.create(prec, geom.nsites);
+  t2.create(prec, geom.nsites);
+  nt = prec == P64 ? 128 : 128;
+}
+
+double Operator::hop_bytes() const {
+  const double spin = prec == P64 ? 192 : prec == P32 ? 96 : 52;
+  const double link = prec == P64 ? 144 : prec == P32 ? 48 : 24;
+  return 2.0 * spin * (double)geom.nsites + link * 4.0 * 2.0 * (double)geom.n4cb;
+}
+
+void Operator::hop(const Field &out, const Field &in, int cb, int dag, double a, const Field *x, const Reduce *red,
+                   const int *skip, cudaStream_t st) {
+  DslashArgs A;
+  memset(&A, 0, sizeof(A));
+  A.g = geom;
+  A.U = G->ptr(prec);
+  A.in = in.ptr();
+  A.out = out.ptr();
+  if (x) A.x = x->ptr();
+  A.cb = cb;
+  A.dag = dag;
+  A.five_d = p.action == CPSB_DWF;
+  A.hop5 = p.action == CPSB_DWF;
+  A.hop5_fact = 2.0 * p.a5_inv;
+  A.hop5_wall = -2.0 * p.mass * p.a5_inv;
+  A.a = a;
+  A.bc_t_sign = (prec != P64 && G->bc_t) ? -1.0 : 1.0;
+  if (red) A.red = *red;
+  A.skip = skip;
+  CK(launch_dslash(prec, A, x != nullptr, red != nullptr, nt, st));
+}
+
+void Operator::dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st) {
+  if (p.action != CPSB_MOBIUS) {
+    hop(out, in, cb, dag, 1.0, nullptr, nullptr, nullptr, st);
+    return;
+  }
+  // mobius_dslash (d_op_mobius/noarch/mobius_dslash.C:23-43): D4 (zmobius_dslash_4)
+  // plus the 5th-direction hop of the input with factor 1/kappa_c.
+  M5Coef mix;
+  memset(&mix, 0, sizeof(mix));
+  mix.K = 0.0;
+  mix.invd = 1.0;
+  mix.b = p.mobius_b;
+  mix.c = p.mobius_c;
+  mix.mass = p.mass;
+  mix.scale = 1.0;
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  if (!dag) {
+    CK(launch_m5(prec, 0, geom, t1.ptr(), in.ptr(), SpinorPtr{}, mix, 0, 0, none, nullptr, st));
+    hop(out, t1, cb, 0, 1.0, nullptr, nullptr, nullptr, st);
+  } else {
+    hop(t1, in, cb, 1, 1.0, nullptr, nullptr, nullptr, st);
+    CK(launch_m5(prec, 1, geom, out.ptr(), t1.ptr(), SpinorPtr{}, mix, 0, 0, none, nullptr, st));
+  }
+  const double kappa_c = 1.0 / (2 * (p.mobius_c * (4 - p.m5) - p.a5_inv));
+  M5Coef h5 = mix;
+  h5.b = 0.0;
+  h5.c = 1.0 / kappa_c;
+  // out = out + H5(in): the m5 kernel in xpay mode (K = 0 makes the sweep the identity)
+  CK(launch_m5(prec, dag, geom, out.ptr(), in.ptr(), out.ptr(), h5, 1, 0, none, nullptr, st));
+}
+
+void Operator::matpc(const Field &out, const Field &in, int dag, const Reduce *red, const int *skip,
+                     cudaStream_t st) {
+  if (p.action != CPSB_MOBIUS) {
+    hop(t1, in, 1, dag, 1.0, nullptr, nullptr, skip, st);
+    hop(out, t1, 0, dag, -kappa * kappa, &in, red, skip, st);
+    return;
+  }
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  if (!dag) {
+    CK(launch_m5(prec, 0, geom, t1.ptr(), in.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
+    hop(t3, t1, 1, 0, kappa_b, nullptr, nullptr, skip, st);
+    CK(launch_m5(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
+    hop(out, t1, 0, 0, -kappa_b, &in, red, skip, st);
+  } else {
+    hop(t1, in, 1, 1, -kappa_b, nullptr, nullptr, skip, st);
+    M5Coef c = m5c[1];
+    c.scale = kappa_b;
+    CK(launch_m5(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, c, 0, 0, none, skip, st));
+    hop(t1, t3, 0, 1, 1.0, nullptr, nullptr, skip, st);
+    CK(launch_m5(prec, 1, geom, out.ptr(), t1.ptr(), in.ptr(), m5c[1], 1, red != nullptr, red ? *red : none, skip,
+                 st));
+  }
+}
+
+void Operator::mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st) {
+  matpc(t2, in, 0, red, skip, st);
+  matpc(out, t2, 1, nullptr, skip, st);
+}
+
+}  // namespace cpsb

@@ -1,0 +1,300 @@
+// solver.cu -- conjugate-gradient drivers on MatPcDagMatPc.
+//
+// Plain FP64 CG restates DiracOp::InvCgShift (cps_pp/src/util/dirac_op/d_op_base/
+// comsrc/inv_cg.C:84-447): the same recurrence, stopping test |r|^2 <=
+// stop_rsd^2 |src|^2 on the iterated residual, at most max_num_iter-1
+// iterations, the true residual computed once at the end, and itr+1 returned.
+//
+// Mixed precision runs the same recurrence in FP32 or FP16 storage (FP32
+// arithmetic, FP64 reductions) and replaces the residual by the FP64 true
+// residual b - A x whenever the iterated residual has dropped by
+// reliable_delta since the last replacement, or claims convergence; the
+// solution is accumulated in FP64 at each replacement, and the solve only ends
+// when the FP64 true residual meets the tolerance.
+//
+// Iterations are launched in batches captured as one CUDA graph: every scalar
+// lives in device memory (CgState) and a halting RHS turns the rest of the batch
+// into early exits, so the host only reads the state between batches.
+#include <math.h>
+#include <string.h>
+
+#include <chrono>
+
+#include "host.h"
+
+namespace cpsb {
+
+CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g), p(pp), sloppy(sl), nrhs(nr) {
+  op64.reset(new Operator(G, p, P64, nrhs));
+  const long n = op64->nsites();
+  x64.create(P64, n);
+  b64.create(P64, n);
+  r64.create(P64, n);
+  Ap64.create(P64, n);
+  if (sloppy != P64) {
+    opS.reset(new Operator(G, p, sloppy, nrhs));
+    G->ptr(sloppy);  // build the reduced-precision links now, never inside a graph capture
+    rS.create(sloppy, n);
+    pS.create(sloppy, n);
+    ApS.create(sloppy, n);
+    xS.create(P32, n);
+  } else {
+    rS.create(P64, n);  // r, p, Ap of the FP64 recurrence
+    pS.create(P64, n);
+    ApS.create(P64, n);
+  }
+  state.alloc(sizeof(CgState));
+  CK(cudaMallocHost((void **)&hstate, sizeof(CgState)));
+  scal.alloc(sizeof(double) * MAX_RHS * 8);
+  tick.alloc(256);
+  CK(cudaMemset(tick.p, 0, 256));
+}
+
+CgSolver::~CgSolver() {
+  if (graph) cudaGraphExecDestroy(graph);
+  if (hstate) cudaFreeHost(hstate);
+}
+
+static Scal2 sc2(int n, double a, double b) {
+  Scal2 s;
+  for (int i = 0; i < MAX_RHS; i++) {
+    s.a[i] = a;
+    s.b[i] = b;
+  }
+  (void)n;
+  return s;
+}
+
+// One batch of k iterations of the (sloppy or FP64) recurrence.
+void CgSolver::launch_batch(int k, cudaStream_t st) {
+  CgState *S = (CgState *)state.p;
+  Operator &op = opS ? *opS : *op64;
+  const int px = opS ? P32 : P64;
+  Field &xx = opS ? xS : x64;
+  Reduce rd = red_d.r(S->d);
+  Reduce rr = red_r.r(nullptr);
+  for (int j = 0; j < k; j++) {
+    op.mdagm(ApS, pS, &rd, S->halt, st);
+    CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), S, rr, st));
+    CK(launch_cg_xp_update(px, op.prec, op.geom, xx.ptr(), pS.ptr(), rS.ptr(), S, (unsigned *)tick.p, st));
+  }
+}
+
+void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool any) {
+  if (!graph || graph_batch != batch) {
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch_batch(batch, st);
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(st, &g));
+    CK(cudaGraphInstantiate(&graph, g, 0));
+    cudaGraphDestroy(g);
+    graph_batch = batch;
+  }
+  for (;;) {
+    CK(cudaGraphLaunch(graph, st));
+    CK(cudaMemcpyAsync(hstate, state.p, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    bool all = true, one = false;
+    for (int q = 0; q < nrhs; q++) {
+      all = all && hstate->halt_done[q];
+      one = one || (hstate->halt_done[q] && !done[q]);
+    }
+    if (all || (any && one)) return;
+  }
+}
+
+// rr_out[q] = |b - A x64|^2 (FP64), leaves r64 = b - A x64.
+void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t st) {
+  (void)bnorm;
+  double *dres = (double *)scal.p;
+  op64->mdagm(Ap64, x64, nullptr, nullptr, st);
+  Reduce rm = red_misc.r(dres);
+  CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, Ap64.ptr(), op64->geom, sc2(nrhs, 1.0, -1.0), nullptr, rm, 1,
+                  st));
+  CK(cudaMemcpyAsync(rr_out, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+}
+
+int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st) {
+  auto t0 = std::chrono::steady_clock::now();
+  const Geom &gg = op64->geom;
+  double bnorm[MAX_RHS], rr[MAX_RHS];
+  double *dres = (double *)scal.p;
+  // |b|^2
+  {
+    Reduce rm = red_misc.r(dres);
+    CK(launch_redot(P64, gg, b64.ptr(), b64.ptr(), rm, st));
+    CK(cudaMemcpyAsync(bnorm, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  // r = b - A x
+  true_residual(rr, bnorm, st);
+  CgState hs;
+  memset(&hs, 0, sizeof(hs));
+  const double delta = sloppy == P64 ? 0.0 : (a.reliable_delta > 0 ? a.reliable_delta : 0.1);
+  hs.delta = delta;
+  hs.max_iter = a.max_num_iter;
+  hs.nrhs = nrhs;
+  int nupd[MAX_RHS] = {0};
+  bool done[MAX_RHS];
+  for (int q = 0; q < nrhs; q++) {
+    hs.rr[q] = rr[q];
+    hs.stp[q] = bnorm[q] * a.stop_rsd * a.stop_rsd;
+    hs.maxr[q] = sqrt(rr[q]);
+    done[q] = (rr[q] <= hs.stp[q]) || (a.max_num_iter - 1 <= 0);
+    hs.halt[q] = hs.halt_done[q] = done[q] ? 1 : 0;
+    hs.reason[q] = done[q] ? HALT_CONVERGED : HALT_NONE;
+    if (bnorm[q] == 0.0) {  // CPS divides by |src|^2; a zero source is solved by x = 0
+      done[q] = true;
+      hs.halt[q] = hs.halt_done[q] = 1;
+    }
+  }
+  // p = r (sloppy copy of r), xS = 0
+  if (opS) {
+    CK(launch_convert(sloppy, rS.ptr(), P64, r64.ptr(), gg.nsites, st));
+    CK(cudaMemsetAsync(xS.data.p, 0, xS.data.bytes, st));
+  } else {
+    CK(cudaMemcpyAsync(rS.data.p, r64.data.p, r64.data.bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  CK(cudaMemcpyAsync(pS.data.p, rS.data.p, rS.data.bytes, cudaMemcpyDeviceToDevice, st));
+  if (pS.norm.p) CK(cudaMemcpyAsync(pS.norm.p, rS.norm.p, rS.norm.bytes, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(state.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st));
+
+  int batch = a.batch > 0 ? a.batch : 16;
+  int status = CPSB_OK;
+  for (;;) {
+    bool all = true;
+    for (int q = 0; q < nrhs; q++) all = all && done[q];
+    if (all) break;
+    run_batches(batch, st, done, opS != nullptr);
+    CgState h = *hstate;
+    if (!opS) {
+      for (int q = 0; q < nrhs; q++) done[q] = true;
+      break;
+    }
+    // Reliable update for every RHS that paused: x += xS, xS = 0, r = b - A x
+    // in FP64.  RHS still iterating are masked out of every update.
+    int *dskip = (int *)((double *)scal.p + MAX_RHS * 4);
+    int skip_h[MAX_RHS];
+    for (int q = 0; q < nrhs; q++) skip_h[q] = (done[q] || !h.halt_done[q]) ? 1 : 0;
+    CK(cudaMemcpyAsync(dskip, skip_h, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, st));
+    Reduce none;
+    memset(&none, 0, sizeof(none));
+    CK(launch_axpby(P64, x64.ptr(), P64, x64.ptr(), P32, xS.ptr(), gg, sc2(nrhs, 1.0, 1.0), dskip, none, 0, st));
+    CK(launch_axpby(P32, xS.ptr(), P32, xS.ptr(), P32, SpinorPtr{}, gg, sc2(nrhs, 0.0, 0.0), dskip, none, 0, st));
+    true_residual(rr, bnorm, st);
+    Scal2 beta = sc2(nrhs, 1.0, 0.0);
+    for (int q = 0; q < nrhs; q++) {
+      if (skip_h[q]) continue;
+      nupd[q]++;
+      const int reason = h.reason[q];
+      if (rr[q] <= h.stp[q]) {
+        done[q] = true;
+        h.reason[q] = HALT_CONVERGED;
+        continue;
+      }
+      if (reason == HALT_MAXITER || reason == HALT_BREAKDOWN) {
+        done[q] = true;
+        continue;
+      }
+      // continue: r_s = r (true), p = r + beta p with beta = rr_true / rr_prev
+      beta.b[q] = rr[q] / h.rr_prev[q];
+      h.rr[q] = rr[q];
+      h.maxr[q] = sqrt(rr[q]);
+      h.halt[q] = h.halt_done[q] = 0;
+      h.reason[q] = HALT_NONE;
+    }
+    // Refresh r and p only for the RHS that paused and now resume.
+    int refresh_skip[MAX_RHS];
+    for (int q = 0; q < nrhs; q++) {
+      const bool resumed = !skip_h[q] && !done[q];
+      refresh_skip[q] = resumed ? 0 : 1;
+      if (done[q]) h.halt[q] = h.halt_done[q] = 1;
+    }
+    CK(cudaMemcpyAsync(dskip, refresh_skip, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, st));
+    CK(launch_axpby(sloppy, rS.ptr(), P64, r64.ptr(), P64, SpinorPtr{}, gg, sc2(nrhs, 1.0, 0.0), dskip, none, 0, st));
+    CK(launch_axpby(sloppy, pS.ptr(), sloppy, rS.ptr(), sloppy, pS.ptr(), gg, beta, dskip, none, 0, st));
+    // The device was idle since the state was read, so h is current for the RHS
+    // that kept running and updated for the others.
+    CK(cudaMemcpyAsync(state.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    *hstate = h;
+  }
+  // Final FP64 true residual (inv_cg.C:401-417).
+  CgState h = *hstate;
+  if (!opS) true_residual(rr, bnorm, st);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int q = 0; q < nrhs; q++) {
+    res[q].iters = h.iters[q] + 1;
+    res[q].true_rsd = bnorm[q] > 0 ? sqrt(rr[q] / bnorm[q]) : 0.0;
+    res[q].iter_rsd = bnorm[q] > 0 ? sqrt(h.rr[q] / bnorm[q]) : 0.0;
+    res[q].reliable_updates = nupd[q];
+    res[q].seconds = secs;
+    int stq = CPSB_OK;
+    if (h.reason[q] == HALT_BREAKDOWN) stq = CPSB_ERR_BREAKDOWN;
+    else if (!(rr[q] <= bnorm[q] * a.stop_rsd * a.stop_rsd) && h.reason[q] != HALT_CONVERGED) stq = CPSB_NOT_CONVERGED;
+    else if (opS && !(rr[q] <= bnorm[q] * a.stop_rsd * a.stop_rsd)) stq = CPSB_NOT_CONVERGED;
+    res[q].status = stq;
+    if (stq == CPSB_ERR_BREAKDOWN) status = stq;
+    else if (stq == CPSB_NOT_CONVERGED && status == CPSB_OK) status = stq;
+  }
+  return status;
+}
+
+// One cached solver per (gauge, parameters, precision, nrhs).
+struct SolverKey {
+  Gauge *G;
+  int action, ls, sloppy, nrhs, pc;
+  double mass, m5, a5, b, c;
+  bool operator<(const SolverKey &o) const {
+    return memcmp(this, &o, sizeof(SolverKey)) < 0;
+  }
+};
+static std::map<SolverKey, std::unique_ptr<CgSolver>> &solvers() {
+  static std::map<SolverKey, std::unique_ptr<CgSolver>> m;
+  return m;
+}
+static std::mutex solvers_mu;
+
+CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs) {
+  SolverKey k;
+  memset(&k, 0, sizeof(k));
+  k.G = G;
+  k.action = p.action;
+  k.ls = p.action == CPSB_WILSON ? 1 : p.ls;
+  k.sloppy = sloppy;
+  k.nrhs = nrhs;
+  k.pc = p.pc_type;
+  k.mass = p.mass;
+  k.m5 = p.m5;
+  k.a5 = p.a5_inv;
+  k.b = p.mobius_b;
+  k.c = p.mobius_c;
+  std::lock_guard<std::mutex> lk(solvers_mu);
+  auto &m = solvers();
+  auto it = m.find(k);
+  if (it != m.end()) return it->second.get();
+  CgSolver *s = new CgSolver(G, p, sloppy, nrhs);
+  m[k].reset(s);
+  return s;
+}
+
+void drop_solvers(Gauge *G) {
+  std::lock_guard<std::mutex> lk(solvers_mu);
+  auto &m = solvers();
+  for (auto it = m.begin(); it != m.end();) {
+    if (it->first.G == G) it = m.erase(it);
+    else ++it;
+  }
+}
+
+}  // namespace cpsb

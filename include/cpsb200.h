@@ -1,0 +1,165 @@
+/* cpsb200.h -- C ABI of the B200 fermion-matrix library (libcpsb200.so).
+ *
+ * A drop-in device implementation of the CPS (RBC-UKQCD/CPS_public, cps_pp)
+ * fermion-matrix hot path: the even-odd preconditioned Wilson, Shamir
+ * domain-wall and Mobius operators and the CG / multishift-CG solvers that
+ * drive them.  Every entry point replaces one CPS interface, cited below by
+ * file:line relative to cps_pp/.  Vectors use CPS storage order: a checkerboard
+ * vector is sites x 24 doubles (r + 2*(colour + 3*spin)); a 5-D vector is Ls
+ * consecutive 4-D slices (5-D checkerboarding for DWF, the DWF_4D_EOPREC_EE
+ * half for Mobius), exactly as DiracOp*::MatPcDagMatPc receives it.
+ *
+ * Errors are reported as status codes (CPS instead prints through ERR and
+ * calls exit(), include/util/error.h:26-80): 0 ok, 1 not converged within
+ * max_num_iter (CPS only warns, inv_cg.C:392-396), negative values are errors.
+ * Host-pointer entry points copy in and out and keep no host pointer after
+ * returning; gauge handles stay resident on the device until freed.
+ */
+#ifndef CPSB200_H
+#define CPSB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPSB_OK 0
+#define CPSB_NOT_CONVERGED 1
+#define CPSB_ERR_ARG (-1)
+#define CPSB_ERR_CUDA (-2)
+#define CPSB_ERR_OOM (-3)
+#define CPSB_ERR_UNSUPPORTED (-4)
+#define CPSB_ERR_BREAKDOWN (-5)
+#define CPSB_ERR_NO_DEVICE (-6)
+#define CPSB_ERR_BUSY (-7)
+
+enum cpsb_action { CPSB_WILSON = 0, CPSB_DWF = 1, CPSB_MOBIUS = 2 };
+enum cpsb_precision { CPSB_PREC_F64 = 0, CPSB_PREC_F32 = 1, CPSB_PREC_F16 = 2 };
+enum cpsb_gauge_order { CPSB_ORDER_CANONICAL = 0, CPSB_ORDER_WILSON = 1 };
+enum cpsb_multishift_type { CPSB_MULTI = 0, CPSB_SINGLE = 1 };
+
+typedef struct cpsb_gauge_s *cpsb_gauge;
+
+/* Operator parameters: the fields CPS reads from CgArg and GJP.
+ *   mass    CgArg::mass (include/alg/cg_arg.h:17-36).  Wilson: kappa =
+ *           1/(2(mass+4)) (d_op_wilson/noarch/d_op_wilson.C:134-137); DWF and
+ *           Mobius: the domain-wall mass m_f.
+ *   m5      GJP.DwfHeight() (include/util/gjp.h:579)
+ *   a5_inv  GJP.DwfA5Inv() (gjp.h:587)
+ *   mobius_b, mobius_c   GJP.Mobius_b/c() (gjp.h:594-601)
+ *   pc_type GJP.ZMobius_PC_Type(): only ZMOB_PC_SYM2 (= 2), the CPS default
+ *           (src/util/gjp/gjp.C:129), is implemented on the device. */
+typedef struct {
+  int action;
+  int ls;
+  double mass;
+  double m5;
+  double a5_inv;
+  double mobius_b;
+  double mobius_c;
+  int pc_type;
+} cpsb_dirac_params;
+
+/* Solver controls: CgArg::stop_rsd / max_num_iter plus the precision forms.
+ *   precision       inner (sloppy) precision; CPSB_PREC_F64 runs the plain CPS
+ *                   CG recurrence in FP64
+ *   reliable_delta  FP64 residual replacement whenever |r| drops by this factor
+ *                   since the last one (mixed precision only; 0 -> 0.1)
+ *   batch           iterations launched per device batch (0 -> automatic) */
+typedef struct {
+  double stop_rsd;
+  int max_num_iter;
+  int precision;
+  double reliable_delta;
+  int batch;
+} cpsb_cg_arg;
+
+/* Per-solve report.  iters follows CPS (DiracOp::InvCg returns itr+1,
+ * inv_cg.C:444); true_rsd = |b - A x|/|b| computed in FP64 after the solve
+ * (inv_cg.C:401-417). */
+typedef struct {
+  int iters;
+  double true_rsd;
+  double iter_rsd;
+  int reliable_updates;
+  double seconds;
+  int status;
+} cpsb_solve_result;
+
+/* Selects the CUDA device and creates the library context (one per process). */
+int cpsb_init(int device);
+const char *cpsb_error_string(int code);
+/* Detail message of the last error raised on the calling thread. */
+const char *cpsb_last_error(void);
+/* Free and total device memory in bytes (the serving loop admits work by it). */
+int cpsb_mem_info(unsigned long long *free_bytes, unsigned long long *total_bytes);
+
+/* Uploads a gauge field and keeps it resident (FP64 plus the reduced-precision
+ * copies made on first use).  u: 4*V 3x3 complex links; order CANONICAL
+ * (Lattice::GaugeField(), lattice/convert/convert_func.C:397-405) or WILSON
+ * (the order DiracOp constructors convert to, convert_func.C:371-405).
+ * bc_t = 1 applies the antiperiodic time boundary as Lattice::BondCond does
+ * (lattice/lattice_base/lattice_base.C:5313-5370).  Replaces the gauge half of
+ * the DiracOp constructor (d_op_dwf/d_op_dwf.C:67-123). */
+int cpsb_gauge_load(cpsb_gauge *h, const double *u, const int dims[4], int order, int bc_t);
+int cpsb_gauge_free(cpsb_gauge h);
+
+/* DiracOp*::Dslash(out, in, cb, dag) (include/util/dirac_op.h:275):
+ * d_op_wilson/noarch/d_op_wilson.C:180 (wilson_dslash), d_op_dwf/d_op_dwf.C:210
+ * (dwf_dslash), d_op_mobius/d_op_mobius.C:273 (mobius_dslash). */
+int cpsb_dslash(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, int cb, int dag);
+
+/* DiracOp*::MatPc (dag = 0) / MatPcDag (dag = 1): d_op_wilson.C:204,228;
+ * d_op_dwf.C:245-300; d_op_mobius.C:319-372. */
+int cpsb_matpc(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, int dag);
+
+/* DiracOp*::MatPcDagMatPc(out, in, dot_prd) (dirac_op.h:262); dot, when not
+ * NULL, receives |MatPc in|^2 as CPS's fused norm does (dwf_mdagm.C:49-55). */
+int cpsb_mdagm(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot);
+
+/* DiracOp::InvCg through Lattice::FmatEvlInv(f_out, f_in, cg_arg, true_res)
+ * (include/util/lattice.h:942; lattice/f_wilson/f_wilson.C:159,
+ * f_dwf_base/f_dwf_base.C:189, f_mobius/f_mobius.C:582): solves
+ * MatPcDagMatPc x = b by CG from the initial guess in x. */
+int cpsb_invcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *x, const double *b,
+               cpsb_solve_result *res);
+
+/* nrhs independent solves batched into one launch sequence (each link load
+ * serves all right-hand sides): the multi-source DiracOpMobius::MatInv
+ * (dirac_op.h:1886) / QUDA split-grid path (d_op_mobius/noarch/mobius_quda.C:32-340)
+ * at the FmatEvlInv level.  x[i], b[i]: nrhs host vectors; res: nrhs reports. */
+int cpsb_invcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs, double **x,
+                     const double *const *b, cpsb_solve_result *res);
+
+/* DiracOp::MInvCG via Lattice::FmatEvlMInv (lattice.h:976; f_dwf_base.C:232,
+ * f_mobius.C:628; d_op_base/noarch/minvcg.C:47-353): solves
+ * (MatPcDagMatPc + shift[s]) x[s] = b for all shifts (shift[0] the smallest).
+ * type CPSB_MULTI writes x[0..nshift); CPSB_SINGLE writes sum_s alpha[s] x_s to
+ * x[0].  rsd[s]: stop_rsd per shift on entry; on return the residual reported
+ * per shift.  With a->precision != F64 the Krylov vectors are kept in that
+ * precision and every shift is then refined by mixed-precision CG to its
+ * tolerance with an FP64 true residual (rsd[s] then holds that true residual). */
+int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double **x, const double *b,
+                const double *shift, int nshift, double *rsd, int type, const double *alpha,
+                cpsb_solve_result *res);
+
+/* Device-resident variants: x, b (and out/in) are device pointers holding CPS
+ * order vectors; stream is a cudaStream_t (NULL = the library stream).  These
+ * are what a caller with fields already in HBM uses. */
+int cpsb_invcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *x, const double *b,
+                   cpsb_solve_result *res, void *stream);
+int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs, double *x,
+                         const double *b, cpsb_solve_result *res, void *stream);
+int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
+                   void *stream);
+
+/* Times `reps` applications of the device Dslash of the given precision on
+ * internally resident data (one checkerboard, dag 0); reports the mean kernel
+ * time in ms measured with CUDA events on the launching stream, and the bytes
+ * each application must move (spinors in + out + links). */
+int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
+                      double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CPSB200_H */
