@@ -1,0 +1,364 @@
+"""Benchmark: Shamir DWF even-odd CG solves/s at true residual 1e-10, mixed vs FP64.
+
+Workload (the reference's headline DWF configuration): 16^3 x 32 lattice,
+Ls = 16, M5 = 1.8, m_f = 0.01, links reunitarise(exp(i 0.2 H)) seeded,
+Gaussian source on the odd checkerboard, stop_rsd 1e-10 on the FP64 true
+residual.  A step is one full solve (MatPcDagMatPc x = b from x = 0).
+
+Arms:
+  (default)        this library: FP16-storage mixed CG is the headline `value`;
+                   FP32-mixed and plain FP64 CG are timed beside it.  `value` uses
+                   device-resident inputs (cpsb_invcg_dev); `e2e` goes through the
+                   host-pointer C ABI (cpsb_invcg) with the H2D copy of b and the
+                   D2H copy of x in every step.
+  --impl reference the CPS noarch CPU code (oracle/_ref/cpsref, compiled from the
+                   reference sources) on all host cores: each step runs one
+                   MatPcDagMatPc per core in parallel processes, and solves/s is
+                   extrapolated with the FP64 CG iteration count of this workload.
+
+Multi-GPU (--gpus N under torchrun): independent replicas, one per GPU, no
+data-path collective; value = solves on all ranks / max elapsed over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (16, 16, 16, 32)
+LS = 16
+M5 = 1.8
+MF = 0.01
+EPS = 0.2
+STOP = 1e-10
+SEED = 2024
+METRIC = "dwf_cg_solves_per_s"
+UNIT = "solves/s"
+# FP64 CG iterations (CPS counting, itr+1) of this workload, measured on B200 by
+# the FP64 solver, which runs CPS's recurrence (its iteration counts match the
+# compiled reference within one on every golden case).  The CPU arm uses it to
+# turn one timed MatPcDagMatPc into solves/s.
+FP64_ITERS = None
+WORKLOAD = {"workload": "shamir_dwf_eo_cg_16x16x16x32_ls16", "lattice": "16^3x32", "ls": LS, "m5": M5, "mf": MF,
+            "link_eps": EPS, "stop_true_rsd": STOP, "source": "gaussian odd checkerboard", "reliable_delta": 0.1,
+            "l2": "inputs larger than L2 (201 MB FP64 / 52 MB FP16 per vector, 75 MB FP64 links)"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if len(r) >= 8 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 8:
+                continue
+            for n, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the FP16 Dslash from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "dslash_dram_traffic.json")))
+        return d
+    except Exception:
+        return None
+
+
+def make_inputs(nsrc):
+    from cps_public_b200 import fields
+    u = fields.random_gauge(DIMS, EPS, SEED)
+    n5 = int(np.prod(DIMS)) // 2 * LS
+    srcs = [fields.random_source(n5, SEED + 1 + i) for i in range(nsrc)]
+    return u, srcs
+
+
+def run_ours(args):
+    import torch
+    import cps_public_b200 as cb
+    from cps_public_b200 import _lib
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    cb.init(local)
+    lib = _lib.load()
+    u, srcs = make_inputs(args.steps + args.warmup)
+    g = cb.Gauge(u, DIMS)
+    op = cb.DiracOp(g, "dwf", mass=MF, ls=LS, m5=M5)
+    n = op.n
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    b_dev = [torch.from_numpy(s).to(dev) for s in srcs]
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    res = cb.SolveResult()
+
+    import ctypes as C
+
+    def solve_on_device(b, prec):
+        x_dev.zero_()
+        a = cb.CgArg(STOP, 100000, prec, 0.1, 0)
+        rc = lib.cpsb_invcg_dev(g.h, C.byref(op.p), C.byref(a), C.c_void_p(x_dev.data_ptr()),
+                                C.c_void_p(b.data_ptr()), C.byref(res), C.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"solve failed rc={rc} {res.as_dict()}")
+        return res.as_dict()
+
+    variants = {"f16_mixed": cb.F16, "f32_mixed": cb.F32, "f64": cb.F64}
+    out = {}
+    sampler = ClockSampler(local)
+    launches0 = C.c_ulonglong()
+    launches1 = C.c_ulonglong()
+    for name, prec in variants.items():
+        for w in range(args.warmup):
+            solve_on_device(b_dev[w % len(b_dev)], prec)
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        if name == "f16_mixed":
+            sampler.start()
+            lib.cpsb_kernel_launches(C.byref(launches0))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        infos = []
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            infos.append(solve_on_device(b_dev[(args.warmup + k) % len(b_dev)], prec))
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if name == "f16_mixed":
+            lib.cpsb_kernel_launches(C.byref(launches1))
+            clocks = sampler.stop()
+        lat = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
+        total_ms = ev[0][0].elapsed_time(ev[-1][1])
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([total_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        out[name] = {"solves_per_s": world * args.steps / (total_ms / 1000.0), "ms_per_step": total_ms / args.steps,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "iters": int(statistics.median(i["iters"] for i in infos)),
+                     "max_true_rsd": max(i["true_rsd"] for i in infos),
+                     "reliable_updates": int(statistics.median(i["reliable_updates"] for i in infos))}
+    # e2e: host buffers through the public host-pointer entry point
+    e2e_lat = []
+    for w in range(args.warmup):
+        op.InvCg(srcs[w], stop_rsd=STOP, max_num_iter=100000, precision=cb.F16)
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        x, r = op.InvCg(srcs[(args.warmup + k) % len(srcs)], stop_rsd=STOP, max_num_iter=100000, precision=cb.F16)
+        e2e_lat.append(time.perf_counter() - t0)
+        assert r.true_rsd <= STOP
+    e2e_total = sum(e2e_lat)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    # Dslash roofline (the dominant kernel of the headline solve: FP16 5-D hop)
+    dsl = {}
+    peak, peak_kind = peak_hbm()
+    for pname, prec in (("f16", cb.F16), ("f32", cb.F32), ("f64", cb.F64)):
+        ms, by = C.c_double(), C.c_double()
+        lib.cpsb_bench_dslash(g.h, C.byref(op.p), prec, 1, 50, C.byref(ms), C.byref(by))
+        gbs = by.value / (ms.value * 1e-3) / 1e9
+        dsl[pname] = {"ms": ms.value, "bytes": by.value, "gbs": gbs, "frac": gbs / peak}
+    traffic = ncu_traffic()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    head = out["f16_mixed"]
+    line = {
+        "metric": METRIC, "value": head["solves_per_s"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16-storage/f32-math, f64 reliable updates",
+        "data": "synthetic (seeded reunitarised exp(i*0.2*H) links, Gaussian source)",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}"),
+        "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
+        "variants": out,
+        "mixed_vs_fp64": head["solves_per_s"] / out["f64"]["solves_per_s"],
+        "e2e": {"value": world * args.steps / e2e_total, "unit": UNIT, "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": n * 8, "path": "cpsb_invcg (host pointers, pinned staging)"},
+        "roofline": {"bound": "hbm", "achieved": dsl["f16"]["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": dsl["f16"]["frac"], "peak_kind": peak_kind,
+                     "traffic": (traffic or {}).get("f16_bytes_per_launch"),
+                     "kernel": "dslash_kernel<P16> (5-D Shamir hop, one checkerboard)",
+                     "algorithmic_bytes": dsl["f16"]["bytes"]},
+        "dslash_gbs": {k: v["gbs"] for k, v in dsl.items()},
+        "dslash_frac": {k: v["frac"] for k, v in dsl.items()},
+        "gpu_launches": int(launches1.value - launches0.value),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(u, srcs[0], out["f64"]["iters"])
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def _ref_mdagm_seconds(u, src, nproc, threads_per_proc=1):
+    """Runs nproc concurrent reference processes, each timing one MatPcDagMatPc;
+    returns (wall seconds, per-process in-harness seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import refrun
+
+    def one(_):
+        _, rp, _ = refrun.run(refrun.OP_BENCH, "dwf", DIMS, u, [src], ls=LS, mass=MF, m5=M5, reps=1,
+                              threads=threads_per_proc)
+        return rp[10]
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=nproc) as ex:
+        ts = list(ex.map(one, range(nproc)))
+    return time.perf_counter() - t0, ts
+
+
+def cpu_baseline(u, src, iters):
+    from oracle import refrun
+    cores = os.cpu_count() or 1
+    if refrun.available():
+        wall, ts = _ref_mdagm_seconds(u, src, cores)
+        per = statistics.median(ts)
+        rate = cores / (per * iters)
+        return {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"{cores} concurrent CPS noarch processes, one MatPcDagMatPc each at 16^3x32x16 "
+                          f"({per:.2f} s each); solves/s extrapolated with {iters} CG iterations",
+                "mdagm_s": per}
+    from oracle import oracle
+    op = oracle.Op("dwf", DIMS, u, ls=LS, mass=MF, m5=M5)
+    t0 = time.perf_counter()
+    op.mdagm(src)
+    per = time.perf_counter() - t0
+    return {"value": 1.0 / (per * iters), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one MatPcDagMatPc of the C oracle ({per:.2f} s); extrapolated with {iters} iterations"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import refrun
+    iters = FP64_ITERS
+    u, srcs = make_inputs(1)
+    cores = os.cpu_count() or 1
+    if not refrun.available():
+        kind = "port"
+    else:
+        kind = "reference"
+    if iters is None:
+        print(json.dumps({"impl": "reference", "unavailable": "FP64 iteration count of the workload not recorded"}))
+        return
+    times = []
+    for k in range(args.warmup + args.steps):
+        if kind == "reference":
+            wall, ts = _ref_mdagm_seconds(u, srcs[0], cores)
+        else:
+            from oracle import oracle
+            op = oracle.Op("dwf", DIMS, u, ls=LS, mass=MF, m5=M5)
+            t0 = time.perf_counter()
+            op.mdagm(srcs[0])
+            wall = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(wall)
+    nper = cores if kind == "reference" else 1
+    step = statistics.mean(times)
+    rate = nper / (step * iters)
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step * 1000 * iters / nper, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism="cpu"), "impl": "reference",
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nper, "kind": kind,
+                             "sample": f"per step: {nper} concurrent MatPcDagMatPc at 16^3x32x16 "
+                                       f"({step:.2f} s wall); extrapolated with {iters} CG iterations"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

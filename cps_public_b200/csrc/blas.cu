@@ -65,19 +65,19 @@ cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, long n, cuda
   if (prec == P64) pack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
   else if (prec == P32) pack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
   else pack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  return cudaGetLastError();
+  return launched();
 }
 
 cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, long n, cudaStream_t st) {
   if (prec == P64) unpack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
   else if (prec == P32) unpack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
   else unpack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  return cudaGetLastError();
+  return launched();
 }
 
 cudaError_t launch_convert(int pd, SpinorPtr dst, int ps, SpinorPtr src, long n, cudaStream_t st) {
   const int g = flat_grid(n);
-#define CV(A, B) if (pd == A && ps == B) { convert_kernel<A, B><<<g, 256, 0, st>>>(dst, src, n); return cudaGetLastError(); }
+#define CV(A, B) if (pd == A && ps == B) { convert_kernel<A, B><<<g, 256, 0, st>>>(dst, src, n); return launched(); }
   CV(P64, P64) CV(P64, P32) CV(P64, P16) CV(P32, P64) CV(P32, P32) CV(P32, P16) CV(P16, P64) CV(P16, P32) CV(P16, P16)
 #undef CV
   return cudaErrorInvalidValue;
@@ -114,9 +114,8 @@ __global__ void gauge_pack_kernel(void *dst, const double *u, int lx, int ly, in
       uint2 *d = (uint2 *)dst;
       for (int k = 0; k < 3; k++) {
         uint2 v;
-        __half2 *h = (__half2 *)&v;
-        h[0] = __floats2half2_rn((float)m[4 * k], (float)m[4 * k + 1]);
-        h[1] = __floats2half2_rn((float)m[4 * k + 2], (float)m[4 * k + 3]);
+        v.x = enc16x2((float)m[4 * k], (float)m[4 * k + 1], 32767.0f);
+        v.y = enc16x2((float)m[4 * k + 2], (float)m[4 * k + 3], 32767.0f);
         d[((long)(par * 4 + mu) * 3 + k) * n4cb + cbi] = v;
       }
     }
@@ -129,7 +128,7 @@ cudaError_t launch_gauge_pack(int prec, void *dst, const double *u, const int di
   if (prec == P64) gauge_pack_kernel<P64><<<g, 256, 0, st>>>(dst, u, dims[0], dims[1], dims[2], dims[3], bc_t);
   else if (prec == P32) gauge_pack_kernel<P32><<<g, 256, 0, st>>>(dst, u, dims[0], dims[1], dims[2], dims[3], bc_t);
   else gauge_pack_kernel<P16><<<g, 256, 0, st>>>(dst, u, dims[0], dims[1], dims[2], dims[3], bc_t);
-  return cudaGetLastError();
+  return launched();
 }
 
 // Max deviation of row 2 from conj(row0 x row1) over all links with the
@@ -153,7 +152,7 @@ __global__ void unitarity_kernel(const double *u, long nlinks, int lx, int ly, i
 cudaError_t launch_unitarity(const double *u, long nlinks, const int dims[4], int bc_t, unsigned long long *out,
                              cudaStream_t st) {
   unitarity_kernel<<<flat_grid(nlinks), 256, 0, st>>>(u, nlinks, dims[0], dims[1], dims[2], dims[3], bc_t, out);
-  return cudaGetLastError();
+  return launched();
 }
 
 // ---------------------------------------------------------------- CG updates
@@ -253,7 +252,7 @@ cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr A
   if (prec == P64) cg_r_update_kernel<P64, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
   else if (prec == P32) cg_r_update_kernel<P32, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
   else cg_r_update_kernel<P16, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
-  return cudaGetLastError();
+  return launched();
 }
 
 cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, SpinorPtr p, SpinorPtr r, CgState *S,
@@ -263,7 +262,7 @@ cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, Sp
   else if (px == P32 && prec == P32) cg_xp_update_kernel<P32, P32, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, ticket);
   else if (px == P32 && prec == P16) cg_xp_update_kernel<P32, P16, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, ticket);
   else return cudaErrorInvalidValue;
-  return cudaGetLastError();
+  return launched();
 }
 
 // ---------------------------------------------------------------- axpby
@@ -320,7 +319,7 @@ cudaError_t launch_axpby(int po, SpinorPtr out, int px, SpinorPtr X, int py, Spi
 #define AX(A, B, C)                                                                               \
   if (po == A && px == B && py == C) {                                                          \
     axpby_kernel<A, B, C, 256><<<grid, 256, 0, st>>>(g, out, X, Y, sc, skip, red, norm);        \
-    return cudaGetLastError();                                                                  \
+    return launched();                                                                  \
   }
   AX(P64, P64, P64) AX(P64, P64, P32) AX(P64, P32, P64) AX(P64, P16, P64) AX(P64, P64, P16)
   AX(P32, P32, P32) AX(P32, P64, P32) AX(P32, P32, P64) AX(P32, P16, P32) AX(P32, P32, P16)
@@ -358,7 +357,7 @@ cudaError_t launch_redot(int prec, const Geom &g, SpinorPtr X, SpinorPtr Y, Redu
   if (prec == P64) redot_kernel<P64, 256><<<grid, 256, 0, st>>>(g, X, Y, red);
   else if (prec == P32) redot_kernel<P32, 256><<<grid, 256, 0, st>>>(g, X, Y, red);
   else redot_kernel<P16, 256><<<grid, 256, 0, st>>>(g, X, Y, red);
-  return cudaGetLastError();
+  return launched();
 }
 
 }  // namespace cpsb

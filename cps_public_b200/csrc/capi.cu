@@ -381,6 +381,12 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
   return CPSB_ERR_UNSUPPORTED;
 }
 
+int cpsb_kernel_launches(unsigned long long *count) {
+  if (!count) return CPSB_ERR_ARG;
+  *count = launch_count();
+  return CPSB_OK;
+}
+
 int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
                       double *bytes) {
   return guarded([&] {
@@ -392,7 +398,7 @@ int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, i
     Field fi(precision, op.nsites()), fo(precision, op.nsites());
     CK(cudaMemsetAsync(fi.data.p, 0, fi.data.bytes, st));
     if (fi.norm.p) CK(cudaMemsetAsync(fi.norm.p, 0, fi.norm.bytes, st));
-    for (int i = 0; i < 3; i++) op.hop(fo, fi, 1, 0, 1.0, nullptr, nullptr, nullptr, st);
+    for (int i = 0; i < 3; i++) op.hop(fo, fi, 1, 0, 1.0, nullptr, nullptr, nullptr, st);  // tunes, warms
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

@@ -8,13 +8,16 @@
 //    Nrhs x Ls slices): chunk k of site i lives at base[k*N + i].
 //      FP64: 12 chunks of double2 = one complex component (spin k/3, colour k%3)
 //      FP32:  6 chunks of float4  = complex components 2k, 2k+1
-//      FP16:  3 chunks of 8 halves (uint4) = components 4k..4k+3, plus one
-//             float per site (the site's max-abs) in a separate norm array.
+//      16-bit: 3 chunks of 8 fixed-point values (uint4) = components 4k..4k+3,
+//             plus one float per site (max-abs / 32767, the quantum) in a
+//             separate norm array.  A value v is stored as the biased integer
+//             rint(v/quantum) + 32768 (15 bits of mantissa against IEEE fp16's 11).
 //  * gauge field, one 4-D checkerboard index x per parity p and direction mu:
 //      FP64 (18 reals): 9 double2 chunks, chunk k = U[k/3][k%3], at
 //                       data[((p*4+mu)*9 + k)*n4cb + x]
 //      FP32 (recon-12): 3 float4 chunks holding rows 0 and 1
-//      FP16 (recon-12): 3 uint2 chunks (4 halves each) holding rows 0 and 1
+//      16-bit (recon-12): 3 uint2 chunks (4 fixed-point values, quantum 1/32767)
+//                         holding rows 0 and 1
 //    Reconstructed links omit the antiperiodic-time sign, which the kernel
 //    applies to the hop (bc_t_sign) at the t boundary.
 //
@@ -68,12 +71,15 @@ struct Coord { int x, y, z, t; };
 // 4-D coordinates of checkerboard index idx of parity par.
 __device__ __forceinline__ Coord decode(const Geom &g, int idx, int par) {
   Coord c;
-  int xh = idx % g.lxh;
-  int r = idx / g.lxh;
-  c.y = r % g.ly; r /= g.ly;
-  c.z = r % g.lz;
-  c.t = r / g.lz;
-  c.x = 2 * xh + ((c.y + c.z + c.t + par) & 1);
+  const unsigned u = (unsigned)idx;
+  const unsigned r0 = u / (unsigned)g.lxh;
+  const unsigned xh = u - r0 * (unsigned)g.lxh;
+  const unsigned r1 = r0 / (unsigned)g.ly;
+  c.y = (int)(r0 - r1 * (unsigned)g.ly);
+  const unsigned r2 = r1 / (unsigned)g.lz;
+  c.z = (int)(r1 - r2 * (unsigned)g.lz);
+  c.t = (int)r2;
+  c.x = 2 * (int)xh + ((c.y + c.z + c.t + par) & 1);
   return c;
 }
 __device__ __forceinline__ int cbindex(const Geom &g, int x, int y, int z, int t) {
@@ -93,6 +99,22 @@ template <int P> struct PrecTraits;
 template <> struct PrecTraits<P64> { typedef double real; };
 template <> struct PrecTraits<P32> { typedef float real; };
 template <> struct PrecTraits<P16> { typedef float real; };
+
+// 16-bit fixed point.  The biased integer u in one half of a 32-bit word is
+// turned into the float 2^23 + u by placing its bits under the exponent byte
+// 0x4B, then 2^23 + 32768 is subtracted: two exact instructions per value.
+__device__ __forceinline__ float dec16(unsigned w, int hi) {
+  const unsigned bits = __byte_perm(w, 0x4B00u, hi ? 0x5432u : 0x5410u);
+  return __int_as_float((int)bits) - 8421376.0f;
+}
+__device__ __forceinline__ unsigned q16(float v, float scale) {
+  int q = __float2int_rn(v * scale);
+  q = max(-32767, min(32767, q));
+  return (unsigned)(q + 32768);
+}
+__device__ __forceinline__ unsigned enc16x2(float a, float b, float scale) {
+  return q16(a, scale) | (q16(b, scale) << 16);
+}
 
 template <int P>
 __device__ __forceinline__ Spinor<typename PrecTraits<P>::real> load_spinor(const SpinorPtr &f, long i);
@@ -131,12 +153,11 @@ __device__ __forceinline__ Spinor<float> load_spinor<P16>(const SpinorPtr &f, lo
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     uint4 v = __ldg(b + k * f.stride + i);
-    const __half2 *h = (const __half2 *)&v;
+    const unsigned w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      float2 w = __half22float2(h[j]);
       int c = 4 * k + j;
-      s.c[c / 3][c % 3] = mk(w.x * nrm, w.y * nrm);
+      s.c[c / 3][c % 3] = mk(dec16(w[j], 0) * nrm, dec16(w[j], 1) * nrm);
     }
   }
   return s;
@@ -170,24 +191,23 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf(s.c[a][c].re), fabsf(s.c[a][c].im)));
-  const float inv = m > 0.f ? 1.0f / m : 0.f;
-  f.norm[i] = m;
+  const float scale = m > 0.f ? 32767.0f / m : 0.f;
+  f.norm[i] = m * (1.0f / 32767.0f);
   uint4 *b = (uint4 *)f.data;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    uint4 v;
-    __half2 *h = (__half2 *)&v;
+    unsigned w[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       int c = 4 * k + j;
-      h[j] = __floats2half2_rn(s.c[c / 3][c % 3].re * inv, s.c[c / 3][c % 3].im * inv);
+      w[j] = enc16x2(s.c[c / 3][c % 3].re, s.c[c / 3][c % 3].im, scale);
     }
-    b[k * f.stride + i] = v;
+    b[k * f.stride + i] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
 // Storage rounding of a spinor: what load_spinor<P> would return after
-// store_spinor<P> (identity except for FP16, whose values are scaled halves).
+// store_spinor<P> (identity except for 16-bit storage).
 template <int P, typename T> __device__ __forceinline__ Spinor<T> rounded(const Spinor<T> &s) {
   if (P != P16) return s;
   float m = 0.f;
@@ -195,14 +215,15 @@ template <int P, typename T> __device__ __forceinline__ Spinor<T> rounded(const 
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf((float)s.c[a][c].re), fabsf((float)s.c[a][c].im)));
-  const float inv = m > 0.f ? 1.0f / m : 0.f;
+  const float scale = m > 0.f ? 32767.0f / m : 0.f;
+  const float nq = m * (1.0f / 32767.0f);
   Spinor<T> o;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      float2 w = __half22float2(__floats2half2_rn((float)s.c[a][c].re * inv, (float)s.c[a][c].im * inv));
-      o.c[a][c] = mk((T)(w.x * m), (T)(w.y * m));
+      const unsigned w = enc16x2((float)s.c[a][c].re, (float)s.c[a][c].im, scale);
+      o.c[a][c] = mk((T)(dec16(w, 0) * nq), (T)(dec16(w, 1) * nq));
     }
   return o;
 }
@@ -252,15 +273,14 @@ __device__ __forceinline__ Link<float> load_link<P32>(const GaugePtr &g, int par
 template <>
 __device__ __forceinline__ Link<float> load_link<P16>(const GaugePtr &g, int par, int mu, int x) {
   const uint2 *b = (const uint2 *)g.data + (long)((par * 4 + mu) * 3) * g.n4cb + x;
+  const float q = 1.0f / 32767.0f;
   Link<float> l;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     uint2 v = __ldg(b + k * g.n4cb);
-    const __half2 *h = (const __half2 *)&v;
-    float2 w0 = __half22float2(h[0]), w1 = __half22float2(h[1]);
     int e0 = 2 * k, e1 = 2 * k + 1;
-    l.u[e0 / 3][e0 % 3] = mk(w0.x, w0.y);
-    l.u[e1 / 3][e1 % 3] = mk(w1.x, w1.y);
+    l.u[e0 / 3][e0 % 3] = mk(dec16(v.x, 0) * q, dec16(v.x, 1) * q);
+    l.u[e1 / 3][e1 % 3] = mk(dec16(v.y, 0) * q, dec16(v.y, 1) * q);
   }
   reconstruct_row2(l);
   return l;

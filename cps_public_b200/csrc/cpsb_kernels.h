@@ -26,12 +26,27 @@ struct DslashArgs {
   double bc_t_sign;       // -1: reconstructed links need the antiperiodic sign at the t boundary
   Reduce red;             // |out|^2 per RHS when requested
   const int *skip;        // per-RHS: nonzero skips that RHS (device memory), may be null
+  int sl;                 // slice lanes per block (set by the launcher)
 };
+
+// Kernel-launch accounting (cpsb_kernel_launches): every launcher calls
+// count_launch(); launches recorded into a CUDA graph are counted when the
+// graph is replayed instead.
+void count_launch(unsigned long long n = 1);
+void set_capturing(bool on);
+unsigned long long launch_count();
+// Every launcher returns through this: counts the launch, reports launch errors.
+inline cudaError_t launched() {
+  count_launch();
+  return cudaGetLastError();
+}
 
 // Grid: blockIdx.y = right-hand side, blockIdx.x strides over the sites of one RHS.
 int grid_blocks(long sites_per_rhs, int nt);
 
-cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int nt, cudaStream_t st);
+// variant: launch shape 0..NUM_DSLASH_VARIANTS-1 (see dslash_impl.cuh), chosen by the autotuner.
+constexpr int NUM_DSLASH_VARIANTS = 6;
+cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st);
 
 // ---------------------------------------------------------------- BLAS
 // All vectors share one Geom (nsites sites, nrhs right-hand sides).  Scalars

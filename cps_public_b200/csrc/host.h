@@ -88,7 +88,6 @@ struct Operator {
   M5Coef m5c[2];           // Mobius M5^-1 coefficient sets (dag 0, dag 1)
   Field t1, t2, t3;
   RedSlot red_inner;
-  int nt = 128;
 
   Operator(Gauge *G, const cpsb_dirac_params &p, int prec, int nrhs);
   long nsites() const { return geom.nsites; }
@@ -121,6 +120,7 @@ struct CgSolver {
   DevBuf tick;                        // ticket for the xp update
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;
+  unsigned long long graph_nodes = 0;
   std::mutex busy;
 
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
@@ -133,6 +133,8 @@ struct CgSolver {
   void run_batches(int batch, cudaStream_t st, const bool *done, bool any);
   void true_residual(double *rr_out, const double *bnorm, cudaStream_t st);
 };
+
+int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_t st);
 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
 

@@ -161,7 +161,7 @@ static cudaError_t m5_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr
 #define M5L(D, XP, NR)                                                                              \
   if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
     m5_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
-    return cudaGetLastError();                                                                      \
+    return launched();                                                                      \
   }
   M5L(0, false, false) M5L(0, true, false) M5L(0, true, true) M5L(0, false, true)
   M5L(1, false, false) M5L(1, true, false) M5L(1, true, true) M5L(1, false, true)

@@ -16,6 +16,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "host.h"
 
 namespace cpsb {
@@ -26,6 +28,14 @@ void check_cuda(cudaError_t e, const char *what) {
   cudaGetLastError();  // clear a non-sticky error
   throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
 }
+
+static std::atomic<unsigned long long> g_launches{0};
+static thread_local bool t_capturing = false;
+void count_launch(unsigned long long n) {
+  if (!t_capturing) g_launches += n;
+}
+void set_capturing(bool on) { t_capturing = on; }
+unsigned long long launch_count() { return g_launches.load(); }
 
 Context &ctx() {
   static Context c;
@@ -171,7 +181,6 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   }
   t1.create(prec, geom.nsites);
   t2.create(prec, geom.nsites);
-  nt = prec == P64 ? 128 : 128;
 }
 
 double Operator::hop_bytes() const {
@@ -199,7 +208,8 @@ void Operator::hop(const Field &out, const Field &in, int cb, int dag, double a,
   A.bc_t_sign = (prec != P64 && G->bc_t) ? -1.0 : 1.0;
   if (red) A.red = *red;
   A.skip = skip;
-  CK(launch_dslash(prec, A, x != nullptr, red != nullptr, nt, st));
+  const int v = tuned_variant(A, prec, x != nullptr, red != nullptr, st);
+  CK(launch_dslash(prec, A, x != nullptr, red != nullptr, v, st));
 }
 
 void Operator::dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st) {

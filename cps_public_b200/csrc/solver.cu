@@ -86,21 +86,35 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
       cudaGraphExecDestroy(graph);
       graph = nullptr;
     }
+    // One uncaptured application tunes the sloppy operator's launch shapes.
+    {
+      CgState *S = (CgState *)state.p;
+      Operator &op = opS ? *opS : *op64;
+      Reduce rd = red_d.r(S->d);
+      op.mdagm(ApS, pS, &rd, S->halt, st);
+    }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    set_capturing(true);
     try {
       launch_batch(batch, st);
     } catch (...) {
+      set_capturing(false);
       cudaStreamEndCapture(st, &g);
       throw;
     }
+    set_capturing(false);
     CK(cudaStreamEndCapture(st, &g));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    graph_nodes = nn;
     CK(cudaGraphInstantiate(&graph, g, 0));
     cudaGraphDestroy(g);
     graph_batch = batch;
   }
   for (;;) {
     CK(cudaGraphLaunch(graph, st));
+    count_launch(graph_nodes);
     CK(cudaMemcpyAsync(hstate, state.p, sizeof(CgState), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     bool all = true, one = false;

@@ -1,0 +1,51 @@
+"""Dslash bandwidth benchmark: python -m cps_public_b200.dslash_bench [--prec f16,f32,f64]
+
+Times the 5-D Shamir DWF hop (one checkerboard, dag 0) on the 16^3x32, Ls=16
+workload with CUDA events over many launches and reports algorithmic GB/s
+(spinor in + out + links per application) against the measured HBM copy peak.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from . import DiracOp, F16, F32, F64, Gauge, _lib, fields, init
+
+PRECS = {"f16": F16, "f32": F32, "f64": F64}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--prec", default="f16,f32,f64")
+    ap.add_argument("--dims", default="16,16,16,32")
+    ap.add_argument("--ls", type=int, default=16)
+    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=50)
+    ap.add_argument("--action", default="dwf")
+    a = ap.parse_args()
+    dims = tuple(int(x) for x in a.dims.split(","))
+    init(0)
+    g = Gauge(fields.random_gauge(dims, 0.2, 7), dims)
+    op = DiracOp(g, a.action, mass=0.01, ls=a.ls, m5=1.8)
+    peak = 6650.0
+    try:
+        peak = float(json.load(open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                                 "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        pass
+    lib = _lib.load()
+    for name in a.prec.split(","):
+        ms, by = C.c_double(), C.c_double()
+        _lib.check(lib.cpsb_bench_dslash(g.h, C.byref(op.p), PRECS[name], a.nrhs, a.reps, C.byref(ms),
+                                         C.byref(by)), "cpsb_bench_dslash")
+        gbs = by.value / (ms.value * 1e-3) / 1e9
+        print(json.dumps({"prec": name, "dims": dims, "ls": a.ls, "nrhs": a.nrhs, "ms": ms.value,
+                          "bytes": by.value, "gbs": gbs, "frac_of_peak": gbs / peak}))
+
+
+if __name__ == "__main__":
+    main()

@@ -152,6 +152,11 @@ int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg
 int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
                    void *stream);
 
+/* Kernels this library has launched in the process (a graph replay counts each
+ * of its kernel nodes): the device analogue of CPS's static flop counter
+ * DiracOp::CGflops (include/util/dirac_op.h:74). */
+int cpsb_kernel_launches(unsigned long long *count);
+
 /* Times `reps` applications of the device Dslash of the given precision on
  * internally resident data (one checkerboard, dag 0); reports the mean kernel
  * time in ms measured with CUDA events on the launching stream, and the bytes
