@@ -164,6 +164,22 @@ int cpsb_kernel_launches(unsigned long long *count);
 int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
                       double *bytes);
 
+/* Real parts of nvec dot products <x_v, y_v> of device vectors of n doubles
+ * each (vector v starts at x + v*n), written to result[0..nvec) in device
+ * memory, in a fixed (reproducible) summation order.  It allocates nothing:
+ * for callers that cannot call cudaMalloc -- code recording a CUDA graph
+ * (allocation is not allowed on a capturing stream), loops that run inside a
+ * pre-reserved HBM arena, codes that must avoid cudaFree's device-wide sync.
+ * Its reduction scratch is an 80 KiB file-scope __device__ array that every
+ * GPU using the library keeps until exit; the first call on a device looks up
+ * that array's address (make it before any stream capture).  Calls whose work
+ * overlaps on the GPU share the array and race: serialise them on one stream.
+ * Limits: 1 <= nvec <= 16, n >= 1; larger nvec is rejected with CPSB_ERR_ARG.
+ * Uses the current CUDA device; needs no cpsb_init.  No counterpart in the
+ * reference: it is the device analogue of Vector::ReDotProductGlbSum
+ * (include/util/vector.h:955) with no allocation of its own. */
+int cpsb_redot_noalloc(const double *x, const double *y, long n, int nvec, double *result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
