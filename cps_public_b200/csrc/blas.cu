@@ -159,19 +159,27 @@ cudaError_t launch_unitarity(const double *u, long nlinks, const int dims[4], in
 // r = r - alpha*Ap (alpha = rr/d from the device state), |r|^2 per RHS; the last
 // block advances the recurrence scalars and decides whether this RHS halts.
 template <int P, int NT>
-__global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, SpinorPtr Ap, CgState *S, Reduce red) {
+__global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, SpinorPtr Ap, SpinorPtr p, CgState *S, Reduce red) {
   typedef typename PrecTraits<P>::real T;
   __shared__ double sh[NT / 32];
   const int rhs = blockIdx.y;
   const long per = (long)g.n4cb * g.ls;
   double acc = 0;
   if (!S->halt[rhs]) {
-    const double alpha = S->rr[rhs] / S->d[rhs];
-    const T a = (T)alpha;
+    const double sigma = S->shift;
+    const double alpha = S->rr[rhs] / (S->d[rhs] + sigma * S->pp[rhs]);
+    const T a = (T)alpha, ts = (T)sigma;
     for (long j = (long)blockIdx.x * NT + threadIdx.x; j < per; j += (long)gridDim.x * NT) {
       const long i = rhs * per + j;
       Spinor<T> rv = load_spinor<P>(r, i);
       Spinor<T> av = load_spinor<P>(Ap, i);
+      if (sigma != 0.0) {
+        const Spinor<T> pv = load_spinor<P>(p, i);
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) av.c[s][c] = av.c[s][c] + cscale(ts, pv.c[s][c]);
+      }
 #pragma unroll
       for (int s = 0; s < 4; s++)
 #pragma unroll
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, Sp
       double c = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
       if (threadIdx.x == 0 && !S->halt[q]) {
         const double rprev = S->rr[q];
-        const double d = S->d[q];
+        const double d = S->d[q] + S->shift * S->pp[q];
         S->alpha[q] = rprev / d;
         S->rr_prev[q] = rprev;
         S->rr[q] = c;
@@ -211,11 +219,14 @@ __global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, Sp
 // x = x + alpha p ; p = r + beta p (skipped in the iteration that halts).
 template <int PX, int P, int NT>
 __global__ void __launch_bounds__(NT) cg_xp_update_kernel(Geom g, SpinorPtr x, SpinorPtr p, SpinorPtr r, CgState *S,
-                                                          unsigned *ticket) {
+                                                          Reduce red) {
   typedef typename PrecTraits<P>::real T;
   typedef typename PrecTraits<PX>::real TX;
+  __shared__ double sh[NT / 32];
   const int rhs = blockIdx.y;
   const long per = (long)g.n4cb * g.ls;
+  const bool want_pp = S->shift != 0.0;
+  double acc = 0;
   if (!S->halt_done[rhs]) {
     const double alpha = S->alpha[rhs], beta = S->beta[rhs];
     const bool upd_p = !S->halt[rhs];
@@ -239,28 +250,39 @@ __global__ void __launch_bounds__(NT) cg_xp_update_kernel(Geom g, SpinorPtr x, S
 #pragma unroll
           for (int c = 0; c < 3; c++) pv.c[s][c] = cscale(b, pv.c[s][c]) + rv.c[s][c];
         store_spinor<P>(p, i, pv);
+        if (want_pp) acc += norm2(rounded<P>(pv));
       }
     }
   }
-  if (last_block(ticket, gridDim.x * gridDim.y) && threadIdx.x == 0) {
-    for (int q = 0; q < g.nrhs; q++) S->halt_done[q] = S->halt[q];
+  const double bsum = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bsum;
+  if (last_block(red.ticket, gridDim.x * gridDim.y)) {
+    for (int q = 0; q < g.nrhs; q++) {
+      const double t = want_pp ? ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh) : 0.0;
+      if (threadIdx.x == 0) {
+        if (want_pp && !S->halt_done[q] && !S->halt[q]) S->pp[q] = t;
+        S->halt_done[q] = S->halt[q];
+      }
+      __syncthreads();
+    }
   }
 }
 
-cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr Ap, CgState *S, Reduce red, cudaStream_t st) {
+cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr Ap, SpinorPtr p, CgState *S, Reduce red,
+                               cudaStream_t st) {
   dim3 grid(grid_blocks((long)g.n4cb * g.ls, 256), g.nrhs);
-  if (prec == P64) cg_r_update_kernel<P64, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
-  else if (prec == P32) cg_r_update_kernel<P32, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
-  else cg_r_update_kernel<P16, 256><<<grid, 256, 0, st>>>(g, r, Ap, S, red);
+  if (prec == P64) cg_r_update_kernel<P64, 256><<<grid, 256, 0, st>>>(g, r, Ap, p, S, red);
+  else if (prec == P32) cg_r_update_kernel<P32, 256><<<grid, 256, 0, st>>>(g, r, Ap, p, S, red);
+  else cg_r_update_kernel<P16, 256><<<grid, 256, 0, st>>>(g, r, Ap, p, S, red);
   return launched();
 }
 
 cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, SpinorPtr p, SpinorPtr r, CgState *S,
-                                unsigned *ticket, cudaStream_t st) {
+                                Reduce red, cudaStream_t st) {
   dim3 grid(grid_blocks((long)g.n4cb * g.ls, 256), g.nrhs);
-  if (px == P64 && prec == P64) cg_xp_update_kernel<P64, P64, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, ticket);
-  else if (px == P32 && prec == P32) cg_xp_update_kernel<P32, P32, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, ticket);
-  else if (px == P32 && prec == P16) cg_xp_update_kernel<P32, P16, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, ticket);
+  if (px == P64 && prec == P64) cg_xp_update_kernel<P64, P64, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, red);
+  else if (px == P32 && prec == P32) cg_xp_update_kernel<P32, P32, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, red);
+  else if (px == P32 && prec == P16) cg_xp_update_kernel<P32, P16, 256><<<grid, 256, 0, st>>>(g, x, p, r, S, red);
   else return cudaErrorInvalidValue;
   return launched();
 }

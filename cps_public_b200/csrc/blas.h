@@ -12,10 +12,10 @@ struct Scal2 {
 
 cudaError_t launch_unitarity(const double *u, long nlinks, const int dims[4], int bc_t, unsigned long long *out,
                              cudaStream_t st);
-cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr Ap, CgState *S, Reduce red,
+cudaError_t launch_cg_r_update(int prec, const Geom &g, SpinorPtr r, SpinorPtr Ap, SpinorPtr p, CgState *S, Reduce red,
                                cudaStream_t st);
 cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, SpinorPtr p, SpinorPtr r, CgState *S,
-                                unsigned *ticket, cudaStream_t st);
+                                Reduce red, cudaStream_t st);
 cudaError_t launch_axpby(int po, SpinorPtr out, int px, SpinorPtr X, int py, SpinorPtr Y, const Geom &g, Scal2 sc,
                          const int *skip, Reduce red, int norm, cudaStream_t st);
 cudaError_t launch_redot(int prec, const Geom &g, SpinorPtr X, SpinorPtr Y, Reduce red, cudaStream_t st);

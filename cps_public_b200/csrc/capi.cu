@@ -375,10 +375,32 @@ int cpsb_invcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *
 int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double **x, const double *b,
                 const double *shift, int nshift, double *rsd, int type, const double *alpha,
                 cpsb_solve_result *res) {
-  (void)h; (void)p; (void)a; (void)x; (void)b; (void)shift; (void)nshift; (void)rsd; (void)type; (void)alpha;
-  (void)res;
-  g_last_error = "multishift CG not built yet";
-  return CPSB_ERR_UNSUPPORTED;
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (!x || !b || !shift || !rsd || nshift < 1 || nshift > 32) throw Error{CPSB_ERR_ARG, "bad multishift arguments"};
+    if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE are implemented"};
+    if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
+    const int nvec = type == CPSB_SINGLE ? 1 : nshift;
+    for (int i = 0; i < nvec; i++)
+      if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
+    cudaStream_t st = ctx().stream;
+    const long n = cb_sites(h, p);
+    Field chi(P64, n);
+    upload(chi, &b, 1, n, st);
+    std::vector<Field> xs(nvec);
+    for (int i = 0; i < nvec; i++) {
+      xs[i].create(P64, n);
+      CK(cudaMemsetAsync(xs[i].data.p, 0, xs[i].data.bytes, st));
+    }
+    cpsb_solve_result r;
+    memset(&r, 0, sizeof(r));
+    const int rc = multishift(&h->g, *p, *a, chi, xs, shift, nshift, rsd, type, alpha, &r, st);
+    for (int i = 0; i < nvec; i++) download(&x[i], 1, n, xs[i], st);
+    if (res) *res = r;
+    return rc;
+  });
 }
 
 int cpsb_kernel_launches(unsigned long long *count) {

@@ -20,8 +20,9 @@ struct CgState {
   double beta[MAX_RHS];
   double stp[MAX_RHS];       // stop when rr <= stp  (stop_rsd^2 |b|^2)
   double maxr[MAX_RHS];      // largest |r| since the last reliable update
+  double pp[MAX_RHS];        // |p|^2 (needed for the shifted operator A + sigma)
   double delta;              // reliable-update threshold (0: pure CG)
-  double shift;              // constant shift sigma of (A + sigma)
+  double shift;              // constant shift sigma of (A + sigma): <p,(A+sigma)p> = d + sigma pp
   int halt[MAX_RHS];         // set by the r-update: this RHS pauses for the host
   int halt_done[MAX_RHS];    // set after the x/p update of the halting iteration
   int reason[MAX_RHS];

@@ -116,8 +116,8 @@ struct CgSolver {
   DevBuf state;                       // CgState
   CgState *hstate = nullptr;          // pinned mirror
   DevBuf scal;                        // misc per-RHS scalars
-  RedSlot red_d, red_r, red_misc;
-  DevBuf tick;                        // ticket for the xp update
+  RedSlot red_d, red_r, red_p, red_misc;
+  double shift = 0;                   // sigma of the solve in progress
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;
   unsigned long long graph_nodes = 0;
@@ -126,7 +126,7 @@ struct CgSolver {
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
   ~CgSolver();
   // Solves with x64 (initial guess) and b64 already packed; fills res[nrhs].
-  int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st);
+  int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma = 0.0);
 
  private:
   void launch_batch(int k, cudaStream_t st);

@@ -46,8 +46,6 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
   state.alloc(sizeof(CgState));
   CK(cudaMallocHost((void **)&hstate, sizeof(CgState)));
   scal.alloc(sizeof(double) * MAX_RHS * 8);
-  tick.alloc(256);
-  CK(cudaMemset(tick.p, 0, 256));
 }
 
 CgSolver::~CgSolver() {
@@ -73,10 +71,11 @@ void CgSolver::launch_batch(int k, cudaStream_t st) {
   Field &xx = opS ? xS : x64;
   Reduce rd = red_d.r(S->d);
   Reduce rr = red_r.r(nullptr);
+  Reduce rp = red_p.r(nullptr);
   for (int j = 0; j < k; j++) {
     op.mdagm(ApS, pS, &rd, S->halt, st);
-    CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), S, rr, st));
-    CK(launch_cg_xp_update(px, op.prec, op.geom, xx.ptr(), pS.ptr(), rS.ptr(), S, (unsigned *)tick.p, st));
+    CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), pS.ptr(), S, rr, st));
+    CK(launch_cg_xp_update(px, op.prec, op.geom, xx.ptr(), pS.ptr(), rS.ptr(), S, rp, st));
   }
 }
 
@@ -126,20 +125,27 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
   }
 }
 
-// rr_out[q] = |b - A x64|^2 (FP64), leaves r64 = b - A x64.
+// rr_out[q] = |b - (A + shift) x64|^2 (FP64), leaves r64 = b - (A + shift) x64.
 void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t st) {
   (void)bnorm;
   double *dres = (double *)scal.p;
   op64->mdagm(Ap64, x64, nullptr, nullptr, st);
   Reduce rm = red_misc.r(dres);
+  if (shift != 0.0) {
+    Reduce none;
+    memset(&none, 0, sizeof(none));
+    CK(launch_axpby(P64, Ap64.ptr(), P64, Ap64.ptr(), P64, x64.ptr(), op64->geom, sc2(nrhs, 1.0, shift), nullptr,
+                    none, 0, st));
+  }
   CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, Ap64.ptr(), op64->geom, sc2(nrhs, 1.0, -1.0), nullptr, rm, 1,
                   st));
   CK(cudaMemcpyAsync(rr_out, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
 }
 
-int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st) {
+int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma) {
   auto t0 = std::chrono::steady_clock::now();
+  shift = sigma;
   const Geom &gg = op64->geom;
   double bnorm[MAX_RHS], rr[MAX_RHS];
   double *dres = (double *)scal.p;
@@ -156,12 +162,14 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   memset(&hs, 0, sizeof(hs));
   const double delta = sloppy == P64 ? 0.0 : (a.reliable_delta > 0 ? a.reliable_delta : 0.1);
   hs.delta = delta;
+  hs.shift = shift;
   hs.max_iter = a.max_num_iter;
   hs.nrhs = nrhs;
   int nupd[MAX_RHS] = {0};
   bool done[MAX_RHS];
   for (int q = 0; q < nrhs; q++) {
     hs.rr[q] = rr[q];
+    hs.pp[q] = rr[q];  // p = r
     hs.stp[q] = bnorm[q] * a.stop_rsd * a.stop_rsd;
     hs.maxr[q] = sqrt(rr[q]);
     done[q] = (rr[q] <= hs.stp[q]) || (a.max_num_iter - 1 <= 0);
@@ -236,7 +244,15 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
     }
     CK(cudaMemcpyAsync(dskip, refresh_skip, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, st));
     CK(launch_axpby(sloppy, rS.ptr(), P64, r64.ptr(), P64, SpinorPtr{}, gg, sc2(nrhs, 1.0, 0.0), dskip, none, 0, st));
-    CK(launch_axpby(sloppy, pS.ptr(), sloppy, rS.ptr(), sloppy, pS.ptr(), gg, beta, dskip, none, 0, st));
+    {
+      Reduce rpp = red_misc.r((double *)scal.p + MAX_RHS);
+      CK(launch_axpby(sloppy, pS.ptr(), sloppy, rS.ptr(), sloppy, pS.ptr(), gg, beta, dskip, rpp, 1, st));
+      double pp_h[MAX_RHS];
+      CK(cudaMemcpyAsync(pp_h, (double *)scal.p + MAX_RHS, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      for (int q = 0; q < nrhs; q++)
+        if (!refresh_skip[q]) h.pp[q] = pp_h[q];
+    }
     // The device was idle since the state was read, so h is current for the RHS
     // that kept running and updated for the others.
     CK(cudaMemcpyAsync(state.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
