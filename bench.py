@@ -48,7 +48,7 @@ UNIT = "solves/s"
 # the FP64 solver, which runs CPS's recurrence (its iteration counts match the
 # compiled reference within one on every golden case).  The CPU arm uses it to
 # turn one timed MatPcDagMatPc into solves/s.
-FP64_ITERS = None
+FP64_ITERS = 348
 WORKLOAD = {"workload": "shamir_dwf_eo_cg_16x16x16x32_ls16", "lattice": "16^3x32", "ls": LS, "m5": M5, "mf": MF,
             "link_eps": EPS, "stop_true_rsd": STOP, "source": "gaussian odd checkerboard", "reliable_delta": 0.1,
             "l2": "inputs larger than L2 (201 MB FP64 / 52 MB FP16 per vector, 75 MB FP64 links)"}
