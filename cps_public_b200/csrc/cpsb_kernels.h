@@ -45,7 +45,7 @@ inline cudaError_t launched() {
 int grid_blocks(long sites_per_rhs, int nt);
 
 // variant: launch shape 0..NUM_DSLASH_VARIANTS-1 (see dslash_impl.cuh), chosen by the autotuner.
-constexpr int NUM_DSLASH_VARIANTS = 6;
+constexpr int NUM_DSLASH_VARIANTS = 7;
 cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st);
 
 // ---------------------------------------------------------------- BLAS

@@ -5,7 +5,8 @@
 // capture, every launch variant is timed on the live arguments with CUDA
 // events and the fastest is kept for the rest of the process.  Launches met
 // during a capture before tuning use variant 0.  CPSB_TUNE=0 disables tuning;
-// CPSB_TUNE_VERBOSE=1 prints each decision.  The tuned kernels recompute the
+// CPSB_TUNE_VERBOSE=1 prints each decision; CPSB_TUNE_FORCE=v pins variant v
+// (for profiling) wherever it fits.  The tuned kernels recompute the
 // same output, so tuning has no effect on results.
 #include <stdio.h>
 #include <stdlib.h>
@@ -57,6 +58,23 @@ int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_
     if (it != table().end()) return it->second;
   }
   if (!tuning_enabled()) return 0;
+  if (const char *f = getenv("CPSB_TUNE_FORCE")) {
+    // Forced launch shape (profiling): used when it fits this configuration.
+    const int v = atoi(f);
+    if (v >= 0 && v < NUM_DSLASH_VARIANTS) {
+      cudaStreamCaptureStatus cs0 = cudaStreamCaptureStatusNone;
+      CK(cudaStreamIsCapturing(st, &cs0));
+      if (cs0 == cudaStreamCaptureStatusNone) {
+        const cudaError_t e = launch_dslash(prec, A, xpay, norm, v, st);
+        if (e == cudaSuccess) {
+          std::lock_guard<std::mutex> lk(mu);
+          table()[k] = v;
+          return v;
+        }
+        if (e != cudaErrorNotSupported) CK(e);
+      }
+    }
+  }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) return 0;
