@@ -121,6 +121,21 @@ class DiracOp:
               "cpsb_mdagm")
         return out, dot.value
 
+    def DslashPrec(self, x, cb, dag, precision):
+        """Dslash with fields and links stored in `precision` (F64, F32 or F16)."""
+        out = np.empty(self.n)
+        check(_lib.load().cpsb_dslash_ex(self.gauge.h, C.byref(self.p), precision, ptr(out), ptr(self._v(x)),
+                                         cb, dag), "cpsb_dslash_ex")
+        return out
+
+    def MatPcDagMatPcPrec(self, x, precision):
+        """MatPcDagMatPc with fields and links stored in `precision`; returns (out, |M x|^2)."""
+        out = np.empty(self.n)
+        dot = C.c_double()
+        check(_lib.load().cpsb_mdagm_ex(self.gauge.h, C.byref(self.p), precision, ptr(out), ptr(self._v(x)),
+                                        C.byref(dot)), "cpsb_mdagm_ex")
+        return out, dot.value
+
     def InvCg(self, src, stop_rsd=1e-10, max_num_iter=5000, precision=F64, guess=None, reliable_delta=0.1,
               batch=0):
         """Solves M^dag M x = src; returns (x, SolveResult)."""

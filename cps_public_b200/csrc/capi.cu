@@ -292,6 +292,44 @@ int cpsb_mdagm(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const doub
   });
 }
 
+int cpsb_dslash_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, double *out, const double *in, int cb,
+                   int dag) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (precision < CPSB_PREC_F64 || precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+    if (!out || !in || (cb != 0 && cb != 1) || (dag != 0 && dag != 1)) throw Error{CPSB_ERR_ARG, "bad argument"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, precision, 1);
+    Field fi(precision, op.nsites()), fo(precision, op.nsites());
+    upload(fi, &in, 1, op.nsites(), st);
+    op.dslash(fo, fi, cb, dag, st);
+    download(&out, 1, op.nsites(), fo, st);
+    return CPSB_OK;
+  });
+}
+
+int cpsb_mdagm_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, double *out, const double *in,
+                  double *dot) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (precision < CPSB_PREC_F64 || precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+    if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, precision, 1);
+    Field fi(precision, op.nsites()), fo(precision, op.nsites());
+    RedSlot rs;
+    DevBuf d(sizeof(double) * MAX_RHS);
+    Reduce r = rs.r((double *)d.p);
+    upload(fi, &in, 1, op.nsites(), st);
+    op.mdagm(fo, fi, &r, nullptr, st);
+    if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    download(&out, 1, op.nsites(), fo, st);
+    return CPSB_OK;
+  });
+}
+
 int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
                    void *stream) {
   return guarded([&] {

@@ -7,8 +7,11 @@
 //  * spinor field of N sites (a 4-D checkerboard, or Ls such slices, or
 //    Nrhs x Ls slices): chunk k of site i lives at base[k*N + i].
 //      FP64: 12 chunks of double2 = one complex component (spin k/3, colour k%3)
-//      FP32:  6 chunks of float4  = complex components 2k, 2k+1
-//      16-bit: 3 chunks of 8 fixed-point values (uint4) = components 4k..4k+3,
+//      FP32:  6 chunks of float4, spin-paired: chunk 3p+c holds colour c of the
+//             spins (2p, 2p+1) as (re_2p, re_2p+1, im_2p, im_2p+1), so the two
+//             spins of a pair sit in the two lanes of a float2 (packed FP32x2 math)
+//      16-bit: 3 chunks of 8 fixed-point values (uint4), the same spin-paired
+//             order (32-bit word w = (3p+c)*2 + re/im holds spins 2p, 2p+1),
 //             plus one float per site (max-abs / 32767, the quantum) in a
 //             separate norm array.  A value v is stored as the biased integer
 //             rint(v/quantum) + 32768 (15 bits of mantissa against IEEE fp16's 11).
@@ -138,9 +141,9 @@ __device__ __forceinline__ Spinor<float> load_spinor<P32>(const SpinorPtr &f, lo
 #pragma unroll
   for (int k = 0; k < 6; k++) {
     float4 v = __ldg(b + k * f.stride + i);
-    int c0 = 2 * k, c1 = 2 * k + 1;
-    s.c[c0 / 3][c0 % 3] = mk(v.x, v.y);
-    s.c[c1 / 3][c1 % 3] = mk(v.z, v.w);
+    const int p = k / 3, c = k % 3;
+    s.c[2 * p][c] = mk(v.x, v.z);
+    s.c[2 * p + 1][c] = mk(v.y, v.w);
   }
   return s;
 }
@@ -155,9 +158,11 @@ __device__ __forceinline__ Spinor<float> load_spinor<P16>(const SpinorPtr &f, lo
     uint4 v = __ldg(b + k * f.stride + i);
     const unsigned w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      int c = 4 * k + j;
-      s.c[c / 3][c % 3] = mk(dec16(w[j], 0) * nrm, dec16(w[j], 1) * nrm);
+    for (int j = 0; j < 4; j += 2) {
+      const int pc = (4 * k + j) / 2;  // = 3p + c
+      const int p = pc / 3, c = pc % 3;
+      s.c[2 * p][c] = mk(dec16(w[j], 0) * nrm, dec16(w[j + 1], 0) * nrm);
+      s.c[2 * p + 1][c] = mk(dec16(w[j], 1) * nrm, dec16(w[j + 1], 1) * nrm);
     }
   }
   return s;
@@ -178,9 +183,8 @@ __device__ __forceinline__ void store_spinor<P32>(const SpinorPtr &f, long i, co
   float4 *b = (float4 *)f.data;
 #pragma unroll
   for (int k = 0; k < 6; k++) {
-    int c0 = 2 * k, c1 = 2 * k + 1;
-    b[k * f.stride + i] = make_float4(s.c[c0 / 3][c0 % 3].re, s.c[c0 / 3][c0 % 3].im,
-                                      s.c[c1 / 3][c1 % 3].re, s.c[c1 / 3][c1 % 3].im);
+    const int p = k / 3, c = k % 3;
+    b[k * f.stride + i] = make_float4(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, s.c[2 * p][c].im, s.c[2 * p + 1][c].im);
   }
 }
 
@@ -198,9 +202,11 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
   for (int k = 0; k < 3; k++) {
     unsigned w[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      int c = 4 * k + j;
-      w[j] = enc16x2(s.c[c / 3][c % 3].re, s.c[c / 3][c % 3].im, scale);
+    for (int j = 0; j < 4; j += 2) {
+      const int pc = (4 * k + j) / 2;
+      const int p = pc / 3, c = pc % 3;
+      w[j] = enc16x2(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, scale);
+      w[j + 1] = enc16x2(s.c[2 * p][c].im, s.c[2 * p + 1][c].im, scale);
     }
     b[k * f.stride + i] = make_uint4(w[0], w[1], w[2], w[3]);
   }

@@ -29,9 +29,9 @@ __device__ __forceinline__ void ld_chunk<P64>(const SpinorPtr &f, long i, int k,
 }
 template <>
 __device__ __forceinline__ void ld_chunk<P32>(const SpinorPtr &f, long i, int k, cplx<float> *v) {
-  float4 a = __ldg((const float4 *)f.data + k * f.stride + i);
-  v[0] = mk(a.x, a.y);
-  v[1] = mk(a.z, a.w);
+  float4 a = __ldg((const float4 *)f.data + k * f.stride + i);  // spin-paired chunk
+  v[0] = mk(a.x, a.z);
+  v[1] = mk(a.y, a.w);
 }
 template <int P>
 __device__ __forceinline__ void st_chunk(const SpinorPtr &f, long i, int k, const cplx<typename ChunkT<P>::T> *v);
@@ -41,7 +41,7 @@ __device__ __forceinline__ void st_chunk<P64>(const SpinorPtr &f, long i, int k,
 }
 template <>
 __device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k, const cplx<float> *v) {
-  ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+  ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[1].re, v[0].im, v[1].im);
 }
 
 // v[s] += f * w[s] on one chunk

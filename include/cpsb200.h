@@ -152,6 +152,18 @@ int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg
 int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
                    void *stream);
 
+/* Dslash and MatPcDagMatPc evaluated with fields and links stored in the
+ * given precision (CPSB_PREC_F32: FP32 spinors, recon-12 FP32 links;
+ * CPSB_PREC_F16: 16-bit fixed-point spinors and links), the operators that
+ * the inner solves of mixed-precision InvCg / MInvCG apply.  Same interfaces
+ * as cpsb_dslash (DiracWilson::Dslash, d_op_wilson.h:135) and cpsb_mdagm
+ * (DiracOp::MatPcDagMatPc, dirac_op.h:198); in and out are FP64 CPS-order host
+ * vectors, converted on the device.  CPS has no reduced-precision counterpart. */
+int cpsb_dslash_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, double *out, const double *in, int cb,
+                   int dag);
+int cpsb_mdagm_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, double *out, const double *in,
+                  double *dot);
+
 /* Kernels this library has launched in the process (a graph replay counts each
  * of its kernel nodes): the device analogue of CPS's static flop counter
  * DiracOp::CGflops (include/util/dirac_op.h:74). */

@@ -135,3 +135,34 @@ def test_multi_rhs_matches_single(action, ls, prec):
         assert rel(xs[i], x1) < 1e-9
         if P == cb.F64:
             assert rs[i].iters == r1.iters
+
+
+@pytest.mark.parametrize("action,ls", [("wilson", 1), ("dwf", 8), ("mobius", 8)])
+@pytest.mark.parametrize("prec", ["F32", "F16"])
+def test_reduced_precision_operators(action, ls, prec):
+    """The FP32 / 16-bit storage kernels (packed FP32x2 arithmetic) against the
+    C oracle on an antiperiodic non-cubic lattice.  Tolerances: FP32 storage
+    2e-6 relative per Dslash; 16-bit fixed point (15-bit mantissa per site)
+    5e-4; MatPcDagMatPc applies four hops, so 4x those."""
+    import cps_public_b200 as cb
+    from cps_public_b200 import fields
+    from oracle import oracle
+    if action == "mobius" and prec == "F16":
+        pytest.skip("16-bit storage is not implemented for Mobius")
+    tol = {"F32": 2e-6, "F16": 5e-4}[prec]
+    P = getattr(cb, prec)
+    dims = (4, 6, 4, 8)
+    u = fields.random_gauge(dims, 0.25, 91)
+    n = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(n, 92)
+    cb.init(0)
+    g = cb.Gauge(u, dims, bc_t=1)
+    op = cb.DiracOp(g, action, mass=0.07, ls=ls)
+    ref = oracle.Op(action, dims, u, ls=ls, mass=0.07, bc_t=1)
+    for cb_ in (0, 1):
+        for dag in (0, 1):
+            assert rel(op.DslashPrec(src, cb_, dag, P), ref.dslash(src, cb_, dag)) < tol, (cb_, dag)
+    out, dot = op.MatPcDagMatPcPrec(src, P)
+    rout, rdot = ref.mdagm(src)
+    assert rel(out, rout) < 4 * tol
+    assert abs(dot - rdot) < 4 * tol * rdot
