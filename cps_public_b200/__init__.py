@@ -188,3 +188,64 @@ def fmat_evl_minv(op: DiracOp, f_in, shifts, cg_args, ms_type=MULTI, alpha=None)
     xs, r, rs = op.MInvCG(f_in, shifts, rsd, ms_type, alpha, cg_args[0].get("max_num_iter", 5000),
                           cg_args[0].get("precision", F64))
     return r.iters, xs, rs
+
+
+class Server:
+    """Request loop for concurrent solves (cpsb_serve_*).
+
+    ``srv = Server(slots=4)``; ``rid = srv.submit(op, [b0, b1], stop_rsd=1e-10, precision=F16)``;
+    ``xs, results, latency_ms = srv.wait(rid)``.  Admission is by the server's HBM
+    budget (``hbm_fraction`` of the free device memory, capped at ``hbm_bytes``).
+    """
+
+    def __init__(self, slots: int = 4, hbm_fraction: float = 0.9, hbm_bytes: int = 0):
+        if _initialised is None:
+            init(0)
+        h = C.c_void_p()
+        check(_lib.load().cpsb_serve_create(C.byref(h), slots, hbm_fraction, hbm_bytes), "cpsb_serve_create")
+        self.h = h
+        self._live = {}
+
+    def submit(self, op: DiracOp, srcs, stop_rsd=1e-10, max_num_iter=5000, precision=F64, guesses=None,
+               reliable_delta=0.1, batch=0) -> int:
+        bs = [op._v(s) for s in srcs]
+        xs = [np.zeros(op.n) if guesses is None else op._v(g).copy() for g in (guesses or [None] * len(bs))]
+        a = CgArg(stop_rsd, max_num_iter, precision, reliable_delta, batch)
+        xp = (_lib._dp * len(xs))(*[ptr(x) for x in xs])
+        bp = (_lib._dp * len(bs))(*[ptr(b) for b in bs])
+        rid = C.c_ulonglong()
+        check(_lib.load().cpsb_serve_submit(self.h, op.gauge.h, C.byref(op.p), C.byref(a), len(bs), xp, bp,
+                                            C.byref(rid)), "cpsb_serve_submit")
+        self._live[rid.value] = (xs, bs, xp, bp, op)  # keep the buffers alive until wait()
+        return rid.value
+
+    def done(self, rid: int) -> bool:
+        d = C.c_int()
+        check(_lib.load().cpsb_serve_poll(self.h, rid, C.byref(d)), "cpsb_serve_poll")
+        return bool(d.value)
+
+    def wait(self, rid: int):
+        """Returns (solutions, [SolveResult per RHS], latency in ms); raises on error."""
+        xs = self._live[rid][0]
+        res = (SolveResult * len(xs))()
+        lat = C.c_double()
+        rc = _lib.load().cpsb_serve_wait(self.h, rid, res, C.byref(lat))
+        self._live.pop(rid, None)
+        check(rc, "cpsb_serve_wait")
+        return xs, list(res), lat.value
+
+    def stats(self) -> dict:
+        st = _lib.ServeStats()
+        check(_lib.load().cpsb_serve_stats(self.h, C.byref(st)), "cpsb_serve_stats")
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            _lib.load().cpsb_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

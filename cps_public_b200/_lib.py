@@ -25,7 +25,8 @@ SYMBOLS = [
     "cpsb_matpc", "cpsb_mdagm", "cpsb_invcg", "cpsb_invcg_multi", "cpsb_minvcg", "cpsb_invcg_dev",
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches",
-    "cpsb_redot_noalloc",
+    "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
+    "cpsb_serve_stats", "cpsb_serve_destroy",
 ]
 
 
@@ -43,6 +44,17 @@ class CgArg(C.Structure):
 class SolveResult(C.Structure):
     _fields_ = [("iters", C.c_int), ("true_rsd", C.c_double), ("iter_rsd", C.c_double),
                 ("reliable_updates", C.c_int), ("seconds", C.c_double), ("status", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("completed", C.c_long), ("failed", C.c_long), ("rhs_completed", C.c_long),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("requests_per_s", C.c_double), ("rhs_per_s", C.c_double), ("peak_running", C.c_int),
+                ("queued", C.c_int), ("running", C.c_int), ("budget_bytes", C.c_double),
+                ("peak_reserved_bytes", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -79,6 +91,13 @@ def load():
     lib.cpsb_mdagm_dev.argtypes = [C.c_void_p, P, C.c_void_p, C.c_void_p, _dp, C.c_void_p]
     lib.cpsb_dslash_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, C.c_int, C.c_int]
     lib.cpsb_mdagm_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, _dp]
+    lib.cpsb_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_ulonglong]
+    lib.cpsb_serve_submit.argtypes = [C.c_void_p, C.c_void_p, P, A, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
+                                      C.POINTER(C.c_ulonglong)]
+    lib.cpsb_serve_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
+    lib.cpsb_serve_wait.argtypes = [C.c_void_p, C.c_ulonglong, R, _dp]
+    lib.cpsb_serve_stats.argtypes = [C.c_void_p, C.POINTER(ServeStats)]
+    lib.cpsb_serve_destroy.argtypes = [C.c_void_p]
     lib.cpsb_redot_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
     lib.cpsb_kernel_launches.argtypes = [C.POINTER(C.c_ulonglong)]
     lib.cpsb_bench_dslash.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_int, _dp, _dp]

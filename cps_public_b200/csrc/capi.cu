@@ -6,7 +6,7 @@
 
 #include <chrono>
 
-#include "host.h"
+#include "abi.h"
 
 using namespace cpsb;
 
@@ -14,28 +14,11 @@ namespace cpsb {
 void drop_solvers(Gauge *G);
 }
 
-struct cpsb_gauge_s {
-  Gauge g;
-};
+namespace cpsb {
 
-namespace {
-
-thread_local std::string g_last_error;
-
-template <class F>
-int guarded(F &&f) {
-  try {
-    return f();
-  } catch (const Error &e) {
-    g_last_error = e.msg;
-    return e.code;
-  } catch (const std::bad_alloc &) {
-    g_last_error = "host allocation failed";
-    return CPSB_ERR_OOM;
-  } catch (...) {
-    g_last_error = "unexpected exception";
-    return CPSB_ERR_CUDA;
-  }
+std::string &last_error_slot() {
+  thread_local std::string msg;
+  return msg;
 }
 
 void need_init() {
@@ -49,9 +32,19 @@ void check_params(cpsb_gauge h, const cpsb_dirac_params *p) {
   if (p->action != CPSB_WILSON && (p->ls < 2 || p->ls > 64)) throw Error{CPSB_ERR_ARG, "ls must be in [2, 64]"};
 }
 
+void check_cg(const cpsb_cg_arg *a) {
+  if (!a) throw Error{CPSB_ERR_ARG, "null cg arguments"};
+  if (!(a->stop_rsd >= 0) || a->max_num_iter < 0) throw Error{CPSB_ERR_ARG, "bad stop_rsd / max_num_iter"};
+  if (a->precision < CPSB_PREC_F64 || a->precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+}
+
 long cb_sites(cpsb_gauge h, const cpsb_dirac_params *p) {
   return h->g.n4cb * (p->action == CPSB_WILSON ? 1 : p->ls);
 }
+
+}  // namespace cpsb
+
+namespace {
 
 // Pinned staging buffer reused across calls (grown on demand).
 struct Staging {
@@ -74,20 +67,6 @@ Staging &staging() {
   return s;
 }
 
-void h2d_vec(Field &f, const double *host, long nsites, long offset_sites, cudaStream_t st, DevBuf &tmp) {
-  const size_t bytes = (size_t)nsites * 24 * sizeof(double);
-  if (tmp.bytes < bytes) tmp.alloc(bytes);
-  Staging &sg = staging();
-  std::lock_guard<std::mutex> lk(sg.mu);
-  void *pin = sg.get(bytes);
-  memcpy(pin, host, bytes);
-  CK(cudaMemcpyAsync(tmp.p, pin, bytes, cudaMemcpyHostToDevice, st));
-  SpinorPtr dst = f.ptr();
-  if (f.prec == P64) dst.data = (char *)dst.data + 0;  // whole-field packing below uses offsets
-  CK(cudaStreamSynchronize(st));
-  (void)offset_sites;
-}
-
 }  // namespace
 
 extern "C" {
@@ -107,7 +86,7 @@ const char *cpsb_error_string(int code) {
   return "unknown status";
 }
 
-const char *cpsb_last_error(void) { return g_last_error.c_str(); }
+const char *cpsb_last_error(void) { return last_error_slot().c_str(); }
 
 int cpsb_init(int device) {
   return guarded([&] {
@@ -351,12 +330,6 @@ int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const 
   });
 }
 
-static int check_cg(const cpsb_cg_arg *a) {
-  if (!a) throw Error{CPSB_ERR_ARG, "null cg arguments"};
-  if (!(a->stop_rsd >= 0) || a->max_num_iter < 0) throw Error{CPSB_ERR_ARG, "bad stop_rsd / max_num_iter"};
-  if (a->precision < CPSB_PREC_F64 || a->precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
-  return 0;
-}
 
 int cpsb_invcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs, double **x,
                      const double *const *b, cpsb_solve_result *res) {

@@ -235,6 +235,7 @@ static cudaError_t dslash_launch_v(DslashArgs A, int xpay, int norm, cudaStream_
   const int npar = A.five_d ? 2 : 1;
   size_t shm = LC ? (size_t)npar * 8 * 9 * tx * sizeof(cplx<T>) : 0;
   if (norm) shm += sizeof(double) * NT * A.g.nrhs;
+  if (shm > 200 * 1024) return cudaErrorNotSupported;  // above the opt-in set below
   static bool attr_set[2][2] = {{false, false}, {false, false}};
   if (shm > 48 * 1024) {
     auto set = [&](const void *f) { return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); };

@@ -192,6 +192,49 @@ int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, i
  * (include/util/vector.h:955) with no allocation of its own. */
 int cpsb_redot_noalloc(const double *x, const double *y, long n, int nvec, double *result, void *stream);
 
+/* Request loop for concurrent solves.  CPS runs one DiracOp at a time
+ * (DiracOp::scope_lock, d_op_base/comsrc/dirac_op_base.C:26,112-118); a caller
+ * that issues many Lattice::FmatEvlInv solves (lattice.h:942) -- differing
+ * lattice, Ls, mass, tolerance and right-hand-side count, against gauge fields
+ * that stay loaded -- submits them here instead.  No counterpart in the
+ * reference.
+ *
+ * cpsb_serve_create: `slots` worker threads, each with its own CUDA stream,
+ *   run admitted solves concurrently.  The HBM budget is hbm_fraction of the
+ *   device memory free at creation (0 < hbm_fraction <= 1), capped at
+ *   hbm_bytes when nonzero.
+ * cpsb_serve_submit: queues the solve of nrhs systems MatPcDagMatPc x = b
+ *   (semantics of cpsb_invcg_multi: x holds the guesses on entry).  x[] and
+ *   b[] must stay valid until cpsb_serve_wait returns.  The request runs as
+ *   work items of up to 16 right-hand sides, each admitted when a slot is free
+ *   and its device footprint fits the unreserved budget; a request of which
+ *   one right-hand side exceeds the budget returns CPSB_ERR_OOM.
+ * cpsb_serve_poll: *done = 1 once every item has finished.
+ * cpsb_serve_wait: blocks until the request is done, fills res[nrhs] and the
+ *   latency (submission to completion, ms), releases the id and returns the
+ *   request's status.
+ * cpsb_serve_stats: latency percentiles and throughput of completed requests.
+ * cpsb_serve_destroy: serves what is queued, then joins the workers. */
+typedef struct cpsb_server_s *cpsb_server;
+typedef struct {
+  long completed;              /* requests finished with status >= 0 */
+  long failed;                 /* requests finished with an error */
+  long rhs_completed;          /* right-hand sides of the completed requests */
+  double p50_ms, p99_ms, mean_ms, max_ms;
+  double requests_per_s;       /* completed / (last completion - first submission) */
+  double rhs_per_s;
+  int peak_running;            /* most work items running at once */
+  int queued, running;
+  double budget_bytes, peak_reserved_bytes;
+} cpsb_serve_stats_t;
+int cpsb_serve_create(cpsb_server *s, int slots, double hbm_fraction, unsigned long long hbm_bytes);
+int cpsb_serve_submit(cpsb_server s, cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs,
+                      double **x, const double *const *b, unsigned long long *id);
+int cpsb_serve_poll(cpsb_server s, unsigned long long id, int *done);
+int cpsb_serve_wait(cpsb_server s, unsigned long long id, cpsb_solve_result *res, double *latency_ms);
+int cpsb_serve_stats(cpsb_server s, cpsb_serve_stats_t *st);
+int cpsb_serve_destroy(cpsb_server s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,3 +41,6 @@ def test_error_strings_and_no_device_status():
     if torch.cuda.is_available():
         pytest.skip("a GPU is present; the no-device path is not reachable")
     assert lib.cpsb_init(0) == -6   # CPSB_ERR_NO_DEVICE, no abort
+    h = C.c_void_p()
+    assert lib.cpsb_serve_create(C.byref(h), 2, 0.5, 0) == -6
+    assert not h.value

@@ -1,0 +1,99 @@
+"""The request loop (cpsb_serve_*) on the GPU.
+
+A mix of DWF solves of differing lattice, Ls, mass, tolerance, right-hand-side
+count and inner precision is run once request by request and once submitted
+all at once to a server with several slots.  Stated tolerance: each result is
+bit-identical alone and in the mix (a request's arithmetic does not depend on
+what else runs; the launch shapes the autotuner chose are cached per operator
+shape), and every solve meets its FP64 true residual.  Admission under a tight
+HBM budget splits requests into single right-hand-side items, never reserves
+more than the budget, and gives the single-RHS InvCg result.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GAUGES = [((4, 4, 4, 4), 0.2, 301), ((4, 4, 4, 8), 0.2, 302), ((8, 8, 8, 8), 0.15, 303)]
+# (gauge, ls, mass, stop_rsd, nrhs, precision)
+REQUESTS = [
+    (0, 4, 0.05, 1e-10, 1, "F16"),
+    (1, 8, 0.01, 1e-8, 2, "F32"),
+    (2, 8, 0.1, 1e-12, 3, "F32"),
+    (0, 6, 0.003, 1e-10, 2, "F64"),
+    (1, 4, 0.02, 1e-10, 1, "F16"),
+    (2, 4, 0.05, 1e-10, 4, "F16"),
+    (0, 12, 0.01, 1e-12, 1, "F32"),
+    (1, 8, 0.05, 1e-8, 3, "F64"),
+]
+
+
+@pytest.fixture(scope="module")
+def setup():
+    import cps_public_b200 as cb
+    from cps_public_b200 import fields
+    cb.init(0)
+    gauges = [cb.Gauge(fields.random_gauge(d, eps, seed), d) for d, eps, seed in GAUGES]
+    reqs = []
+    for k, (gi, ls, mass, tol, nrhs, prec) in enumerate(REQUESTS):
+        op = cb.DiracOp(gauges[gi], "dwf", mass=mass, ls=ls, m5=1.8)
+        n = op.n // 24
+        srcs = [fields.random_source(n, 1000 + 17 * k + i) for i in range(nrhs)]
+        reqs.append((op, srcs, tol, getattr(cb, prec)))
+    return cb, gauges, reqs
+
+
+def true_rsd(op, x, b):
+    ax, _ = op.MatPcDagMatPc(x)
+    return np.linalg.norm(b - ax) / np.linalg.norm(b)
+
+
+def test_alone_equals_mix(setup):
+    cb, _, reqs = setup
+    alone = []
+    srv = cb.Server(slots=1)
+    for op, srcs, tol, prec in reqs:
+        rid = srv.submit(op, srcs, stop_rsd=tol, precision=prec)
+        alone.append(srv.wait(rid))
+    srv.close()
+    srv = cb.Server(slots=4)
+    ids = [srv.submit(op, srcs, stop_rsd=tol, precision=prec) for op, srcs, tol, prec in reqs]
+    mix = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["peak_running"] >= 2, st          # the mix really overlapped
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    for (op, srcs, tol, prec), (xa, ra, _), (xm, rm, _) in zip(reqs, alone, mix):
+        for i, b in enumerate(srcs):
+            assert np.array_equal(xa[i], xm[i])
+            assert ra[i].iters == rm[i].iters
+            assert rm[i].status == 0 and rm[i].true_rsd <= tol
+            assert true_rsd(op, xm[i], b) <= 1.5 * tol
+
+
+def test_admission_budget_splits_requests(setup):
+    cb, _, reqs = setup
+    op, srcs, tol, prec = reqs[5]           # 8^4, Ls 4, four right-hand sides, 16-bit inner
+    n = op.n // 24
+    one_rhs = n * (192 * 5 + 192 * 2 + 52 * 5 + 96) + (8 << 20)  # footprint of one RHS (serve.cu)
+    srv = cb.Server(slots=4, hbm_bytes=one_rhs + (1 << 20))
+    rid = srv.submit(op, srcs, stop_rsd=tol, precision=prec)
+    xs, rs, _ = srv.wait(rid)
+    st = srv.stats()
+    srv.close()
+    assert st["peak_running"] == 1 and st["peak_reserved_bytes"] <= st["budget_bytes"]
+    for i, b in enumerate(srcs):
+        x1, r1 = op.InvCg(b, stop_rsd=tol, precision=prec)
+        assert np.array_equal(xs[i], x1) and rs[i].iters == r1.iters
+        assert true_rsd(op, xs[i], b) <= 1.5 * tol
+
+
+def test_request_larger_than_budget_is_refused(setup):
+    cb, _, reqs = setup
+    op, srcs, tol, prec = reqs[0]
+    srv = cb.Server(slots=2, hbm_bytes=1 << 20)
+    with pytest.raises(cb.CpsbError) as e:
+        srv.submit(op, srcs, stop_rsd=tol, precision=prec)
+    assert e.value.code == -3
+    srv.close()
