@@ -44,8 +44,10 @@ inline cudaError_t launched() {
 // Grid: blockIdx.y = right-hand side, blockIdx.x strides over the sites of one RHS.
 int grid_blocks(long sites_per_rhs, int nt);
 
-// variant: launch shape 0..NUM_DSLASH_VARIANTS-1 (see dslash_impl.cuh), chosen by the autotuner.
-constexpr int NUM_DSLASH_VARIANTS = 7;
+// variant: launch shape 0..NUM_DSLASH_VARIANTS-1 (dslash_impl.cuh: 0-6 for FP64;
+// dslash_x2.cuh: 0-11 for FP32 / 16-bit), chosen by the autotuner; a launcher
+// returns cudaErrorNotSupported for shapes it does not have.
+constexpr int NUM_DSLASH_VARIANTS = 12;
 cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st);
 
 // ---------------------------------------------------------------- BLAS

@@ -4,6 +4,6 @@
 
 namespace cpsb {
 cudaError_t launch_dslash_f16(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
-  return dslash_x2_launch_p<P16>(A, xpay, norm, variant, st);
+  return dslash_fp32x2_launch<P16>(A, xpay, norm, variant, st);
 }
 }  // namespace cpsb

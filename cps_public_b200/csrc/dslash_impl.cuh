@@ -267,7 +267,8 @@ static cudaError_t dslash_launch_p(const DslashArgs &A, int xpay, int norm, int 
     case 4: return dslash_launch_v<P, 256, 1, true>(A, xpay, norm, st);
     case 5: return dslash_launch_v<P, 256, 2, true>(A, xpay, norm, st);
     case 6: return dslash_launch_v<P, 128, 4, true>(A, xpay, norm, st);
-    default: return dslash_launch_v<P, 128, 1, false>(A, xpay, norm, st);
+    case 0: return dslash_launch_v<P, 128, 1, false>(A, xpay, norm, st);
+    default: return cudaErrorNotSupported;
   }
 }
 

@@ -522,7 +522,295 @@ static cudaError_t dslash_x2_launch_p(const DslashArgs &A, int xpay, int norm, i
     case 4: return dslash_x2_launch_v<P, 256, 1, true>(A, xpay, norm, st);
     case 5: return dslash_x2_launch_v<P, 256, 2, true>(A, xpay, norm, st);
     case 6: return dslash_x2_launch_v<P, 128, 4, true>(A, xpay, norm, st);
-    default: return dslash_x2_launch_v<P, 128, 1, false>(A, xpay, norm, st);
+    case 0: return dslash_x2_launch_v<P, 128, 1, false>(A, xpay, norm, st);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Parity-class kernel: links of a tile held once in shared memory for every
+// slice and right-hand side of one output parity, neighbour indices computed
+// once per tile.
+//
+// A work unit is (tile of TX checkerboard sites, output-parity class).  For the
+// 5-D checkerboard (DWF) the slices of one class are s0, s0+2, ... and all use
+// the links of that 4-D parity, so the unit's 8*TX links are decoded and
+// reconstructed once into shared memory as (Re, Im) pairs and every slice and
+// right-hand side of the unit reads them from there; each thread computes its
+// site's 8 neighbour indices and boundary flags once and then sweeps its
+// (rhs, slice) pairs -- SL lanes of the block share them.
+// ---------------------------------------------------------------------------
+namespace x3 {
+
+template <int P> __device__ __forceinline__ SpX2 load(const SpinorPtr &f, unsigned i, float *nrm) {
+  return load_x2<P>(f, (long)i, nrm);
+}
+
+// A site as loaded from memory, before unpacking (so loads can be issued
+// ahead of the arithmetic that consumes them).
+template <int P> struct Raw;
+template <> struct Raw<P32> { float4 c[6]; };
+template <> struct Raw<P16> { uint4 c[3]; float nrm; };
+
+template <int P> __device__ __forceinline__ Raw<P> load_raw(const SpinorPtr &f, unsigned i);
+template <> __device__ __forceinline__ Raw<P32> load_raw<P32>(const SpinorPtr &f, unsigned i) {
+  Raw<P32> r;
+#pragma unroll
+  for (int k = 0; k < 6; k++) r.c[k] = __ldg((const float4 *)f.data + k * f.stride + i);
+  return r;
+}
+template <> __device__ __forceinline__ Raw<P16> load_raw<P16>(const SpinorPtr &f, unsigned i) {
+  Raw<P16> r;
+#pragma unroll
+  for (int k = 0; k < 3; k++) r.c[k] = __ldg((const uint4 *)f.data + k * f.stride + i);
+  r.nrm = __ldg(f.norm + i);
+  return r;
+}
+
+__device__ __forceinline__ SpX2 unpack(const Raw<P32> &r, float *nrm) {
+  SpX2 s;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    s.re[k / 3][k % 3] = f2(r.c[k].x, r.c[k].y);
+    s.im[k / 3][k % 3] = f2(r.c[k].z, r.c[k].w);
+  }
+  *nrm = 1.0f;
+  return s;
+}
+__device__ __forceinline__ SpX2 unpack(const Raw<P16> &r, float *nrm) {
+  SpX2 s;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int pa = 2 * k, pb = 2 * k + 1;
+    s.re[pa / 3][pa % 3] = dec16x2(r.c[k].x);
+    s.im[pa / 3][pa % 3] = dec16x2(r.c[k].y);
+    s.re[pb / 3][pb % 3] = dec16x2(r.c[k].z);
+    s.im[pb / 3][pb % 3] = dec16x2(r.c[k].w);
+  }
+  *nrm = r.nrm;
+  return s;
+}
+
+// U h / U^dag h with the link elements (ur, ui) read from shared memory.
+template <bool DAG> __device__ __forceinline__ HfX2 umul(const float2 *sh, int TX, const HfX2 &h) {
+  float2 e[3][3];
+#pragma unroll
+  for (int k = 0; k < 9; k++) e[k / 3][k % 3] = sh[k * TX];
+  HfX2 o;
+  float2 nh[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) nh[k] = DAG ? f2(-h.re[k].x, -h.re[k].y) : f2(-h.im[k].x, -h.im[k].y);
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float2 re = f2b(0.f), im = f2b(0.f);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float2 u = DAG ? e[k][r] : e[r][k];
+      const float2 ur = f2b(u.x), ui = f2b(u.y);
+      re = fma2(ur, h.re[k], re);
+      im = fma2(ur, h.im[k], im);
+      if (DAG) {
+        re = fma2(ui, h.im[k], re);
+        im = fma2(ui, nh[k], im);
+      } else {
+        re = fma2(ui, nh[k], re);
+        im = fma2(ui, h.re[k], im);
+      }
+    }
+    o.re[r] = re;
+    o.im[r] = im;
+  }
+  return o;
+}
+
+// DEPTH: neighbours whose loads are issued ahead of the one being computed
+// (0: each is loaded where it is used; 8: all eight at the start of the site).
+template <int P, int NT, int MINB, int SL, int DEPTH, bool XPAY, bool NORM>
+__global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
+  constexpr int TX = NT / SL;
+  const Geom &g = A.g;
+  __shared__ double red[NT / 32];
+  extern __shared__ double dyn_sh[];
+  float2 *lsh = (float2 *)dyn_sh;                       // [8*9][TX]
+  double *nrm_sh = dyn_sh + (size_t)72 * TX * sizeof(float2) / sizeof(double);
+  const int tx = threadIdx.x % TX, sl = threadIdx.x / TX;
+  const int ntiles = (g.n4cb + TX - 1) / TX;
+  const int nclass = A.five_d ? 2 : 1;
+  const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
+  if (NORM)
+    for (int q = 0; q < g.nrhs; q++) nrm_sh[q * NT + threadIdx.x] = 0;
+  const float2 a2 = f2b((float)A.a);
+  const float sdag = A.dag ? -1.f : 1.f;
+  const int L[4] = {g.lx, g.ly, g.lz, g.lt};
+  for (int unit = blockIdx.x; unit < ntiles * nclass; unit += gridDim.x) {
+    const int tile = unit / nclass, cls = unit - tile * nclass;
+    // output parity of the class and its first slice
+    const int par_out = A.five_d ? cls : 1 - A.cb;
+    const int s0 = A.five_d ? ((par_out + A.cb + 1) & 1) : 0;
+    const int sstep = A.five_d ? 2 : 1;
+    const int nsl = (g.ls - s0 + sstep - 1) / sstep;
+    __syncthreads();  // the previous unit is done with the links
+    for (int it = threadIdx.x; it < TX * 8; it += NT) {
+      const int xi = it % TX, j = it / TX;
+      const int xx = tile * TX + xi;
+      if (xx >= g.n4cb) continue;
+      Link<float> l;
+      if (j < 4) {
+        l = load_link<P>(A.U, par_out, j, xx);
+      } else {
+        const int mu = j - 4;
+        const Coord c = decode(g, xx, par_out);
+        int p[4] = {c.x, c.y, c.z, c.t};
+        p[mu] = (p[mu] == 0) ? L[mu] - 1 : p[mu] - 1;
+        l = load_link<P>(A.U, 1 - par_out, mu, cbindex(g, p[0], p[1], p[2], p[3]));
+      }
+#pragma unroll
+      for (int k = 0; k < 9; k++) lsh[(j * 9 + k) * TX + xi] = make_float2(l.u[k / 3][k % 3].re, l.u[k / 3][k % 3].im);
+    }
+    __syncthreads();
+    const int x = tile * TX + tx;
+    if (x >= g.n4cb) continue;
+    const Coord c = decode(g, x, par_out);
+    int nb[8];
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      int p[4] = {c.x, c.y, c.z, c.t};
+      p[mu] = (p[mu] + 1 == L[mu]) ? 0 : p[mu] + 1;
+      nb[mu] = cbindex(g, p[0], p[1], p[2], p[3]);
+      int q[4] = {c.x, c.y, c.z, c.t};
+      q[mu] = (q[mu] == 0) ? L[mu] - 1 : q[mu] - 1;
+      nb[4 + mu] = cbindex(g, q[0], q[1], q[2], q[3]);
+    }
+    const bool flip_f = A.bc_t_sign < 0 && c.t == g.lt - 1;
+    const bool flip_b = A.bc_t_sign < 0 && c.t == 0;
+    const float2 *lx = lsh + tx;
+    for (int w = sl; w < g.nrhs * nsl; w += SL) {
+      const int rhs = w / nsl;
+      const int s = s0 + sstep * (w - rhs * nsl);
+      if (A.skip && A.skip[rhs]) continue;
+      const unsigned rbase = (unsigned)rhs * per;
+      const unsigned sbase = rbase + (unsigned)s * (unsigned)g.n4cb;
+      AccX2 acc;
+      zero_x2(acc);
+      Raw<P> rw[8];
+#pragma unroll
+      for (int j = 0; j < DEPTH && j < 8; j++) rw[j] = load_raw<P>(A.in, sbase + (unsigned)nb[j]);
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (DEPTH > 0 && j + DEPTH < 8) rw[j + DEPTH] = load_raw<P>(A.in, sbase + (unsigned)nb[j + DEPTH]);
+        float nrm;
+        const SpX2 v = unpack(DEPTH > 0 ? rw[j] : load_raw<P>(A.in, sbase + (unsigned)nb[j]), &nrm);
+        const float sg = j < 4 ? -sdag : sdag;
+        const float f = (j == 3 && flip_f) || (j == 7 && flip_b) ? -nrm : nrm;
+        const float2 *lj = lx + j * 9 * TX;
+        switch (j & 3) {
+          case 0: {
+            const HfX2 h = project_x2<0>(v, sg);
+            accum_x2<0>(acc, j < 4 ? umul<false>(lj, TX, h) : umul<true>(lj, TX, h), sg, f);
+          } break;
+          case 1: {
+            const HfX2 h = project_x2<1>(v, sg);
+            accum_x2<1>(acc, j < 4 ? umul<false>(lj, TX, h) : umul<true>(lj, TX, h), sg, f);
+          } break;
+          case 2: {
+            const HfX2 h = project_x2<2>(v, sg);
+            accum_x2<2>(acc, j < 4 ? umul<false>(lj, TX, h) : umul<true>(lj, TX, h), sg, f);
+          } break;
+          default: {
+            const HfX2 h = project_x2<3>(v, sg);
+            accum_x2<3>(acc, j < 4 ? umul<false>(lj, TX, h) : umul<true>(lj, TX, h), sg, f);
+          } break;
+        }
+      }
+      if (A.hop5) hop5_x2<P>(A, x, s, (long)rbase, acc);
+      SpX2 o = merge_x2(acc);
+      const unsigned i = sbase + (unsigned)x;
+      if (XPAY) {
+        float xn;
+        const SpX2 xv = load<P>(A.x, i, &xn);
+#pragma unroll
+        for (int p = 0; p < 2; p++)
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++) {
+            if (P == P16) {
+              o.re[p][cc] = fma2(xv.re[p][cc], f2b(xn), mul2(a2, o.re[p][cc]));
+              o.im[p][cc] = fma2(xv.im[p][cc], f2b(xn), mul2(a2, o.im[p][cc]));
+            } else {
+              o.re[p][cc] = fma2(a2, o.re[p][cc], xv.re[p][cc]);
+              o.im[p][cc] = fma2(a2, o.im[p][cc], xv.im[p][cc]);
+            }
+          }
+      } else if (A.a != 1.0) {
+#pragma unroll
+        for (int p = 0; p < 2; p++)
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++) {
+            o.re[p][cc] = mul2(a2, o.re[p][cc]);
+            o.im[p][cc] = mul2(a2, o.im[p][cc]);
+          }
+      }
+      const double n2 = store_x2<P>(A.out, (long)i, o);
+      if (NORM) nrm_sh[rhs * NT + threadIdx.x] += n2;
+    }
+  }
+  if (NORM) {
+    for (int q = 0; q < g.nrhs; q++) {
+      const double bs = block_sum<NT>(nrm_sh[q * NT + threadIdx.x], red);
+      if (threadIdx.x == 0) A.red.partial[q * gridDim.x + blockIdx.x] = bs;
+    }
+    if (last_block(A.red.ticket, gridDim.x)) {
+      for (int q = 0; q < g.nrhs; q++) {
+        double t = ordered_sum<NT>(A.red.partial + q * gridDim.x, gridDim.x, red);
+        if (threadIdx.x == 0 && !(A.skip && A.skip[q])) A.red.result[q] = t;
+        __syncthreads();
+      }
+    }
+  }
+}
+
+template <int P, int NT, int MINB, int SL, int DEPTH>
+static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
+  constexpr int TX = NT / SL;
+  const int nclass = A.five_d ? 2 : 1;
+  const int nsl = A.five_d ? (A.g.ls + 1) / 2 : A.g.ls;
+  // every lane of the block must have work for this shape to make sense
+  if (SL > 1 && nsl * A.g.nrhs < SL) return cudaErrorNotSupported;
+  const long units = (long)((A.g.n4cb + TX - 1) / TX) * nclass;
+  const long nb = units < 148L * 16 ? units : 148L * 16;
+  size_t shm = (size_t)72 * TX * sizeof(float2);
+  if (norm) shm += sizeof(double) * NT * A.g.nrhs;
+  if (shm > 200 * 1024) return cudaErrorNotSupported;  // above the opt-in set below
+  static bool attr_set[2][2] = {{false, false}, {false, false}};
+  if (shm > 48 * 1024 && !attr_set[xpay][norm]) {
+    const void *f = xpay && norm ? (const void *)kernel<P, NT, MINB, SL, DEPTH, true, true>
+                  : xpay         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, true, false>
+                  : norm         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, false, true>
+                                 : (const void *)kernel<P, NT, MINB, SL, DEPTH, false, false>;
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set[xpay][norm] = true;
+  }
+  if (xpay && norm) kernel<P, NT, MINB, SL, DEPTH, true, true><<<(unsigned)nb, NT, shm, st>>>(A);
+  else if (xpay) kernel<P, NT, MINB, SL, DEPTH, true, false><<<(unsigned)nb, NT, shm, st>>>(A);
+  else if (norm) kernel<P, NT, MINB, SL, DEPTH, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
+  else kernel<P, NT, MINB, SL, DEPTH, false, false><<<(unsigned)nb, NT, shm, st>>>(A);
+  return launched();
+}
+
+}  // namespace x3
+
+// Launch shapes the autotuner chooses from: 0-6 the kernel above, 7-11 the
+// parity-class kernel with (threads, min blocks/SM, slice lanes, load depth).
+template <int P>
+static cudaError_t dslash_fp32x2_launch(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
+  switch (variant) {
+    case 7: return x3::launch_v<P, 128, 3, 4, 8>(A, xpay, norm, st);
+    case 8: return x3::launch_v<P, 128, 4, 4, 8>(A, xpay, norm, st);
+    case 9: return x3::launch_v<P, 128, 4, 4, 0>(A, xpay, norm, st);
+    case 10: return x3::launch_v<P, 128, 3, 4, 4>(A, xpay, norm, st);
+    case 11: return x3::launch_v<P, 128, 4, 4, 2>(A, xpay, norm, st);
+    default: return dslash_x2_launch_p<P>(A, xpay, norm, variant, st);
   }
 }
 

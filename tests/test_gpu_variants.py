@@ -1,0 +1,64 @@
+"""Every autotuner launch shape of the hop kernels against the C oracle.
+
+The autotuner picks one launch shape per operator shape, so the parity tests
+exercise only the winners; here each shape is pinned in a fresh process
+(CPSB_TUNE_FORCE) and Dslash / MatPcDagMatPc are compared with the oracle for
+Wilson, DWF and Mobius at FP64 (tolerance 1e-13), FP32 (2e-6 per hop) and
+16-bit storage (5e-4 per hop; Mobius has no 16-bit storage), on two non-cubic
+antiperiodic lattices: 4x6x4x8 (tiles of consecutive sites) and 8x8x4x6 (32
+sites per (z, t) plane, so the multi-plane tiles are used).
+"""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TOL = {0: 1e-13, 1: 2e-6, 2: 5e-4}
+
+
+def _child():
+    import numpy as np
+    import cps_public_b200 as cb
+    from cps_public_b200 import fields
+    from oracle import oracle
+    out = {}
+    cb.init(0)
+    for dims, action, ls in [(d, a, l) for d in ((4, 6, 4, 8), (8, 8, 4, 6))
+                             for a, l in (("wilson", 1), ("dwf", 8), ("mobius", 8))]:
+        u = fields.random_gauge(dims, 0.25, 41)
+        g = cb.Gauge(u, dims, bc_t=1)
+        n = int(np.prod(dims)) // 2 * ls
+        src = fields.random_source(n, 42)
+        op = cb.DiracOp(g, action, mass=0.07, ls=ls)
+        ref = oracle.Op(action, dims, u, ls=ls, mass=0.07, bc_t=1)
+        rd = ref.dslash(src, 1, 0)
+        rdd = ref.dslash(src, 0, 1)
+        rm, rdot = ref.mdagm(src)
+        for prec in (0, 1, 2):
+            if action == "mobius" and prec == 2:
+                continue
+            d0 = op.DslashPrec(src, 1, 0, prec)
+            d1 = op.DslashPrec(src, 0, 1, prec)
+            m, dot = op.MatPcDagMatPcPrec(src, prec)
+            rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            out[f"{dims}/{action}/{prec}"] = [rel(d0, rd), rel(d1, rdd), rel(m, rm), abs(dot - rdot) / rdot]
+    print(json.dumps(out))
+
+
+@pytest.mark.parametrize("variant", list(range(12)))
+def test_launch_shape_matches_oracle(variant):
+    env = dict(os.environ, CPSB_TUNE_FORCE=str(variant))
+    p = subprocess.run([sys.executable, "-c", "import tests.test_gpu_variants as t; t._child()"], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    res = json.loads(p.stdout.strip().splitlines()[-1])
+    for key, errs in res.items():
+        prec = int(key.split("/")[2])
+        tol = TOL[prec]
+        assert errs[0] < tol and errs[1] < tol, (key, errs)
+        assert errs[2] < 4 * tol and errs[3] < 4 * tol, (key, errs)
