@@ -3,14 +3,19 @@
 Workload (the reference's headline DWF configuration): 16^3 x 32 lattice,
 Ls = 16, M5 = 1.8, m_f = 0.01, links reunitarise(exp(i 0.2 H)) seeded,
 Gaussian source on the odd checkerboard, stop_rsd 1e-10 on the FP64 true
-residual.  A step is one full solve (MatPcDagMatPc x = b from x = 0).
+residual.  A step is one full solve (MatPcDagMatPc x = b from x = 0) of the
+arm's right-hand sides.
 
 Arms:
-  (default)        this library: FP16-storage mixed CG is the headline `value`;
-                   FP32-mixed and plain FP64 CG are timed beside it.  `value` uses
-                   device-resident inputs (cpsb_invcg_dev); `e2e` goes through the
-                   host-pointer C ABI (cpsb_invcg) with the H2D copy of b and the
-                   D2H copy of x in every step.
+  (default)        this library.  The headline `value` is the 16-bit-storage
+                   mixed-precision CG solving 12 right-hand sides in one batched
+                   solve (solves/s counts right-hand sides, each to FP64 true
+                   residual 1e-10); FP32-mixed x12, single-RHS 16-bit and FP32
+                   mixed, and the plain FP64 CG on one right-hand side are timed
+                   beside it.  `value` uses device-resident inputs
+                   (cpsb_invcg_multi_dev); `e2e` goes through the host-pointer C
+                   ABI (cpsb_invcg_multi) with the H2D copies of guesses and sources
+                   and the D2H copy of the solutions in every step.
   --impl reference the CPS noarch CPU code (oracle/_ref/cpsref, compiled from the
                    reference sources) on all host cores: each step runs one
                    MatPcDagMatPc per core in parallel processes, and solves/s is
@@ -143,7 +148,22 @@ def make_inputs(nsrc):
     return u, srcs
 
 
+# Solver arms: (name, inner precision, right-hand sides per solve).  The
+# headline is the 16-bit-storage mixed-precision CG on NRHS right-hand sides in
+# one batched solve (every RHS to FP64 true residual 1e-10); the plain FP64 CG
+# on one right-hand side is its reference point (mixed_vs_fp64).
+NRHS = 12
+HEADLINE = "f16_mixed_x12"
+
+
+def arms(cb):
+    return [("f16_mixed_x12", cb.F16, NRHS), ("f32_mixed_x12", cb.F32, NRHS), ("f16_mixed", cb.F16, 1),
+            ("f32_mixed", cb.F32, 1), ("f64", cb.F64, 1)]
+
+
 def run_ours(args):
+    import ctypes as C
+
     import torch
     import cps_public_b200 as cb
     from cps_public_b200 import _lib
@@ -155,51 +175,59 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     cb.init(local)
     lib = _lib.load()
-    u, srcs = make_inputs(args.steps + args.warmup)
+    npool = NRHS + 4
+    u, srcs = make_inputs(npool)
     g = cb.Gauge(u, DIMS)
     op = cb.DiracOp(g, "dwf", mass=MF, ls=LS, m5=M5)
     n = op.n
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    b_dev = [torch.from_numpy(s).to(dev) for s in srcs]
-    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
-    res = cb.SolveResult()
+    pool = torch.stack([torch.from_numpy(s) for s in srcs]).to(dev)      # npool x n, device resident
+    b_dev = torch.empty((NRHS, n), dtype=torch.float64, device=dev)
+    x_dev = torch.zeros((NRHS, n), dtype=torch.float64, device=dev)
+    res = (cb.SolveResult * NRHS)()
 
-    import ctypes as C
+    def batch(k, nrhs):
+        # step k solves pool rows k, k+1, ... (mod npool): inputs differ from step to step
+        idx = torch.tensor([(k + i) % npool for i in range(nrhs)], device=dev)
+        torch.index_select(pool, 0, idx, out=b_dev[:nrhs])
 
-    def solve_on_device(b, prec):
-        x_dev.zero_()
+    def solve_on_device(nrhs, prec):
+        x_dev[:nrhs].zero_()
         a = cb.CgArg(STOP, 100000, prec, 0.1, 0)
-        rc = lib.cpsb_invcg_dev(g.h, C.byref(op.p), C.byref(a), C.c_void_p(x_dev.data_ptr()),
-                                C.c_void_p(b.data_ptr()), C.byref(res), C.c_void_p(stream.cuda_stream))
+        rc = lib.cpsb_invcg_multi_dev(g.h, C.byref(op.p), C.byref(a), nrhs, C.c_void_p(x_dev.data_ptr()),
+                                      C.c_void_p(b_dev.data_ptr()), res, C.c_void_p(stream.cuda_stream))
         if rc != 0:
-            raise RuntimeError(f"solve failed rc={rc} {res.as_dict()}")
-        return res.as_dict()
+            raise RuntimeError(f"solve failed rc={rc} ({lib.cpsb_last_error().decode()}) {res[0].as_dict()}")
+        return [res[i].as_dict() for i in range(nrhs)]
 
-    variants = {"f16_mixed": cb.F16, "f32_mixed": cb.F32, "f64": cb.F64}
     out = {}
     sampler = ClockSampler(local)
     launches0 = C.c_ulonglong()
     launches1 = C.c_ulonglong()
-    for name, prec in variants.items():
+    clocks = None
+    for name, prec, nrhs in arms(cb):
         for w in range(args.warmup):
-            solve_on_device(b_dev[w % len(b_dev)], prec)
+            batch(w, nrhs)
+            solve_on_device(nrhs, prec)
         torch.cuda.synchronize()
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
-        if name == "f16_mixed":
+        head = name == HEADLINE
+        if head:
             sampler.start()
             lib.cpsb_kernel_launches(C.byref(launches0))
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         infos = []
         torch.cuda.synchronize()
         for k in range(args.steps):
+            batch(args.warmup + k, nrhs)
             ev[k][0].record(stream)
-            infos.append(solve_on_device(b_dev[(args.warmup + k) % len(b_dev)], prec))
+            infos += solve_on_device(nrhs, prec)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
-        if name == "f16_mixed":
+        if head:
             lib.cpsb_kernel_launches(C.byref(launches1))
             clocks = sampler.stop()
         lat = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
@@ -209,55 +237,61 @@ def run_ours(args):
             t = torch.tensor([total_ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             total_ms = float(t.item())
-        out[name] = {"solves_per_s": world * args.steps / (total_ms / 1000.0), "ms_per_step": total_ms / args.steps,
+        out[name] = {"solves_per_s": world * nrhs * args.steps / (total_ms / 1000.0), "rhs_per_solve": nrhs,
+                     "ms_per_step": total_ms / args.steps,
                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                      "iters": int(statistics.median(i["iters"] for i in infos)),
                      "max_true_rsd": max(i["true_rsd"] for i in infos),
                      "reliable_updates": int(statistics.median(i["reliable_updates"] for i in infos))}
-    # e2e: host buffers through the public host-pointer entry point
+        assert out[name]["max_true_rsd"] <= STOP, (name, out[name])
+    head_prec = dict((a[0], a[1]) for a in arms(cb))[HEADLINE]
+    # e2e: host buffers through the public host-pointer entry point (cpsb_invcg_multi):
+    # every step copies the NRHS guesses and sources in and the NRHS solutions out.
     e2e_lat = []
-    for w in range(args.warmup):
-        op.InvCg(srcs[w], stop_rsd=STOP, max_num_iter=100000, precision=cb.F16)
-    for k in range(args.steps):
+    for k in range(args.warmup + args.steps):
+        bs = [srcs[(k + i) % npool] for i in range(NRHS)]
         t0 = time.perf_counter()
-        x, r = op.InvCg(srcs[(args.warmup + k) % len(srcs)], stop_rsd=STOP, max_num_iter=100000, precision=cb.F16)
-        e2e_lat.append(time.perf_counter() - t0)
-        assert r.true_rsd <= STOP
+        xs, rs = op.InvCgMulti(bs, stop_rsd=STOP, max_num_iter=100000, precision=head_prec)
+        if k >= args.warmup:
+            e2e_lat.append(time.perf_counter() - t0)
+        assert max(r.true_rsd for r in rs) <= STOP
     e2e_total = sum(e2e_lat)
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    # Dslash roofline (the dominant kernel of the headline solve: FP16 5-D hop)
+    # Dslash roofline: the 16-bit 5-D hop on NRHS right-hand sides, the dominant
+    # kernel of the headline solve, timed with CUDA events on its stream.
     dsl = {}
     peak, peak_kind = peak_hbm()
-    for pname, prec in (("f16", cb.F16), ("f32", cb.F32), ("f64", cb.F64)):
+    for pname, prec, nr in (("f16_x12", cb.F16, NRHS), ("f16", cb.F16, 1), ("f32", cb.F32, 1), ("f64", cb.F64, 1)):
         ms, by = C.c_double(), C.c_double()
-        lib.cpsb_bench_dslash(g.h, C.byref(op.p), prec, 1, 50, C.byref(ms), C.byref(by))
+        lib.cpsb_bench_dslash(g.h, C.byref(op.p), prec, nr, 50 if nr == 1 else 10, C.byref(ms), C.byref(by))
         gbs = by.value / (ms.value * 1e-3) / 1e9
         dsl[pname] = {"ms": ms.value, "bytes": by.value, "gbs": gbs, "frac": gbs / peak}
     traffic = ncu_traffic()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    head = out["f16_mixed"]
+    head = out[HEADLINE]
     line = {
         "metric": METRIC, "value": head["solves_per_s"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f16-storage/f32-math, f64 reliable updates",
-        "data": "synthetic (seeded reunitarised exp(i*0.2*H) links, Gaussian source)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}"),
+        "data": "synthetic (seeded reunitarised exp(i*0.2*H) links, Gaussian sources)",
+        "config": dict(WORKLOAD, rhs_per_solve=NRHS, parallelism=f"replicas x{world}"),
         "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
         "variants": out,
         "mixed_vs_fp64": head["solves_per_s"] / out["f64"]["solves_per_s"],
-        "e2e": {"value": world * args.steps / e2e_total, "unit": UNIT, "h2d_bytes_per_step": n * 8,
-                "d2h_bytes_per_step": n * 8, "path": "cpsb_invcg (host pointers, pinned staging)"},
-        "roofline": {"bound": "hbm", "achieved": dsl["f16"]["gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": dsl["f16"]["frac"], "peak_kind": peak_kind,
-                     "traffic": (traffic or {}).get("f16_bytes_per_launch"),
-                     "kernel": "dslash_kernel<P16> (5-D Shamir hop, one checkerboard)",
-                     "algorithmic_bytes": dsl["f16"]["bytes"]},
+        "e2e": {"value": world * NRHS * args.steps / e2e_total, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * NRHS * n * 8, "d2h_bytes_per_step": NRHS * n * 8,
+                "path": "cpsb_invcg_multi (host pointers, pinned staging)"},
+        "roofline": {"bound": "hbm", "achieved": dsl["f16_x12"]["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": dsl["f16_x12"]["frac"], "peak_kind": peak_kind,
+                     "traffic": (traffic or {}).get("f16_x12_bytes_per_launch"),
+                     "kernel": f"16-bit 5-D Shamir hop, one checkerboard, {NRHS} right-hand sides",
+                     "algorithmic_bytes": dsl["f16_x12"]["bytes"]},
         "dslash_gbs": {k: v["gbs"] for k, v in dsl.items()},
         "dslash_frac": {k: v["frac"] for k, v in dsl.items()},
         "gpu_launches": int(launches1.value - launches0.value),

@@ -237,7 +237,7 @@ static cudaError_t dslash_launch_v(DslashArgs A, int xpay, int norm, cudaStream_
   if (norm) shm += sizeof(double) * NT * A.g.nrhs;
   if (shm > 200 * 1024) return cudaErrorNotSupported;  // above the opt-in set below
   static bool attr_set[2][2] = {{false, false}, {false, false}};
-  if (shm > 48 * 1024) {
+  if (shm + 1024 > 48 * 1024) {  // the 48 KB default counts static shared memory too
     auto set = [&](const void *f) { return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); };
     cudaError_t e = cudaSuccess;
     if (!attr_set[xpay][norm]) {

@@ -492,7 +492,7 @@ static cudaError_t dslash_x2_launch_v(DslashArgs A, int xpay, int norm, cudaStre
   if (norm) shm += sizeof(double) * NT * A.g.nrhs;
   if (shm > 200 * 1024) return cudaErrorNotSupported;  // above the opt-in set below
   static bool attr_set[2][2] = {{false, false}, {false, false}};
-  if (shm > 48 * 1024) {
+  if (shm + 1024 > 48 * 1024) {  // the 48 KB default counts static shared memory too
     auto set = [&](const void *f) { return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); };
     cudaError_t e = cudaSuccess;
     if (!attr_set[xpay][norm]) {
@@ -626,15 +626,24 @@ template <bool DAG> __device__ __forceinline__ HfX2 umul(const float2 *sh, int T
 
 // DEPTH: neighbours whose loads are issued ahead of the one being computed
 // (0: each is loaded where it is used; 8: all eight at the start of the site).
-template <int P, int NT, int MINB, int SL, int DEPTH, bool XPAY, bool NORM>
+// WG: slice lanes inside one warp.  WG = 1: a warp is 32 consecutive sites of
+// one slice.  WG = SL: a warp is 32/WG consecutive sites x WG slices, so the
+// WG lanes that share a site read the same link words from shared memory
+// (one wavefront serves them) while each slice's sites stay one 16-byte-per-
+// site contiguous segment per chunk.
+template <int P, int NT, int MINB, int SL, int DEPTH, int WG, bool XPAY, bool NORM>
 __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
   constexpr int TX = NT / SL;
+  static_assert(WG == 1 || WG == SL, "slice lanes are either all inside a warp or all across warps");
   const Geom &g = A.g;
   __shared__ double red[NT / 32];
   extern __shared__ double dyn_sh[];
   float2 *lsh = (float2 *)dyn_sh;                       // [8*9][TX]
   double *nrm_sh = dyn_sh + (size_t)72 * TX * sizeof(float2) / sizeof(double);
-  const int tx = threadIdx.x % TX, sl = threadIdx.x / TX;
+  constexpr int GX = 32 / WG;  // consecutive sites per warp and slice lane
+  const int lane = threadIdx.x & 31;
+  const int tx = WG == 1 ? (int)(threadIdx.x % TX) : (int)(threadIdx.x >> 5) * GX + lane % GX;
+  const int sl = WG == 1 ? (int)(threadIdx.x / TX) : lane / GX;
   const int ntiles = (g.n4cb + TX - 1) / TX;
   const int nclass = A.five_d ? 2 : 1;
   const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
@@ -769,7 +778,7 @@ __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
   }
 }
 
-template <int P, int NT, int MINB, int SL, int DEPTH>
+template <int P, int NT, int MINB, int SL, int DEPTH, int WG>
 static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
   constexpr int TX = NT / SL;
   const int nclass = A.five_d ? 2 : 1;
@@ -782,34 +791,35 @@ static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
   if (norm) shm += sizeof(double) * NT * A.g.nrhs;
   if (shm > 200 * 1024) return cudaErrorNotSupported;  // above the opt-in set below
   static bool attr_set[2][2] = {{false, false}, {false, false}};
-  if (shm > 48 * 1024 && !attr_set[xpay][norm]) {
-    const void *f = xpay && norm ? (const void *)kernel<P, NT, MINB, SL, DEPTH, true, true>
-                  : xpay         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, true, false>
-                  : norm         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, false, true>
-                                 : (const void *)kernel<P, NT, MINB, SL, DEPTH, false, false>;
+  if (shm + 1024 > 48 * 1024 && !attr_set[xpay][norm]) {  // the 48 KB default counts static shared memory too
+    const void *f = xpay && norm ? (const void *)kernel<P, NT, MINB, SL, DEPTH, WG, true, true>
+                  : xpay         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, WG, true, false>
+                  : norm         ? (const void *)kernel<P, NT, MINB, SL, DEPTH, WG, false, true>
+                                 : (const void *)kernel<P, NT, MINB, SL, DEPTH, WG, false, false>;
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return e;
     attr_set[xpay][norm] = true;
   }
-  if (xpay && norm) kernel<P, NT, MINB, SL, DEPTH, true, true><<<(unsigned)nb, NT, shm, st>>>(A);
-  else if (xpay) kernel<P, NT, MINB, SL, DEPTH, true, false><<<(unsigned)nb, NT, shm, st>>>(A);
-  else if (norm) kernel<P, NT, MINB, SL, DEPTH, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
-  else kernel<P, NT, MINB, SL, DEPTH, false, false><<<(unsigned)nb, NT, shm, st>>>(A);
+  if (xpay && norm) kernel<P, NT, MINB, SL, DEPTH, WG, true, true><<<(unsigned)nb, NT, shm, st>>>(A);
+  else if (xpay) kernel<P, NT, MINB, SL, DEPTH, WG, true, false><<<(unsigned)nb, NT, shm, st>>>(A);
+  else if (norm) kernel<P, NT, MINB, SL, DEPTH, WG, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
+  else kernel<P, NT, MINB, SL, DEPTH, WG, false, false><<<(unsigned)nb, NT, shm, st>>>(A);
   return launched();
 }
 
 }  // namespace x3
 
 // Launch shapes the autotuner chooses from: 0-6 the kernel above, 7-11 the
-// parity-class kernel with (threads, min blocks/SM, slice lanes, load depth).
+// parity-class kernel with (threads, min blocks/SM, slice lanes, load depth,
+// slice lanes per warp).
 template <int P>
 static cudaError_t dslash_fp32x2_launch(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
   switch (variant) {
-    case 7: return x3::launch_v<P, 128, 3, 4, 8>(A, xpay, norm, st);
-    case 8: return x3::launch_v<P, 128, 4, 4, 8>(A, xpay, norm, st);
-    case 9: return x3::launch_v<P, 128, 4, 4, 0>(A, xpay, norm, st);
-    case 10: return x3::launch_v<P, 128, 3, 4, 4>(A, xpay, norm, st);
-    case 11: return x3::launch_v<P, 128, 4, 4, 2>(A, xpay, norm, st);
+    case 7: return x3::launch_v<P, 128, 4, 4, 8, 4>(A, xpay, norm, st);
+    case 8: return x3::launch_v<P, 128, 4, 4, 8, 1>(A, xpay, norm, st);
+    case 9: return x3::launch_v<P, 128, 4, 2, 8, 2>(A, xpay, norm, st);
+    case 10: return x3::launch_v<P, 128, 3, 4, 8, 4>(A, xpay, norm, st);
+    case 11: return x3::launch_v<P, 128, 4, 4, 2, 4>(A, xpay, norm, st);
     default: return dslash_x2_launch_p<P>(A, xpay, norm, variant, st);
   }
 }

@@ -166,3 +166,24 @@ def test_reduced_precision_operators(action, ls, prec):
     rout, rdot = ref.mdagm(src)
     assert rel(out, rout) < 4 * tol
     assert abs(dot - rdot) < 4 * tol * rdot
+
+
+@pytest.mark.parametrize("prec", ["F16", "F32", "F64"])
+def test_max_rhs_batch(prec):
+    """A batch of MAX_RHS = 16 right-hand sides (the largest per-RHS shared-memory
+    footprint of every launch shape) solves every RHS to its FP64 true residual
+    and agrees with the single-RHS solve."""
+    import cps_public_b200 as cb
+    from cps_public_b200 import fields
+    dims = (8, 8, 8, 8)
+    u = fields.random_gauge(dims, 0.2, 9)
+    cb.init(0)
+    g = cb.Gauge(u, dims)
+    op = cb.DiracOp(g, "dwf", mass=0.05, ls=8)
+    n = op.n // 24
+    srcs = [fields.random_source(n, 500 + i) for i in range(16)]
+    P = getattr(cb, prec)
+    xs, rs = op.InvCgMulti(srcs, stop_rsd=1e-10, precision=P)
+    for i in (0, 7, 15):
+        x1, r1 = op.InvCg(srcs[i], stop_rsd=1e-10, precision=P)
+        assert rs[i].true_rsd <= 1e-10 and rel(xs[i], x1) < 1e-8
