@@ -1,0 +1,159 @@
+"""Benchmarks of the multi-RHS Mobius and the multishift workloads:
+
+  python -m cps_public_b200.config_bench mobius12
+      Mobius DWF (b = 1.5, c = 0.5, SYM2 preconditioning) on 24^3x64, Ls = 16,
+      M5 = 1.8, m_f = 0.005, links reunitarise(exp(i 0.15 H)) seeded: the 12
+      spin-colour point sources at one seeded odd site (4-D source embedded on
+      s = 0 / Ls-1 by chirality) solved in one batched mixed-precision CG
+      (FP32 inner, FP64 reliable updates) to FP64 true residual 1e-10, against
+      the plain FP64 CG on one of the sources.
+
+  python -m cps_public_b200.config_bench multishift
+      Shamir DWF on 24^3x64, Ls = 12, m_f = 0.01, links as above: MInvCG with 12
+      shifts log-spaced in [1e-4, 10], per-shift tolerance 1e-10, Gaussian source;
+      FP32 Krylov vectors with per-shift mixed-precision refinement to the FP64
+      true residual, against the FP64 MInvCG.
+
+Each prints one JSON line: solves/s (right-hand sides or shift systems per
+second) with sources and solutions resident in device memory (the *_dev entry
+points; torch provides the device buffers), the same through the host-pointer
+entry points ("e2e", host copies included), iteration counts and the worst
+FP64 true residual.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import ctypes as C
+
+import numpy as np
+
+from . import F32, F64, MULTI, CgArg, DiracOp, Gauge, SolveResult, _lib, fields, init
+
+DIMS = (24, 24, 24, 64)
+
+
+def mobius12(a):
+    init(0)
+    u = fields.random_gauge(DIMS, 0.15, 2401)
+    g = Gauge(u, DIMS)
+    op = DiracOp(g, "mobius", mass=0.005, ls=16, m5=1.8, b=1.5, c=0.5)
+    rng = np.random.default_rng(2402)
+    while True:  # a seeded site of the solve checkerboard (odd 4-D parity)
+        site = tuple(int(rng.integers(d)) for d in DIMS)
+        if sum(site) % 2 == 1:
+            break
+    srcs = [fields.point_source(DIMS, 16, site, sp, c, cb=1, five_d_parity=False) for sp in range(4) for c in range(3)]
+    import torch
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    nr = len(srcs)
+    b_d = torch.from_numpy(np.stack(srcs)).to(dev)
+    x_d = torch.zeros_like(b_d)
+    res = (SolveResult * nr)()
+
+    def solve_dev(nrhs, prec, maxit):
+        x_d.zero_()
+        torch.cuda.synchronize()
+        arg = CgArg(a.stop, maxit, prec, 0.1, 0)
+        t0 = time.perf_counter()
+        rc = lib.cpsb_invcg_multi_dev(g.h, C.byref(op.p), C.byref(arg), nrhs, C.c_void_p(x_d.data_ptr()),
+                                      C.c_void_p(b_d.data_ptr()), res, None)
+        dt = time.perf_counter() - t0
+        _lib.check(rc, "cpsb_invcg_multi_dev")
+        return dt, [res[i].as_dict() for i in range(nrhs)]
+
+    # warm-up: tunes every launch shape and captures the iteration graphs
+    solve_dev(nr, F32, 40)
+    solve_dev(1, F64, 40)
+    t_mixed, r_mixed = solve_dev(nr, F32, 100000)
+    x_mixed0 = x_d[0].cpu().numpy()
+    t_f64, r_f64 = solve_dev(1, F64, 100000)
+    x64 = x_d[0].cpu().numpy()
+    agree = float(np.linalg.norm(x_mixed0 - x64) / np.linalg.norm(x64))
+    del b_d, x_d
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    xs, rs = op.InvCgMulti(srcs, stop_rsd=a.stop, max_num_iter=100000, precision=F32)
+    t_e2e = time.perf_counter() - t0
+    out = {"workload": "mobius_multi_rhs_24x24x24x64_ls16", "rhs": nr, "site": site,
+           "mixed_f32_x12": {"solves_per_s": nr / t_mixed, "seconds": t_mixed,
+                             "iters": max(r["iters"] for r in r_mixed),
+                             "max_true_rsd": max(r["true_rsd"] for r in r_mixed),
+                             "reliable_updates": max(r["reliable_updates"] for r in r_mixed)},
+           "f64_x1": {"solves_per_s": 1.0 / t_f64, "seconds": t_f64, "iters": r_f64[0]["iters"],
+                      "true_rsd": r_f64[0]["true_rsd"]},
+           "mixed_vs_fp64": (nr / t_mixed) * t_f64,
+           "rhs0_mixed_vs_fp64_rel_diff": agree,
+           "e2e_mixed_f32_x12": {"solves_per_s": nr / t_e2e, "seconds": t_e2e,
+                                 "max_true_rsd": max(r.true_rsd for r in rs),
+                                 "path": "cpsb_invcg_multi (host vectors, copies included)"}}
+    print(json.dumps(out))
+
+
+def multishift(a):
+    init(0)
+    u = fields.random_gauge(DIMS, 0.15, 2403)
+    g = Gauge(u, DIMS)
+    op = DiracOp(g, "dwf", mass=0.01, ls=12, m5=1.8)
+    src = fields.random_source(op.n // 24, 2404)
+    shifts = list(np.logspace(-4, 1, 12))
+    rsd = [a.stop] * 12
+    import torch
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    ns = len(shifts)
+    b_d = torch.from_numpy(src).to(dev)
+    x_d = torch.zeros((ns, op.n), dtype=torch.float64, device=dev)
+    xptr = (C.c_void_p * ns)(*[C.c_void_p(x_d[k].data_ptr()) for k in range(ns)])
+    sh = np.array(shifts)
+    al = np.ones(ns)
+
+    def minv_dev(prec, maxit):
+        rs_ = np.array(rsd, np.float64)
+        arg = CgArg(a.stop, maxit, prec, 0.1, 0)
+        r = SolveResult()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = lib.cpsb_minvcg_dev(g.h, C.byref(op.p), C.byref(arg), xptr, C.c_void_p(b_d.data_ptr()),
+                                 _lib.ptr(sh), ns, _lib.ptr(rs_), MULTI, _lib.ptr(al), C.byref(r), None)
+        dt = time.perf_counter() - t0
+        _lib.check(rc, "cpsb_minvcg_dev")
+        return dt, r, rs_
+
+    minv_dev(F32, 30)   # warm-up / tuning
+    minv_dev(F64, 30)
+    res = {}
+    for name, prec in (("f32_krylov_refined", F32), ("f64", F64)):
+        dt, r, rs_ = minv_dev(prec, 100000)
+        worst = 0.0
+        for k in (0, 5, 11):  # FP64 true residual of the smallest, a middle and the largest shift
+            xk = x_d[k].cpu().numpy()
+            ax, _ = op.MatPcDagMatPc(xk)
+            worst = max(worst, float(np.linalg.norm(src - ax - shifts[k] * xk) / np.linalg.norm(src)))
+        res[name] = {"seconds": dt, "shift_systems_per_s": ns / dt, "iters": r.iters,
+                     "max_reported_rsd": float(np.max(rs_)), "checked_true_rsd": worst}
+    del b_d, x_d
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    op.MInvCG(src, shifts, rsd, ms_type=MULTI, max_num_iter=100000, precision=F32)
+    t_e2e = time.perf_counter() - t0
+    out = {"workload": "dwf_multishift_24x24x24x64_ls12", "shifts": shifts, **res,
+           "mixed_vs_fp64": res["f64"]["seconds"] / res["f32_krylov_refined"]["seconds"],
+           "e2e_f32_krylov_refined": {"seconds": t_e2e, "shift_systems_per_s": ns / t_e2e,
+                                      "path": "cpsb_minvcg (host vectors, copies included)"}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", choices=["mobius12", "multishift"])
+    ap.add_argument("--stop", type=float, default=1e-10)
+    a = ap.parse_args()
+    {"mobius12": mobius12, "multishift": multishift}[a.workload](a)
+
+
+if __name__ == "__main__":
+    main()

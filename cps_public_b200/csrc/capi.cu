@@ -186,21 +186,24 @@ int cpsb_gauge_free(cpsb_gauge h) {
 
 namespace {
 
-// Copies nvec host vectors (each nsites*24 doubles, CPS order) into one device
-// CPS-order buffer, packs it into f (precision f.prec).
+// Copies nvec host vectors (each nsites_each*24 doubles, CPS order) into the
+// multi-RHS field f one right-hand side at a time through a pinned buffer and
+// a device buffer of one vector, packing each into its slice of f.
 void upload(Field &f, const double *const *host, int nvec, long nsites_each, cudaStream_t st) {
   static DevBuf tmp;
   static std::mutex mu;
   std::lock_guard<std::mutex> lk(mu);
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
-  if (tmp.bytes < each * nvec) tmp.alloc(each * nvec);
+  if (tmp.bytes < each) tmp.alloc(each);
   Staging &sg = staging();
   std::lock_guard<std::mutex> lk2(sg.mu);
-  void *pin = sg.get(each * nvec);
-  for (int i = 0; i < nvec; i++) memcpy((char *)pin + i * each, host[i], each);
-  CK(cudaMemcpyAsync(tmp.p, pin, each * nvec, cudaMemcpyHostToDevice, st));
-  CK(launch_pack(f.prec, f.ptr(), (const double *)tmp.p, f.nsites, st));
-  CK(cudaStreamSynchronize(st));
+  void *pin = sg.get(each);
+  for (int i = 0; i < nvec; i++) {
+    memcpy(pin, host[i], each);
+    CK(cudaMemcpyAsync(tmp.p, pin, each, cudaMemcpyHostToDevice, st));
+    CK(launch_pack(f.prec, f.view((long)i * nsites_each), (const double *)tmp.p, nsites_each, st));
+    CK(cudaStreamSynchronize(st));  // pin and tmp are reused by the next vector
+  }
 }
 
 void download(double *const *host, int nvec, long nsites_each, const Field &f, cudaStream_t st) {
@@ -208,14 +211,16 @@ void download(double *const *host, int nvec, long nsites_each, const Field &f, c
   static std::mutex mu;
   std::lock_guard<std::mutex> lk(mu);
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
-  if (tmp.bytes < each * nvec) tmp.alloc(each * nvec);
-  CK(launch_unpack(f.prec, (double *)tmp.p, f.ptr(), f.nsites, st));
+  if (tmp.bytes < each) tmp.alloc(each);
   Staging &sg = staging();
   std::lock_guard<std::mutex> lk2(sg.mu);
-  void *pin = sg.get(each * nvec);
-  CK(cudaMemcpyAsync(pin, tmp.p, each * nvec, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  for (int i = 0; i < nvec; i++) memcpy(host[i], (char *)pin + i * each, each);
+  void *pin = sg.get(each);
+  for (int i = 0; i < nvec; i++) {
+    CK(launch_unpack(f.prec, (double *)tmp.p, f.view((long)i * nsites_each), nsites_each, st));
+    CK(cudaMemcpyAsync(pin, tmp.p, each, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    memcpy(host[i], pin, each);
+  }
 }
 
 }  // namespace
@@ -409,6 +414,38 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
     memset(&r, 0, sizeof(r));
     const int rc = multishift(&h->g, *p, *a, chi, xs, shift, nshift, rsd, type, alpha, &r, st);
     for (int i = 0; i < nvec; i++) download(&x[i], 1, n, xs[i], st);
+    if (res) *res = r;
+    return rc;
+  });
+}
+
+int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *const *x,
+                    const double *b, const double *shift, int nshift, double *rsd, int type, const double *alpha,
+                    cpsb_solve_result *res, void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (!x || !b || !shift || !rsd || nshift < 1 || nshift > 32) throw Error{CPSB_ERR_ARG, "bad multishift arguments"};
+    if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE are implemented"};
+    if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
+    const int nvec = type == CPSB_SINGLE ? 1 : nshift;
+    for (int i = 0; i < nvec; i++)
+      if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    const long n = cb_sites(h, p);
+    Field chi(P64, n);
+    CK(launch_pack(P64, chi.ptr(), b, n, st));
+    std::vector<Field> xs(nvec);
+    for (int i = 0; i < nvec; i++) {
+      xs[i].create(P64, n);
+      CK(cudaMemsetAsync(xs[i].data.p, 0, xs[i].data.bytes, st));
+    }
+    cpsb_solve_result r;
+    memset(&r, 0, sizeof(r));
+    const int rc = multishift(&h->g, *p, *a, chi, xs, shift, nshift, rsd, type, alpha, &r, st);
+    for (int i = 0; i < nvec; i++) CK(launch_unpack(P64, x[i], xs[i].ptr(), n, st));
+    CK(cudaStreamSynchronize(st));
     if (res) *res = r;
     return rc;
   });

@@ -818,8 +818,8 @@ static cudaError_t dslash_fp32x2_launch(const DslashArgs &A, int xpay, int norm,
     case 7: return x3::launch_v<P, 128, 4, 4, 8, 4>(A, xpay, norm, st);
     case 8: return x3::launch_v<P, 128, 4, 4, 8, 1>(A, xpay, norm, st);
     case 9: return x3::launch_v<P, 128, 4, 2, 8, 2>(A, xpay, norm, st);
-    case 10: return x3::launch_v<P, 128, 3, 4, 8, 4>(A, xpay, norm, st);
-    case 11: return x3::launch_v<P, 128, 4, 4, 2, 4>(A, xpay, norm, st);
+    case 10: return x3::launch_v<P, 128, 5, 4, 2, 4>(A, xpay, norm, st);
+    case 11: return x3::launch_v<P, 128, 6, 4, 2, 4>(A, xpay, norm, st);
     default: return dslash_x2_launch_p<P>(A, xpay, norm, variant, st);
   }
 }

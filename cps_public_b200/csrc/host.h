@@ -66,6 +66,12 @@ struct Field {
   Field(int prec, long nsites) { create(prec, nsites); }
   void create(int prec, long nsites);
   SpinorPtr ptr() const { return SpinorPtr{data.p, (float *)norm.p, nsites}; }
+  // The sites [off, off + n) of the field as a field of its own (same chunk
+  // stride): one right-hand side of a multi-RHS field.  Chunks are 16 bytes
+  // in every precision.
+  SpinorPtr view(long off) const {
+    return SpinorPtr{(char *)data.p + off * 16, norm.p ? (float *)norm.p + off : nullptr, nsites};
+  }
   size_t bytes() const { return data.bytes + norm.bytes; }
 };
 size_t field_bytes(int prec, long nsites);
@@ -91,15 +97,30 @@ struct Operator {
 
   Operator(Gauge *G, const cpsb_dirac_params &p, int prec, int nrhs);
   long nsites() const { return geom.nsites; }
-  // out = a * D(cb, dag) in [+ x] with optional |out|^2 into red.
-  void hop(const Field &out, const Field &in, int cb, int dag, double a, const Field *x, const Reduce *red,
-           const int *skip, cudaStream_t st);
+  // out = a * D(cb, dag) in [+ x] with optional |out|^2 into red.  Vectors are
+  // views (SpinorPtr) with nsites() sites each; the Field forms pass whole fields.
+  void hop(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, double a, const SpinorPtr *x,
+           const Reduce *red, const int *skip, cudaStream_t st);
   // DiracOp::Dslash front end
-  void dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st);
+  void dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, cudaStream_t st);
   // out = MatPc in (dag 0) or MatPcDag in (dag 1); |out|^2 into red when given.
-  void matpc(const Field &out, const Field &in, int dag, const Reduce *red, const int *skip, cudaStream_t st);
+  void matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip, cudaStream_t st);
   // out = MatPcDagMatPc in; |MatPc in|^2 into red when given.
-  void mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st);
+  void mdagm(const SpinorPtr &out, const SpinorPtr &in, const Reduce *red, const int *skip, cudaStream_t st);
+  void hop(const Field &out, const Field &in, int cb, int dag, double a, const Field *x, const Reduce *red,
+           const int *skip, cudaStream_t st) {
+    const SpinorPtr xp = x ? x->ptr() : SpinorPtr{};
+    hop(out.ptr(), in.ptr(), cb, dag, a, x ? &xp : nullptr, red, skip, st);
+  }
+  void dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st) {
+    dslash(out.ptr(), in.ptr(), cb, dag, st);
+  }
+  void matpc(const Field &out, const Field &in, int dag, const Reduce *red, const int *skip, cudaStream_t st) {
+    matpc(out.ptr(), in.ptr(), dag, red, skip, st);
+  }
+  void mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st) {
+    mdagm(out.ptr(), in.ptr(), red, skip, st);
+  }
   // Bytes one hop application must move (spinors in + out + links), for the roofline.
   double hop_bytes() const;
 };
@@ -110,8 +131,9 @@ struct CgSolver {
   cpsb_dirac_params p;
   int sloppy;
   int nrhs;
-  std::unique_ptr<Operator> op64, opS;
-  Field x64, b64, r64, Ap64;          // FP64 (x64/b64 are the caller's vectors packed)
+  std::unique_ptr<Operator> op64, opS;  // op64: one RHS (applied per RHS) when sloppy != P64
+  Geom geom;                           // all right-hand sides
+  Field x64, b64, r64;                // FP64 (x64/b64 are the caller's vectors packed; r64 = b - A x)
   Field rS, pS, ApS, xS;              // sloppy (xS is FP32 when sloppy is FP16)
   DevBuf state;                       // CgState
   CgState *hstate = nullptr;          // pinned mirror

@@ -75,7 +75,11 @@ RedSlot::RedSlot() {
   // partials: grid_blocks cap (148*16) * MAX_RHS; + ticket + padding
   const size_t nparts = 148 * 16 * MAX_RHS;
   buf.alloc(nparts * sizeof(double) + 256);
+  // The ticket must be zero before the first kernel that uses the slot runs.
+  // cudaMemset goes to the legacy stream, which does not order against the
+  // library's non-blocking streams, so wait for it here.
   CK(cudaMemset(buf.p, 0, buf.bytes));
+  CK(cudaStreamSynchronize(cudaStreamLegacy));
 }
 Reduce RedSlot::r(double *result) {
   Reduce q;
@@ -189,15 +193,15 @@ double Operator::hop_bytes() const {
   return 2.0 * spin * (double)geom.nsites + link * 4.0 * 2.0 * (double)geom.n4cb;
 }
 
-void Operator::hop(const Field &out, const Field &in, int cb, int dag, double a, const Field *x, const Reduce *red,
-                   const int *skip, cudaStream_t st) {
+void Operator::hop(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, double a, const SpinorPtr *x,
+                   const Reduce *red, const int *skip, cudaStream_t st) {
   DslashArgs A;
   memset(&A, 0, sizeof(A));
   A.g = geom;
   A.U = G->ptr(prec);
-  A.in = in.ptr();
-  A.out = out.ptr();
-  if (x) A.x = x->ptr();
+  A.in = in;
+  A.out = out;
+  if (x) A.x = *x;
   A.cb = cb;
   A.dag = dag;
   A.five_d = p.action == CPSB_DWF;
@@ -212,7 +216,7 @@ void Operator::hop(const Field &out, const Field &in, int cb, int dag, double a,
   CK(launch_dslash(prec, A, x != nullptr, red != nullptr, v, st));
 }
 
-void Operator::dslash(const Field &out, const Field &in, int cb, int dag, cudaStream_t st) {
+void Operator::dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, cudaStream_t st) {
   if (p.action != CPSB_MOBIUS) {
     hop(out, in, cb, dag, 1.0, nullptr, nullptr, nullptr, st);
     return;
@@ -230,48 +234,48 @@ void Operator::dslash(const Field &out, const Field &in, int cb, int dag, cudaSt
   Reduce none;
   memset(&none, 0, sizeof(none));
   if (!dag) {
-    CK(launch_m5(prec, 0, geom, t1.ptr(), in.ptr(), SpinorPtr{}, mix, 0, 0, none, nullptr, st));
-    hop(out, t1, cb, 0, 1.0, nullptr, nullptr, nullptr, st);
+    CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, mix, 0, 0, none, nullptr, st));
+    hop(out, t1.ptr(), cb, 0, 1.0, nullptr, nullptr, nullptr, st);
   } else {
-    hop(t1, in, cb, 1, 1.0, nullptr, nullptr, nullptr, st);
-    CK(launch_m5(prec, 1, geom, out.ptr(), t1.ptr(), SpinorPtr{}, mix, 0, 0, none, nullptr, st));
+    hop(t1.ptr(), in, cb, 1, 1.0, nullptr, nullptr, nullptr, st);
+    CK(launch_m5(prec, 1, geom, out, t1.ptr(), SpinorPtr{}, mix, 0, 0, none, nullptr, st));
   }
   const double kappa_c = 1.0 / (2 * (p.mobius_c * (4 - p.m5) - p.a5_inv));
   M5Coef h5 = mix;
   h5.b = 0.0;
   h5.c = 1.0 / kappa_c;
   // out = out + H5(in): the m5 kernel in xpay mode (K = 0 makes the sweep the identity)
-  CK(launch_m5(prec, dag, geom, out.ptr(), in.ptr(), out.ptr(), h5, 1, 0, none, nullptr, st));
+  CK(launch_m5(prec, dag, geom, out, in, out, h5, 1, 0, none, nullptr, st));
 }
 
-void Operator::matpc(const Field &out, const Field &in, int dag, const Reduce *red, const int *skip,
+void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
                      cudaStream_t st) {
   if (p.action != CPSB_MOBIUS) {
-    hop(t1, in, 1, dag, 1.0, nullptr, nullptr, skip, st);
-    hop(out, t1, 0, dag, -kappa * kappa, &in, red, skip, st);
+    hop(t1.ptr(), in, 1, dag, 1.0, nullptr, nullptr, skip, st);
+    hop(out, t1.ptr(), 0, dag, -kappa * kappa, &in, red, skip, st);
     return;
   }
   Reduce none;
   memset(&none, 0, sizeof(none));
   if (!dag) {
-    CK(launch_m5(prec, 0, geom, t1.ptr(), in.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
-    hop(t3, t1, 1, 0, kappa_b, nullptr, nullptr, skip, st);
+    CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
+    hop(t3.ptr(), t1.ptr(), 1, 0, kappa_b, nullptr, nullptr, skip, st);
     CK(launch_m5(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
-    hop(out, t1, 0, 0, -kappa_b, &in, red, skip, st);
+    hop(out, t1.ptr(), 0, 0, -kappa_b, &in, red, skip, st);
   } else {
-    hop(t1, in, 1, 1, -kappa_b, nullptr, nullptr, skip, st);
+    hop(t1.ptr(), in, 1, 1, -kappa_b, nullptr, nullptr, skip, st);
     M5Coef c = m5c[1];
     c.scale = kappa_b;
     CK(launch_m5(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, c, 0, 0, none, skip, st));
-    hop(t1, t3, 0, 1, 1.0, nullptr, nullptr, skip, st);
-    CK(launch_m5(prec, 1, geom, out.ptr(), t1.ptr(), in.ptr(), m5c[1], 1, red != nullptr, red ? *red : none, skip,
+    hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+    CK(launch_m5(prec, 1, geom, out, t1.ptr(), in, m5c[1], 1, red != nullptr, red ? *red : none, skip,
                  st));
   }
 }
 
-void Operator::mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st) {
-  matpc(t2, in, 0, red, skip, st);
-  matpc(out, t2, 1, nullptr, skip, st);
+void Operator::mdagm(const SpinorPtr &out, const SpinorPtr &in, const Reduce *red, const int *skip, cudaStream_t st) {
+  matpc(t2.ptr(), in, 0, red, skip, st);
+  matpc(out, t2.ptr(), 1, nullptr, skip, st);
 }
 
 }  // namespace cpsb

@@ -42,17 +42,18 @@ static double now_ms() {
 }
 
 // Device bytes a CgSolver for nrhs right-hand sides of n sites each holds,
-// plus the CPS-order FP64 staging buffer of the work item.
+// plus the one-vector CPS-order FP64 staging buffer of the work item.
 static size_t solve_footprint(const cpsb_dirac_params &p, long n, int sloppy, int nrhs) {
   const long N = n * nrhs;
-  const int op_tmp = p.action == CPSB_MOBIUS ? 3 : 2;  // Operator::t1, t2 (t3 for Mobius)
-  size_t b = field_bytes(P64, N) * (4 + op_tmp + 1);    // x, b, r, Ap; operator temporaries; staging
+  const int op_tmp = p.action == CPSB_MOBIUS ? 3 : 2;   // Operator::t1, t2 (t3 for Mobius)
+  size_t b = field_bytes(P64, N) * 3 + field_bytes(P64, n);  // x, b, r; staging
   if (sloppy == P64) {
-    b += field_bytes(P64, N) * 3;                       // r, p, Ap of the FP64 recurrence
+    b += field_bytes(P64, N) * (3 + op_tmp);             // r, p, Ap; temporaries of the FP64 operator
   } else {
+    b += field_bytes(P64, n) * op_tmp;                   // one-RHS FP64 operator (true residuals)
     b += field_bytes(sloppy, N) * (3 + op_tmp) + field_bytes(P32, N);  // r, p, Ap, temporaries; x
   }
-  return b + (size_t)(8u << 20);                        // reduction slots, state, graph
+  return b + (size_t)(8u << 20);                         // reduction slots, state, graph
 }
 
 struct ServeRequest {
@@ -122,17 +123,18 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
   const long n = cb_sites(r.h, &r.p);
   const size_t each = (size_t)n * 24 * sizeof(double);
   CgSolver s(G, r.p, r.a.precision, it.nrhs);
-  DevBuf stage(each * it.nrhs);
-  for (int q = 0; q < it.nrhs; q++)
-    CK(cudaMemcpyAsync((char *)stage.p + q * each, r.x[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
-  CK(launch_pack(P64, s.x64.ptr(), (const double *)stage.p, s.x64.nsites, st));
-  for (int q = 0; q < it.nrhs; q++)
-    CK(cudaMemcpyAsync((char *)stage.p + q * each, r.b[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
-  CK(launch_pack(P64, s.b64.ptr(), (const double *)stage.p, s.b64.nsites, st));
+  DevBuf stage(each);
+  for (int q = 0; q < it.nrhs; q++) {
+    CK(cudaMemcpyAsync(stage.p, r.x[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
+    CK(launch_pack(P64, s.x64.view((long)q * n), (const double *)stage.p, n, st));
+    CK(cudaMemcpyAsync(stage.p, r.b[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
+    CK(launch_pack(P64, s.b64.view((long)q * n), (const double *)stage.p, n, st));
+  }
   const int rc = s.solve(r.a, r.res.data() + it.rhs0, st);
-  CK(launch_unpack(P64, (double *)stage.p, s.x64.ptr(), s.x64.nsites, st));
-  for (int q = 0; q < it.nrhs; q++)
-    CK(cudaMemcpyAsync(r.x[it.rhs0 + q], (char *)stage.p + q * each, each, cudaMemcpyDeviceToHost, st));
+  for (int q = 0; q < it.nrhs; q++) {
+    CK(launch_unpack(P64, (double *)stage.p, s.x64.view((long)q * n), n, st));
+    CK(cudaMemcpyAsync(r.x[it.rhs0 + q], stage.p, each, cudaMemcpyDeviceToHost, st));
+  }
   CK(cudaStreamSynchronize(st));
   if (rc != CPSB_OK) throw Error{rc, "solve did not converge"};
 }

@@ -25,12 +25,17 @@
 namespace cpsb {
 
 CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g), p(pp), sloppy(sl), nrhs(nr) {
-  op64.reset(new Operator(G, p, P64, nrhs));
-  const long n = op64->nsites();
+  // The FP64 operator serves the FP64 recurrence (all right-hand sides at once)
+  // or, for mixed precision, only the true residuals, which it forms one
+  // right-hand side at a time so that its temporaries are one vector each.
+  op64.reset(new Operator(G, p, P64, sl == P64 ? nr : 1));
+  geom = op64->geom;
+  geom.nrhs = nr;
+  geom.nsites = op64->geom.nsites / op64->geom.nrhs * nr;
+  const long n = geom.nsites;
   x64.create(P64, n);
   b64.create(P64, n);
   r64.create(P64, n);
-  Ap64.create(P64, n);
   if (sloppy != P64) {
     opS.reset(new Operator(G, p, sloppy, nrhs));
     G->ptr(sloppy);  // build the reduced-precision links now, never inside a graph capture
@@ -129,15 +134,21 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
 void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t st) {
   (void)bnorm;
   double *dres = (double *)scal.p;
-  op64->mdagm(Ap64, x64, nullptr, nullptr, st);
+  // r = b - (A + shift) x, formed in place in r (no separate A x vector)
+  if (op64->nrhs == nrhs) {
+    op64->mdagm(r64, x64, nullptr, nullptr, st);
+  } else {
+    const long n1 = op64->nsites();
+    for (int q = 0; q < nrhs; q++) op64->mdagm(r64.view(q * n1), x64.view(q * n1), nullptr, nullptr, st);
+  }
   Reduce rm = red_misc.r(dres);
   if (shift != 0.0) {
     Reduce none;
     memset(&none, 0, sizeof(none));
-    CK(launch_axpby(P64, Ap64.ptr(), P64, Ap64.ptr(), P64, x64.ptr(), op64->geom, sc2(nrhs, 1.0, shift), nullptr,
+    CK(launch_axpby(P64, r64.ptr(), P64, r64.ptr(), P64, x64.ptr(), geom, sc2(nrhs, 1.0, shift), nullptr,
                     none, 0, st));
   }
-  CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, Ap64.ptr(), op64->geom, sc2(nrhs, 1.0, -1.0), nullptr, rm, 1,
+  CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, r64.ptr(), geom, sc2(nrhs, 1.0, -1.0), nullptr, rm, 1,
                   st));
   CK(cudaMemcpyAsync(rr_out, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -146,7 +157,7 @@ void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t s
 int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma) {
   auto t0 = std::chrono::steady_clock::now();
   shift = sigma;
-  const Geom &gg = op64->geom;
+  const Geom &gg = geom;
   double bnorm[MAX_RHS], rr[MAX_RHS];
   double *dres = (double *)scal.p;
   // |b|^2

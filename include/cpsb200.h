@@ -151,6 +151,11 @@ int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg
                          const double *b, cpsb_solve_result *res, void *stream);
 int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
                    void *stream);
+/* cpsb_minvcg with b and the solutions x[s] in device memory (x: host array of
+ * device pointers). */
+int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *const *x,
+                    const double *b, const double *shift, int nshift, double *rsd, int type, const double *alpha,
+                    cpsb_solve_result *res, void *stream);
 
 /* Dslash and MatPcDagMatPc evaluated with fields and links stored in the
  * given precision (CPSB_PREC_F32: FP32 spinors, recon-12 FP32 links;

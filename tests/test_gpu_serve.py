@@ -76,7 +76,7 @@ def test_admission_budget_splits_requests(setup):
     cb, _, reqs = setup
     op, srcs, tol, prec = reqs[5]           # 8^4, Ls 4, four right-hand sides, 16-bit inner
     n = op.n // 24
-    one_rhs = n * (192 * 5 + 192 * 2 + 52 * 5 + 96) + (8 << 20)  # footprint of one RHS (serve.cu)
+    one_rhs = n * (192 * 6 + 52 * 5 + 96) + (8 << 20)  # footprint of one RHS (serve.cu)
     srv = cb.Server(slots=4, hbm_bytes=one_rhs + (1 << 20))
     rid = srv.submit(op, srcs, stop_rsd=tol, precision=prec)
     xs, rs, _ = srv.wait(rid)
