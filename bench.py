@@ -69,6 +69,24 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(value: float, device=None) -> float:
+    """The maximum of a per-rank number over all ranks (identity without a
+    process group): every multi-GPU time in this file is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rate(units_per_rank: float, world: int, max_seconds: float) -> float:
+    """Whole-job throughput of independent replicas: all ranks' units over the
+    slowest rank's time."""
+    return world * units_per_rank / max_seconds
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -231,13 +249,8 @@ def run_ours(args):
             lib.cpsb_kernel_launches(C.byref(launches1))
             clocks = sampler.stop()
         lat = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
-        total_ms = ev[0][0].elapsed_time(ev[-1][1])
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-        out[name] = {"solves_per_s": world * nrhs * args.steps / (total_ms / 1000.0), "rhs_per_solve": nrhs,
+        total_ms = max_over_ranks(ev[0][0].elapsed_time(ev[-1][1]), dev)
+        out[name] = {"solves_per_s": rate(nrhs * args.steps, world, total_ms / 1000.0), "rhs_per_solve": nrhs,
                      "ms_per_step": total_ms / args.steps,
                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                      "iters": int(statistics.median(i["iters"] for i in infos)),
@@ -255,12 +268,7 @@ def run_ours(args):
         if k >= args.warmup:
             e2e_lat.append(time.perf_counter() - t0)
         assert max(r.true_rsd for r in rs) <= STOP
-    e2e_total = sum(e2e_lat)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(sum(e2e_lat), dev)
     # Dslash roofline: the 16-bit 5-D hop on NRHS right-hand sides, the dominant
     # kernel of the headline solve, timed with CUDA events on its stream.
     dsl = {}
@@ -284,7 +292,7 @@ def run_ours(args):
         "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
         "variants": out,
         "mixed_vs_fp64": head["solves_per_s"] / out["f64"]["solves_per_s"],
-        "e2e": {"value": world * NRHS * args.steps / e2e_total, "unit": UNIT,
+        "e2e": {"value": rate(NRHS * args.steps, world, e2e_total), "unit": UNIT,
                 "h2d_bytes_per_step": 2 * NRHS * n * 8, "d2h_bytes_per_step": NRHS * n * 8,
                 "path": "cpsb_invcg_multi (host pointers, pinned staging)"},
         "roofline": {"bound": "hbm", "achieved": dsl["f16_x12"]["gbs"], "peak": peak, "unit": "GB/s",
