@@ -5,8 +5,8 @@ Python front end of libcpsb200.so, mirroring the CPS interfaces it replaces:
 * ``Gauge``        resident gauge field (the gauge half of the DiracOp constructor)
 * ``DiracOp``      Dslash / MatPc / MatPcDag / MatPcDagMatPc / InvCg / MInvCG for the
                    Wilson, DWF and Mobius actions (cps_pp/include/util/dirac_op.h)
-* ``fmat_evl_inv`` / ``fmat_evl_minv``  the Lattice::FmatEvlInv / FmatEvlMInv entry
-                   points (cps_pp/include/util/lattice.h:942,976)
+* ``fmat_evl_inv`` / ``fmat_evl_minv`` / ``fmat_inv``  the Lattice::FmatEvlInv /
+                   FmatEvlMInv / FmatInv entry points (cps_pp/include/util/lattice.h:942,976,1114)
 
 All compute runs in the CUDA library; this module only marshals numpy arrays.
 """
@@ -159,6 +159,22 @@ class DiracOp:
               "cpsb_invcg_multi")
         return xs, list(res)
 
+    def MatInv(self, src_full, guess_full=None, stop_rsd=1e-10, max_num_iter=5000, precision=F64,
+               reliable_delta=0.1, batch=0):
+        """Full-lattice solve M out = in (DiracOp*::MatInv); vectors hold both
+        checkerboards (Wilson/DWF odd half first, Mobius even half first).
+        Returns (out, SolveResult of the preconditioned CG)."""
+        src = np.ascontiguousarray(src_full, np.float64)
+        if src.size != 2 * self.n:
+            raise ValueError(f"full vector has {src.size} reals, expected {2 * self.n}")
+        out = np.zeros(2 * self.n) if guess_full is None else np.array(guess_full, np.float64)
+        a = CgArg(stop_rsd, max_num_iter, precision, reliable_delta, batch)
+        r = SolveResult()
+        rc = check(_lib.load().cpsb_matinv(self.gauge.h, C.byref(self.p), C.byref(a), ptr(out), ptr(src),
+                                           C.byref(r)), "cpsb_matinv")
+        r.rc = rc
+        return out, r
+
     def MInvCG(self, src, shifts, rsd, ms_type=MULTI, alpha=None, max_num_iter=5000, precision=F64):
         ns = len(shifts)
         nvec = 1 if ms_type == SINGLE else ns
@@ -180,6 +196,13 @@ def fmat_evl_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
     x, r = op.InvCg(f_in, cg_arg.get("stop_rsd", 1e-10), cg_arg.get("max_num_iter", 5000),
                     cg_arg.get("precision", F64), guess=f_out)
     return r.iters, x, r.true_rsd
+
+
+def fmat_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
+    """Lattice::FmatInv (lattice.h:1114): full-lattice solve; returns (iterations, f_out, true_res)."""
+    out, r = op.MatInv(f_in, f_out, cg_arg.get("stop_rsd", 1e-10), cg_arg.get("max_num_iter", 5000),
+                       cg_arg.get("precision", F64))
+    return r.iters, out, r.true_rsd
 
 
 def fmat_evl_minv(op: DiracOp, f_in, shifts, cg_args, ms_type=MULTI, alpha=None):

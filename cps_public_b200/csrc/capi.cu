@@ -451,6 +451,76 @@ int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg 
   });
 }
 
+int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
+                cpsb_solve_result *res) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (!out || !in || !res) throw Error{CPSB_ERR_ARG, "null vector or result"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    const long n = op.nsites();
+    const Geom &g = op.geom;
+    // solve-checkerboard (c) and other (e) halves of the full vectors
+    const bool mob = p->action == CPSB_MOBIUS;
+    const double *in_c = in + (mob ? 24 * n : 0), *in_e = in + (mob ? 0 : 24 * n);
+    double *out_c = out + (mob ? 24 * n : 0), *out_e = out + (mob ? 0 : 24 * n);
+    Field fin_c(P64, n), fin_e(P64, n), fout_c(P64, n), fout_e(P64, n), t(P64, n), t2(P64, n);
+    upload(fin_c, &in_c, 1, n, st);
+    upload(fin_e, &in_e, 1, n, st);
+    upload(fout_c, (const double *const *)&out_c, 1, n, st);
+    Reduce none;
+    memset(&none, 0, sizeof(none));
+    auto lin = [&](const Field &o, double fa, const Field &x, double fb, const Field *y) {
+      Scal2 c;
+      for (int i = 0; i < MAX_RHS; i++) {
+        c.a[i] = fa;
+        c.b[i] = fb;
+      }
+      CK(launch_axpby(P64, o.ptr(), P64, x.ptr(), P64, y ? y->ptr() : SpinorPtr{}, g, c, nullptr, none, 0, st));
+    };
+    double kb = 0;
+    if (!mob) {
+      // d_op_wilson.C:257-334, d_op_dwf.C:316-507
+      op.dslash(t, fin_e, 0, 0, st);
+      lin(t, op.kappa, t, 1.0, &fin_c);        // t = kappa D in_e + in_o
+    } else {
+      // d_op_mobius.C:389-640, ZMOB_PC_SYM2
+      kb = op.kappa_b;
+      op.mobius_m5inv(t.ptr(), fin_e.ptr(), st);
+      op.mobius_d4(t2.ptr(), t.ptr(), 0, st);
+      lin(t, kb, t2, 1.0, &fin_c);             // t = kappa_b D4 M5^-1 in_e + in_o
+      CK(cudaMemcpyAsync(t2.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
+      const double kappa_c = 1.0 / (2 * (p->mobius_c * (4 - p->m5) - p->a5_inv));
+      op.mobius_hop5_add(fout_c.ptr(), t2.ptr(), t2.ptr(), kb / kappa_c, st);  // SYM2 guess
+    }
+    CgSolver *s = get_solver(&h->g, *p, a->precision, 1);
+    std::lock_guard<std::mutex> lk(s->busy);
+    op.matpc(s->b64, t, 1, nullptr, nullptr, st);  // src = MatPcDag t
+    CK(cudaMemcpyAsync(s->x64.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
+    const int rc = s->solve(*a, res, st);
+    CK(cudaMemcpyAsync(fout_c.data.p, s->x64.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
+    if (!mob) {
+      op.dslash(t, fout_c, 1, 0, st);
+      lin(fout_e, op.kappa, t, 1.0, &fin_e);   // out_e = kappa D out_o + in_e
+    } else {
+      op.mobius_m5inv(t.ptr(), fout_c.ptr(), st);
+      CK(cudaMemcpyAsync(fout_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      op.mobius_d4(t.ptr(), fout_c.ptr(), 1, st);
+      lin(t2, kb, t, 0.0, nullptr);            // kappa_b D4 out_o
+      op.mobius_m5inv(fout_e.ptr(), t2.ptr(), st);
+      op.mobius_m5inv(t.ptr(), fin_e.ptr(), st);
+      lin(fout_e, 1.0, fout_e, 1.0, &t);       // + M5^-1 in_e
+      lin(fout_e, 2 * kb, fout_e, 0.0, nullptr);
+      lin(fout_c, 2 * kb, fout_c, 0.0, nullptr);
+    }
+    download(&out_c, 1, n, fout_c, st);
+    download(&out_e, 1, n, fout_e, st);
+    return rc;
+  });
+}
+
 int cpsb_kernel_launches(unsigned long long *count) {
   if (!count) return CPSB_ERR_ARG;
   *count = launch_count();

@@ -121,6 +121,12 @@ struct Operator {
   void mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st) {
     mdagm(out.ptr(), in.ptr(), red, skip, st);
   }
+  // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
+  // (zmobius_m5inv, dag 0); out = D4(cb) in (zmobius_dslash_4, dag 0);
+  // out = x + f H5 in (zmobius_kappa_dslash_5_plus_cmplx with factor f, dag 0).
+  void mobius_m5inv(const SpinorPtr &out, const SpinorPtr &in, cudaStream_t st);
+  void mobius_d4(const SpinorPtr &out, const SpinorPtr &in, int cb, cudaStream_t st);
+  void mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const SpinorPtr &x, double f, cudaStream_t st);
   // Bytes one hop application must move (spinors in + out + links), for the roofline.
   double hop_bytes() const;
 };

@@ -273,6 +273,44 @@ void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const R
   }
 }
 
+void Operator::mobius_m5inv(const SpinorPtr &out, const SpinorPtr &in, cudaStream_t st) {
+  M5Coef c = m5c[0];
+  c.b = 1.0;  // no mixing after the sweeps
+  c.c = 0.0;
+  c.scale = 1.0;
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  CK(launch_m5(prec, 0, geom, out, in, SpinorPtr{}, c, 0, 0, none, nullptr, st));
+}
+
+void Operator::mobius_d4(const SpinorPtr &out, const SpinorPtr &in, int cb, cudaStream_t st) {
+  M5Coef mix;  // K = 0: the sweeps are the identity, leaving b in + c H5 in
+  memset(&mix, 0, sizeof(mix));
+  mix.invd = 1.0;
+  mix.b = p.mobius_b;
+  mix.c = p.mobius_c;
+  mix.mass = p.mass;
+  mix.scale = 1.0;
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, mix, 0, 0, none, nullptr, st));
+  hop(out, t1.ptr(), cb, 0, 1.0, nullptr, nullptr, nullptr, st);
+}
+
+void Operator::mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const SpinorPtr &x, double f,
+                               cudaStream_t st) {
+  M5Coef h;
+  memset(&h, 0, sizeof(h));
+  h.invd = 1.0;
+  h.b = 0.0;
+  h.c = f;
+  h.mass = p.mass;
+  h.scale = 1.0;
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  CK(launch_m5(prec, 0, geom, out, in, x, h, 1, 0, none, nullptr, st));
+}
+
 void Operator::mdagm(const SpinorPtr &out, const SpinorPtr &in, const Reduce *red, const int *skip, cudaStream_t st) {
   matpc(t2.ptr(), in, 0, red, skip, st);
   matpc(out, t2.ptr(), 1, nullptr, skip, st);

@@ -142,6 +142,17 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
                 const double *shift, int nshift, double *rsd, int type, const double *alpha,
                 cpsb_solve_result *res);
 
+/* DiracOp*::MatInv(out, in, true_res, PRESERVE_YES) (include/util/dirac_op.h:294)
+ * and Lattice::FmatInv (lattice.h:1114): the full-lattice solve.  in, out are
+ * full vectors of both checkerboards in the action's order (Wilson, DWF: odd
+ * half first, d_op_wilson.C:284-287, d_op_dwf.C:316-507; Mobius: even half first,
+ * d_op_mobius.C:389-640, ZMOB_PC_SYM2 only).  The solve-checkerboard half of out
+ * is the CG's initial guess on entry.  Source preparation, MatPcDag, the CG (of
+ * the requested precision) and the reconstruction of the other checkerboard run
+ * on the device; res reports the CG as cpsb_invcg does. */
+int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
+                cpsb_solve_result *res);
+
 /* Device-resident variants: x, b (and out/in) are device pointers holding CPS
  * order vectors; stream is a cudaStream_t (NULL = the library stream).  These
  * are what a caller with fields already in HBM uses. */

@@ -785,3 +785,77 @@ int orc_minvcg(const orc_op *op, double **psi, const double *chi, double chi_nor
   free(rsd_sq);
   return k;
 }
+
+/* ------------------------------------------------------------------ */
+/* Full-lattice solve: DiracOp*::MatInv with the source preserved      */
+/* ------------------------------------------------------------------ */
+/* out/in: full vectors of 2 checkerboards.  Wilson / DWF order odd half first
+ * (d_op_wilson.C:257-334, d_op_dwf.C:316-507):
+ *   t = kappa D(in_e, CHKB_EVEN) + in_o;  src = MatPcDag t;  CG on
+ *   MatPcDagMatPc out_o = src from the guess in out_o;
+ *   out_e = kappa D(out_o, CHKB_ODD) + in_e.
+ * Mobius (SYM2) order even half first (d_op_mobius.C:389-640):
+ *   t = kappa_b D4(M5^-1 in_e, CHKB_EVEN) + in_o;  out_o += (kappa_b/kappa_c)-weighted
+ *   5th-direction hop of the guess;  src = MatPcDag t;  CG;
+ *   out_o = M5^-1 out_o;  out_e = M5^-1 (kappa_b D4(out_o, CHKB_ODD)) + M5^-1 in_e;
+ *   out *= 2 kappa_b.
+ * Returns the CG iteration count; *true_res as InvCg reports it. */
+int orc_matinv(const orc_op *op, double *out, const double *in, double stop_rsd, int max_num_iter,
+               double *true_res) {
+  const long n = orc_op_size(op);
+  double *t = scratch(n), *src = scratch(n);
+  int it;
+  if (op->action != 2) {
+    const double kappa = op->action == 0 ? 1.0 / (2.0 * (op->mass + 4.0))
+                                         : 1.0 / (2 * (4 + op->a5_inv - op->m5));
+    const double *in_o = in, *in_e = in + n;
+    double *out_o = out, *out_e = out + n;
+    orc_dslash(op, t, in_e, 0, 0);
+    for (long i = 0; i < n; i++) t[i] = kappa * t[i] + in_o[i];   /* fTimesV1PlusV2 */
+    orc_matpc(op, src, t, 1);
+    it = orc_invcg(op, out_o, src, stop_rsd, max_num_iter, true_res, NULL);
+    orc_dslash(op, t, out_o, 1, 0);
+    for (long i = 0; i < n; i++) out_e[i] = kappa * t[i] + in_e[i];
+  } else {
+    orc_mobius_params p = op->mob;
+    p.mass = op->mass;
+    const int ls = p.ls;
+    const long n4 = n / ls;
+    cplx kb[64], kc[64], kr[64];
+    mobius_kappas(&p, kb, kc, kr);
+    const double *in_e = in, *in_o = in + n;
+    double *out_e = out, *out_o = out + n;
+    double *t2 = scratch(n);
+    memcpy(t, in_e, n * sizeof(double));
+    orc_mobius_m5inv(t, 0, op->dims, &p);
+    orc_mobius_dslash_4(t2, op->u, t, 0, 0, op->dims, &p);
+    for (int s = 0; s < ls; s++) {                                /* zmobius_zvectTimesV1PlusV2 */
+      for (long i = 0; i < n4 / 2; i++) {
+        cplx x = {t2[s * n4 + 2 * i], t2[s * n4 + 2 * i + 1]};
+        cplx r = cmul(kb[s], x);
+        t[s * n4 + 2 * i] = r.re + in_o[s * n4 + 2 * i];
+        t[s * n4 + 2 * i + 1] = r.im + in_o[s * n4 + 2 * i + 1];
+      }
+    }
+    memcpy(t2, out_o, n * sizeof(double));                       /* SYM2: guess transform */
+    orc_zmobius_dslash_5_plus(out_o, t2, p.mass, 0, op->dims, ls, kr);
+    orc_matpc(op, src, t, 1);
+    it = orc_invcg(op, out_o, src, stop_rsd, max_num_iter, true_res, NULL);
+    memcpy(t, out_o, n * sizeof(double));
+    orc_mobius_m5inv(t, 0, op->dims, &p);
+    memcpy(out_o, t, n * sizeof(double));
+    orc_mobius_dslash_4(t, op->u, out_o, 1, 0, op->dims, &p);
+    for (int s = 0; s < ls; s++) zscale(t + s * n4, kb[s], n4);   /* zmobius_zvectTimesEquComplex */
+    memcpy(out_e, t, n * sizeof(double));
+    orc_mobius_m5inv(out_e, 0, op->dims, &p);
+    memcpy(t, in_e, n * sizeof(double));
+    orc_mobius_m5inv(t, 0, op->dims, &p);
+    for (long i = 0; i < n; i++) out_e[i] += t[i];               /* VecAddEquVec */
+    const double two_kb = 2.0 * kb[0].re;
+    for (long i = 0; i < 2 * n; i++) out[i] *= two_kb;
+    free(t2);
+  }
+  free(t);
+  free(src);
+  return it;
+}

@@ -150,6 +150,17 @@ class Op:
         return sols[:nvec], it, rs
 
 
+    def matinv(self, src_full, guess_full=None, stop_rsd=1e-10, max_iter=5000):
+        """DiracOp*::MatInv on a full vector (2 checkerboards; Wilson/DWF odd
+        half first, Mobius even half first); returns (solution, iterations, true_res)."""
+        src = np.ascontiguousarray(src_full, np.float64)
+        assert src.size == 2 * self.n
+        out = np.zeros(2 * self.n) if guess_full is None else np.array(guess_full, np.float64)
+        tr = C.c_double(0)
+        it = lib().orc_matinv(C.byref(self.s), _p(out), _p(src), C.c_double(stop_rsd), max_iter, C.byref(tr))
+        return out, it, tr.value
+
+
 def _seqsum(x: np.ndarray) -> float:
     return float(np.cumsum(x * x)[-1])
 
@@ -158,6 +169,7 @@ def _setup():
     L = lib()
     L.orc_dslash.restype = C.c_int
     L.orc_matpc.restype = C.c_int
+    L.orc_matinv.restype = C.c_int
     L.orc_mdagm.restype = C.c_int
     L.orc_invcg.restype = C.c_int
     L.orc_invcg.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_double), _dp]

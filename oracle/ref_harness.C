@@ -17,6 +17,8 @@
 //      4-argument InvCg wrapper at inv_cg.C:449-454 has no return statement, so
 //      it is bypassed here -- see DESIGN.md)
 //   Lattice::FmatEvlMInv -> DiracOp::MInvCG         f_dwf_base.C:232-270, minvcg.C:47-353
+//   DiracOp*::MatInv (full-lattice solve)           d_op_wilson.C:257-334, d_op_dwf.C:316-507,
+//                                                   d_op_mobius.C:389-640
 //   zmobius_m5inv / zmobius_dslash_4                d_op_zmobius/noarch/zmobius_m5inv.C:807-845,
 //                                                   zmobius_dslash_4.C:210-221
 //
@@ -53,7 +55,7 @@
 USING_NAMESPACE_CPS
 
 enum { OP_DSLASH = 1, OP_MATPC = 2, OP_MDAGM = 3, OP_INVCG = 4, OP_MINVCG = 5,
-       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8 };
+       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -139,6 +141,7 @@ int main(int argc, char **argv) {
   cg_arg.mass = par[0];
   cg_arg.stop_rsd = par[5];
   cg_arg.max_num_iter = max_iter;
+  cg_arg.Inverter = CG;
 
   int64_t rhdr[8] = {0}; double rpar[64] = {0};
   std::vector<double> out_payload;
@@ -226,6 +229,26 @@ int main(int argc, char **argv) {
     const int nvec = type == 1 ? 1 : nshift;
     for (int s = 0; s < nvec; s++)
       out_payload.insert(out_payload.end(), (double *)sol[s], (double *)sol[s] + fsz);
+  } else if (op == OP_MATINV) {
+    // full-lattice source and initial guess (2 checkerboards each, in the
+    // action's full-vector order); MatInv with the source preserved.
+    Vector *fin = (Vector *)smalloc(2 * fsz * sizeof(double));
+    Vector *fout = (Vector *)smalloc(2 * fsz * sizeof(double));
+    read_all(fi, fin, 2 * fsz * sizeof(double));
+    read_all(fi, fout, 2 * fsz * sizeof(double));
+    DiracOp *d = 0;
+    if (action == 0) d = new DiracOpWilson(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+    else if (action == 1) d = new DiracOpDwf(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+    else d = new DiracOpMobius(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+    Float true_res = 0;
+    double t0 = now_s();
+    d->MatInv(fout, fin, &true_res, PRESERVE_YES);
+    rpar[10] = now_s() - t0;
+    delete d;
+    rpar[0] = true_res;
+    out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
+    sfree(fin);
+    sfree(fout);
   } else {
     die("unknown op");
   }

@@ -15,7 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 CPSREF = os.path.join(HERE, "_ref", "cpsref")
 
-OP_DSLASH, OP_MATPC, OP_MDAGM, OP_INVCG, OP_MINVCG, OP_M5INV, OP_MOBIUS_D4, OP_BENCH = 1, 2, 3, 4, 5, 6, 7, 8
+OP_DSLASH, OP_MATPC, OP_MDAGM, OP_INVCG, OP_MINVCG, OP_M5INV, OP_MOBIUS_D4, OP_BENCH, OP_MATINV = 1, 2, 3, 4, 5, 6, 7, 8, 9
 ACTIONS = {"wilson": 0, "dwf": 1, "mobius": 2}
 
 

@@ -93,6 +93,31 @@ def gen_baseline_config0():
             "seed": 100, "mass": 0.1, "cg_sol": r, "cg_iters": it, "cg_true_res": rp[0]}
 
 
+def matinv_inputs(rec):
+    """Full-lattice source and initial guess of the MatInv fixtures: Gaussian
+    checkerboards from seed+500..503 (the guess scaled by 0.01)."""
+    dims = tuple(int(d) for d in rec["dims"])
+    n = int(np.prod(dims)) // 2 * int(rec.get("ls", 1))
+    seed = int(rec["seed"])
+    src = np.concatenate([fields.random_source(n, seed + 500), fields.random_source(n, seed + 501)])
+    guess = 0.01 * np.concatenate([fields.random_source(n, seed + 502), fields.random_source(n, seed + 503)])
+    return src, guess
+
+
+def gen_matinv(name, action, dims, ls, eps, seed, mass, extra):
+    """DiracOp*::MatInv (full-lattice solve, source preserved) of the case."""
+    u = fields.random_gauge(dims, eps, seed)
+    base = {"dims": np.array(dims), "ls": ls, "seed": seed}
+    src, guess = matinv_inputs(base)
+    it, rp, out = refrun.run(refrun.OP_MATINV, action, dims, u, [src, guess], ls=ls, mass=mass,
+                             stop_rsd=1e-10, max_iter=5000, threads=1, **extra)
+    rec = {"gauge_sha": sha(u), "matinv_src_sha": sha(src), "matinv_guess_sha": sha(guess), "dims": np.array(dims),
+           "ls": ls, "eps": eps, "seed": seed, "mass": mass, "matinv_sol": out, "matinv_true_res": rp[0]}
+    for k, v in extra.items():
+        rec[k] = v
+    return rec
+
+
 def main():
     if not refrun.available():
         sys.exit("oracle/_ref/cpsref missing: run oracle/build_ref.sh first")
@@ -102,7 +127,17 @@ def main():
         print("wrote", case[0])
     np.savez_compressed(os.path.join(OUT, "wilson_8x8x8x8_cg.npz"), **gen_baseline_config0())
     print("wrote wilson_8x8x8x8_cg")
+    main_matinv()
+
+
+def main_matinv():
+    for case in CASES:
+        if "bc_t" in case[7]:
+            continue
+        rec = gen_matinv(*case)
+        np.savez_compressed(os.path.join(OUT, "matinv_" + case[0] + ".npz"), **rec)
+        print("wrote matinv_" + case[0])
 
 
 if __name__ == "__main__":
-    main()
+    main_matinv() if "--matinv" in sys.argv else main()

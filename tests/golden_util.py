@@ -27,3 +27,15 @@ def load(name):
 
 def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+def load_matinv(name):
+    """MatInv fixture: (record, gauge, full source, full initial guess)."""
+    from tests.golden.make_golden import matinv_inputs
+    rec = dict(np.load(os.path.join(GOLDEN, "matinv_" + name + ".npz")))
+    dims = tuple(int(d) for d in rec["dims"])
+    u = fields.random_gauge(dims, float(rec["eps"]), int(rec["seed"]))
+    src, guess = matinv_inputs(rec)
+    assert sha(u) == str(rec["gauge_sha"]), "gauge generator drifted from the fixture"
+    assert sha(src) == str(rec["matinv_src_sha"]) and sha(guess) == str(rec["matinv_guess_sha"])
+    return rec, u, src, guess

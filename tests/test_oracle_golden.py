@@ -79,3 +79,15 @@ def test_wilson_8x8x8x8_cg_config():
     assert it == int(rec["cg_iters"])
     assert tr == float(rec["cg_true_res"]) and tr <= 1e-10
     np.testing.assert_array_equal(sol, rec["cg_sol"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_matinv_bitexact(name):
+    """DiracOp*::MatInv (full-lattice solve with source preparation and
+    even/odd reconstruction) from a nonzero initial guess."""
+    from tests.golden_util import load_matinv
+    rec, u, src, guess = load_matinv(name)
+    op = make_op(rec, u, name.split("_")[0])
+    out, it, tr = op.matinv(src, guess, stop_rsd=1e-10, max_iter=5000)
+    np.testing.assert_array_equal(out, rec["matinv_sol"])
+    assert tr == float(rec["matinv_true_res"])
