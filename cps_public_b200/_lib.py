@@ -19,6 +19,7 @@ WILSON, DWF, MOBIUS = 0, 1, 2
 F64, F32, F16 = 0, 1, 2
 ORDER_CANONICAL, ORDER_WILSON = 0, 1
 MULTI, SINGLE = 0, 1
+FERMION_CB, FERMION_4D_EE = 0, 1
 
 SYMBOLS = [
     "cpsb_init", "cpsb_error_string", "cpsb_last_error", "cpsb_mem_info", "cpsb_gauge_load", "cpsb_gauge_free", "cpsb_dslash",
@@ -26,7 +27,7 @@ SYMBOLS = [
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches",
     "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
-    "cpsb_serve_stats", "cpsb_serve_destroy",
+    "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert",
 ]
 
 
@@ -101,6 +102,8 @@ def load():
     lib.cpsb_serve_wait.argtypes = [C.c_void_p, C.c_ulonglong, R, _dp]
     lib.cpsb_serve_stats.argtypes = [C.c_void_p, C.POINTER(ServeStats)]
     lib.cpsb_serve_destroy.argtypes = [C.c_void_p]
+    lib.cpsb_fermion_convert.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
     lib.cpsb_redot_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
     lib.cpsb_kernel_launches.argtypes = [C.POINTER(C.c_ulonglong)]
     lib.cpsb_bench_dslash.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_int, _dp, _dp]

@@ -122,6 +122,40 @@ __global__ void gauge_pack_kernel(void *dst, const double *u, int lx, int ly, in
   }
 }
 
+// Lattice::Fconvert between CANONICAL and the checkerboarded fermion orders
+// (lattice/convert/convert_func.C:429-495, convert.C:635-1010): a permutation
+// of 24-real sites.  One thread moves one site (12 double2).  order 0: [odd |
+// even] per 4-D slice, or for ls > 1 the 5-D checkerboard (sites with
+// x+y+z+t+s odd first); order 1: DWF_4D_EOPREC_EE (4-D even half of every
+// slice, then the odd half).  direction 0: CANONICAL -> order, 1: back.
+__global__ void fconvert_kernel(double2 *out, const double2 *in, int lx, int ly, int lz, int lt, int ls, int order,
+                                int direction) {
+  const long vol = (long)lx * ly * lz * lt, h = vol / 2, n = vol * ls;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const long s = i / vol, site = i - s * vol;
+    const int x = (int)(site % lx), y = (int)((site / lx) % ly), z = (int)((site / ((long)lx * ly)) % lz),
+              t = (int)(site / ((long)lx * ly * lz));
+    const int par = (x + y + z + t) & 1;
+    const long cbi = x / 2 + (long)(lx / 2) * (y + (long)ly * (z + (long)lz * t));
+    int second;  // 1: the site goes to the second half
+    if (order == 0) second = ls > 1 ? 1 - ((par + (int)s) & 1) : 1 - par;  // even (5-D / 4-D) sites second
+    else second = par;                                                       // 4-D odd sites second
+    const long j = second * ls * h + s * h + cbi;
+    const double2 *src = in + 12 * (direction == 0 ? i : j);
+    double2 *dst = out + 12 * (direction == 0 ? j : i);
+#pragma unroll
+    for (int k = 0; k < 12; k++) dst[k] = src[k];
+  }
+}
+
+cudaError_t launch_fconvert(double *out, const double *in, const int dims[4], int ls, int order, int direction,
+                            cudaStream_t st) {
+  const long n = (long)dims[0] * dims[1] * dims[2] * dims[3] * ls;
+  fconvert_kernel<<<flat_grid(n), 256, 0, st>>>((double2 *)out, (const double2 *)in, dims[0], dims[1], dims[2],
+                                                dims[3], ls, order, direction);
+  return launched();
+}
+
 cudaError_t launch_gauge_pack(int prec, void *dst, const double *u, const int dims[4], int bc_t, cudaStream_t st) {
   const long n = (long)dims[0] * dims[1] * dims[2] * dims[3] * 4;
   const int g = flat_grid(n);

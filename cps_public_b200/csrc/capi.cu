@@ -521,6 +521,23 @@ int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
   });
 }
 
+int cpsb_fermion_convert(const int dims[4], int ls, int order, int direction, double *out, const double *in,
+                         void *stream) {
+  return guarded([&] {
+    need_init();
+    if (!dims || !out || !in || out == in) throw Error{CPSB_ERR_ARG, "bad vectors (out and in must differ)"};
+    for (int k = 0; k < 4; k++)
+      if (dims[k] < 2 || dims[k] % 2) throw Error{CPSB_ERR_ARG, "lattice extents must be even and >= 2"};
+    if (ls < 1 || ls > 64) throw Error{CPSB_ERR_ARG, "ls out of range"};
+    if ((order != CPSB_FERMION_CB && order != CPSB_FERMION_4D_EE) || (direction != 0 && direction != 1))
+      throw Error{CPSB_ERR_ARG, "bad order / direction"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    CK(launch_fconvert(out, in, dims, ls, order, direction, st));
+    CK(cudaStreamSynchronize(st));
+    return CPSB_OK;
+  });
+}
+
 int cpsb_kernel_launches(unsigned long long *count) {
   if (!count) return CPSB_ERR_ARG;
   *count = launch_count();

@@ -59,6 +59,8 @@ struct CgState;   // defined in cg_state.h
 cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, long nsites, cudaStream_t st);
 cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, long nsites, cudaStream_t st);
 cudaError_t launch_convert(int pdst, SpinorPtr dst, int psrc, SpinorPtr src, long nsites, cudaStream_t st);
+cudaError_t launch_fconvert(double *out, const double *in, const int dims[4], int ls, int order, int direction,
+                            cudaStream_t st);
 cudaError_t launch_gauge_pack(int prec, void *dst, const double *u_canonical, const int dims[4],
                               int bc_t, cudaStream_t st);
 

@@ -36,6 +36,7 @@ enum cpsb_action { CPSB_WILSON = 0, CPSB_DWF = 1, CPSB_MOBIUS = 2 };
 enum cpsb_precision { CPSB_PREC_F64 = 0, CPSB_PREC_F32 = 1, CPSB_PREC_F16 = 2 };
 enum cpsb_gauge_order { CPSB_ORDER_CANONICAL = 0, CPSB_ORDER_WILSON = 1 };
 enum cpsb_multishift_type { CPSB_MULTI = 0, CPSB_SINGLE = 1 };
+enum cpsb_fermion_order { CPSB_FERMION_CB = 0, CPSB_FERMION_4D_EE = 1 };
 
 typedef struct cpsb_gauge_s *cpsb_gauge;
 
@@ -152,6 +153,17 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
  * on the device; res reports the CG as cpsb_invcg does. */
 int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
                 cpsb_solve_result *res);
+
+/* Lattice::Fconvert for fermion fields (include/util/lattice.h:1326;
+ * lattice/convert/convert_func.C:429-495, convert.C:635-1010) on the device:
+ * CANONICAL (slice s slowest, then site x+lx*(y+ly*(z+lz*t))) <-> the
+ * checkerboarded order the solvers take.  order CPSB_FERMION_CB: WILSON
+ * (odd 4-D half first; for ls > 1 the 5-D checkerboard, sites with x+y+z+t+s
+ * odd first); CPSB_FERMION_4D_EE: DWF_4D_EOPREC_EE (Mobius: 4-D even half of
+ * every slice first).  direction 0: CANONICAL -> order, 1: order -> CANONICAL.
+ * out, in: distinct device buffers of vol*ls*24 doubles. */
+int cpsb_fermion_convert(const int dims[4], int ls, int order, int direction, double *out, const double *in,
+                         void *stream);
 
 /* Device-resident variants: x, b (and out/in) are device pointers holding CPS
  * order vectors; stream is a cudaStream_t (NULL = the library stream).  These

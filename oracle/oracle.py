@@ -179,3 +179,41 @@ def _setup():
 
 
 _setup()
+
+
+def fermion_convert(v, dims, ls=1, order="wilson", inverse=False):
+    """Lattice::Fconvert between CANONICAL and the checkerboarded orders, as a
+    permutation of 24-real sites.  TEST INFRASTRUCTURE ONLY.
+
+    CANONICAL: slice s (slowest), then site x + lx*(y + ly*(z + lz*t)).
+    order "wilson": each slice first to [odd | even] 4-D halves
+    (FcanonToWilson, lattice/convert/convert_func.C:429-495); for ls > 1 the
+    5-D checkerboard of FdwfBase::Fconvert (convert.C:700-755): the first half
+    holds the sites with x+y+z+t+s odd (slice by slice), the second half the
+    others.
+    order "4d_ee" (DWF_4D_EOPREC_EE, convert.C:793-830): the 4-D even half of
+    every slice, then the 4-D odd half of every slice.
+    inverse=True maps the checkerboarded order back to CANONICAL.
+    """
+    lx, ly, lz, lt = dims
+    vol = lx * ly * lz * lt
+    h = vol // 2
+    t, z, y, x = np.meshgrid(np.arange(lt), np.arange(lz), np.arange(ly), np.arange(lx), indexing="ij")
+    par = ((x + y + z + t) % 2).reshape(-1)                   # canonical site -> 4-D parity
+    cbi = (x // 2 + (lx // 2) * (y + ly * (z + lz * t))).reshape(-1)
+    dst = np.empty((ls, vol), np.int64)
+    for s in range(ls):
+        if order == "wilson" and ls > 1:
+            half = ((par + s) % 2 == 0).astype(np.int64)     # 5-D odd sites first
+        elif order == "wilson":
+            half = (par == 0).astype(np.int64)               # 4-D odd sites first
+        else:
+            half = (par == 1).astype(np.int64)               # 4-D even sites first
+        dst[s] = half * (ls * h) + s * h + cbi
+    v = np.asarray(v, np.float64).reshape(ls * vol, 24)
+    out = np.empty_like(v)
+    if inverse:
+        out[:] = v[dst.reshape(-1)]
+    else:
+        out[dst.reshape(-1)] = v
+    return out.reshape(-1)

@@ -19,6 +19,8 @@
 //   Lattice::FmatEvlMInv -> DiracOp::MInvCG         f_dwf_base.C:232-270, minvcg.C:47-353
 //   DiracOp*::MatInv (full-lattice solve)           d_op_wilson.C:257-334, d_op_dwf.C:316-507,
 //                                                   d_op_mobius.C:389-640
+//   Lattice::Fconvert (fermion storage order)       lattice/convert/convert.C:444-570 (Wilson),
+//                                                   :635-1010 (DWF / Mobius)
 //   zmobius_m5inv / zmobius_dslash_4                d_op_zmobius/noarch/zmobius_m5inv.C:807-845,
 //                                                   zmobius_dslash_4.C:210-221
 //
@@ -30,7 +32,9 @@
 //   hdr: 0 op, 1 action (0 Wilson, 1 DWF, 2 Mobius), 2..5 lx ly lz lt, 6 ls,
 //        7 cb, 8 dag, 9 max_iter, 10 nshift, 11 multishift type (0 MULTI,
 //        1 SINGLE), 12 zmobius pc type, 13 t boundary (0 periodic, 1 antiperiodic),
-//        14 repetitions (OP_BENCH: MatPcDagMatPc applied this many times)
+//        14 repetitions (OP_BENCH: MatPcDagMatPc applied this many times),
+//        15 fermion order for OP_FCONVERT (0 WILSON, 1 DWF_4D_EOPREC_EE),
+//        16 OP_FCONVERT direction (0 CANONICAL -> order, 1 order -> CANONICAL)
 //   rpar[10] = wall seconds spent inside the timed CPS call(s) (MINVCG: rpar[42],
 //   since rpar[0..nshift) holds the per-shift residuals)
 //   par: 0 mass, 1 M5 (dwf_height), 2 a5_inv, 3 mobius b, 4 mobius c, 5 stop_rsd,
@@ -55,7 +59,7 @@
 USING_NAMESPACE_CPS
 
 enum { OP_DSLASH = 1, OP_MATPC = 2, OP_MDAGM = 3, OP_INVCG = 4, OP_MINVCG = 5,
-       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9 };
+       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9, OP_FCONVERT = 10 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -249,6 +253,15 @@ int main(int argc, char **argv) {
     out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
     sfree(fin);
     sfree(fout);
+  } else if (op == OP_FCONVERT) {
+    const size_t full = 2 * fsz;  // both checkerboards
+    Vector *f = (Vector *)smalloc(full * sizeof(double));
+    read_all(fi, f, full * sizeof(double));
+    const StrOrdType order = hdr[15] ? DWF_4D_EOPREC_EE : WILSON;
+    if (hdr[16] == 0) lat.Fconvert(f, order, CANONICAL);
+    else lat.Fconvert(f, CANONICAL, order);
+    out_payload.assign((double *)f, (double *)f + full);
+    sfree(f);
   } else {
     die("unknown op");
   }

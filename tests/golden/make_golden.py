@@ -118,6 +118,33 @@ def gen_matinv(name, action, dims, ls, eps, seed, mass, extra):
     return rec
 
 
+FCONVERT_CASES = [("wilson", (4, 4, 4, 6), 1, 0, {}), ("dwf", (4, 4, 4, 6), 4, 0, {"m5": 1.8}),
+                  ("mobius", (4, 4, 4, 6), 4, 1, {"m5": 1.8, "b": 1.5, "c": 0.5})]
+
+
+def coded_field(dims, ls):
+    """Full fermion field whose site i carries i + c/32 in component c."""
+    n = int(np.prod(dims)) * ls
+    return (np.arange(n)[:, None] + np.arange(24)[None, :] / 32.0).reshape(-1)
+
+
+def gen_fconvert():
+    """Lattice::Fconvert as site permutations: perm[j] = canonical site that
+    lands at position j (CANONICAL -> order) and its inverse direction."""
+    rec = {}
+    for action, dims, ls, order, extra in FCONVERT_CASES:
+        u = fields.random_gauge(dims, 0.2, 7)
+        v = coded_field(dims, ls)
+        for direction in (0, 1):
+            _, _, out = refrun.run(refrun.OP_FCONVERT, action, dims, u, [v], ls=ls, order=order,
+                                   direction=direction, threads=1, **extra)
+            site = out.reshape(-1, 24)
+            perm = np.floor(site[:, 0]).astype(np.int32)
+            assert np.array_equal(site - perm[:, None], np.tile(np.arange(24) / 32.0, (len(perm), 1)))
+            rec[f"{action}_dir{direction}"] = perm
+    return rec
+
+
 def main():
     if not refrun.available():
         sys.exit("oracle/_ref/cpsref missing: run oracle/build_ref.sh first")
@@ -128,6 +155,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "wilson_8x8x8x8_cg.npz"), **gen_baseline_config0())
     print("wrote wilson_8x8x8x8_cg")
     main_matinv()
+    main_fconvert()
 
 
 def main_matinv():
@@ -139,5 +167,15 @@ def main_matinv():
         print("wrote matinv_" + case[0])
 
 
+def main_fconvert():
+    np.savez_compressed(os.path.join(OUT, "fconvert_4x4x4x6.npz"), **gen_fconvert())
+    print("wrote fconvert_4x4x4x6")
+
+
 if __name__ == "__main__":
-    main_matinv() if "--matinv" in sys.argv else main()
+    if "--matinv" in sys.argv:
+        main_matinv()
+    elif "--fconvert" in sys.argv:
+        main_fconvert()
+    else:
+        main()

@@ -91,3 +91,20 @@ def test_matinv_bitexact(name):
     out, it, tr = op.matinv(src, guess, stop_rsd=1e-10, max_iter=5000)
     np.testing.assert_array_equal(out, rec["matinv_sol"])
     assert tr == float(rec["matinv_true_res"])
+
+
+@pytest.mark.parametrize("action,order", [("wilson", "wilson"), ("dwf", "wilson"), ("mobius", "4d_ee")])
+def test_fermion_convert_matches_reference(action, order):
+    """Lattice::Fconvert (CANONICAL <-> WILSON / 5-D checkerboard /
+    DWF_4D_EOPREC_EE) as recorded from the compiled reference: the oracle's
+    permutation moves every site exactly where CPS puts it, both directions."""
+    import os
+    from tests.golden.make_golden import FCONVERT_CASES, coded_field
+    rec = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "fconvert_4x4x4x6.npz")))
+    dims, ls = [(c[1], c[2]) for c in FCONVERT_CASES if c[0] == action][0]
+    v = coded_field(dims, ls)
+    for direction in (0, 1):
+        out = oracle.fermion_convert(v, dims, ls, order, inverse=bool(direction)).reshape(-1, 24)
+        perm = rec[f"{action}_dir{direction}"]
+        np.testing.assert_array_equal(np.floor(out[:, 0]).astype(np.int32), perm)
+        np.testing.assert_array_equal(out, coded_field(dims, ls).reshape(-1, 24)[perm])
