@@ -175,6 +175,20 @@ class DiracOp:
         r.rc = rc
         return out, r
 
+    def MinResExt(self, phi, prev):
+        """DiracOp::MinResExt: chronological guess from previous solutions.
+        Returns (psi, orthonormalised prev, MatPcDagMatPc of them, |phi - A psi|/|phi|)."""
+        deg = len(prev)
+        v = [np.array(self._v(x), np.float64) for x in prev]
+        vm = [np.zeros(self.n) for _ in range(deg)]
+        psi = np.zeros(self.n)
+        vp = (_lib._dp * max(deg, 1))(*[ptr(x) for x in v])
+        vmp = (_lib._dp * max(deg, 1))(*[ptr(x) for x in vm])
+        res = C.c_double()
+        check(_lib.load().cpsb_minresext(self.gauge.h, C.byref(self.p), ptr(psi), ptr(self._v(phi)), vp, vmp, deg,
+                                         C.byref(res)), "cpsb_minresext")
+        return psi, v, vm, res.value
+
     def MInvCG(self, src, shifts, rsd, ms_type=MULTI, alpha=None, max_num_iter=5000, precision=F64):
         ns = len(shifts)
         nvec = 1 if ms_type == SINGLE else ns

@@ -27,7 +27,7 @@ SYMBOLS = [
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches",
     "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
-    "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert",
+    "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert", "cpsb_minresext",
 ]
 
 
@@ -104,6 +104,7 @@ def load():
     lib.cpsb_serve_destroy.argtypes = [C.c_void_p]
     lib.cpsb_fermion_convert.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                          C.c_void_p]
+    lib.cpsb_minresext.argtypes = [C.c_void_p, P, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp]
     lib.cpsb_redot_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
     lib.cpsb_kernel_launches.argtypes = [C.POINTER(C.c_ulonglong)]
     lib.cpsb_bench_dslash.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_int, _dp, _dp]

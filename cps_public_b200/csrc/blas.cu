@@ -408,6 +408,57 @@ __global__ void __launch_bounds__(NT) redot_kernel(Geom g, SpinorPtr X, SpinorPt
   }
 }
 
+// conj(X).Y of FP64 fields (one RHS): result[0] = real part, result[1] =
+// imaginary part (Vector::CompDotProductGlbSum, vector/comsrc/vector.C:196);
+// every double2 chunk is one complex number.
+template <int NT>
+__global__ void __launch_bounds__(NT) cdot_kernel(long nchunks, const double2 *X, const double2 *Y, Reduce red) {
+  __shared__ double sh[NT / 32];
+  double re = 0, im = 0;
+  for (long j = (long)blockIdx.x * NT + threadIdx.x; j < nchunks; j += (long)gridDim.x * NT) {
+    const double2 a = X[j], b = Y[j];
+    re += a.x * b.x + a.y * b.y;
+    im += a.x * b.y - a.y * b.x;
+  }
+  const double br = block_sum<NT>(re, sh);
+  const double bi = block_sum<NT>(im, sh);
+  if (threadIdx.x == 0) {
+    red.partial[blockIdx.x] = br;
+    red.partial[gridDim.x + blockIdx.x] = bi;
+  }
+  if (last_block(red.ticket, gridDim.x)) {
+    for (int q = 0; q < 2; q++) {
+      const double c = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
+      if (threadIdx.x == 0) red.result[q] = c;
+      __syncthreads();
+    }
+  }
+}
+
+cudaError_t launch_cdot(SpinorPtr X, SpinorPtr Y, long nsites, Reduce red, cudaStream_t st) {
+  const long nch = nsites * 12;  // FP64 chunked layout: 12 complex chunks per site, contiguous per chunk array
+  if (X.stride != nsites || Y.stride != nsites) return cudaErrorInvalidValue;
+  cdot_kernel<256><<<grid_blocks(nch, 256), 256, 0, st>>>(nch, (const double2 *)X.data, (const double2 *)Y.data,
+                                                            red);
+  return launched();
+}
+
+// out = c X + Y on FP64 fields (Vector::CTimesV1PlusV2, vector_util.C:910).
+__global__ void caxpy_kernel(long nchunks, double2 *out, double cr, double ci, const double2 *X, const double2 *Y) {
+  for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < nchunks; j += (long)gridDim.x * blockDim.x) {
+    const double2 x = X[j], y = Y[j];
+    out[j] = make_double2(cr * x.x - ci * x.y + y.x, cr * x.y + ci * x.x + y.y);
+  }
+}
+
+cudaError_t launch_caxpy(SpinorPtr out, double cr, double ci, SpinorPtr X, SpinorPtr Y, long nsites, cudaStream_t st) {
+  const long nch = nsites * 12;
+  if (out.stride != nsites || X.stride != nsites || Y.stride != nsites) return cudaErrorInvalidValue;
+  caxpy_kernel<<<flat_grid(nch), 256, 0, st>>>(nch, (double2 *)out.data, cr, ci, (const double2 *)X.data,
+                                               (const double2 *)Y.data);
+  return launched();
+}
+
 cudaError_t launch_redot(int prec, const Geom &g, SpinorPtr X, SpinorPtr Y, Reduce red, cudaStream_t st) {
   dim3 grid(grid_blocks((long)g.n4cb * g.ls, 256), g.nrhs);
   if (prec == P64) redot_kernel<P64, 256><<<grid, 256, 0, st>>>(g, X, Y, red);

@@ -19,6 +19,9 @@ cudaError_t launch_cg_xp_update(int px, int prec, const Geom &g, SpinorPtr x, Sp
 cudaError_t launch_axpby(int po, SpinorPtr out, int px, SpinorPtr X, int py, SpinorPtr Y, const Geom &g, Scal2 sc,
                          const int *skip, Reduce red, int norm, cudaStream_t st);
 cudaError_t launch_redot(int prec, const Geom &g, SpinorPtr X, SpinorPtr Y, Reduce red, cudaStream_t st);
+// FP64 whole fields of nsites sites: conj(X).Y into red.result[0..1]; out = (cr + i ci) X + Y.
+cudaError_t launch_cdot(SpinorPtr X, SpinorPtr Y, long nsites, Reduce red, cudaStream_t st);
+cudaError_t launch_caxpy(SpinorPtr out, double cr, double ci, SpinorPtr X, SpinorPtr Y, long nsites, cudaStream_t st);
 
 // Mobius 5th-direction kernels (m5.cu).
 struct M5Coef {

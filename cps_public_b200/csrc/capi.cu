@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <chrono>
+#include <complex>
 
 #include "abi.h"
 
@@ -534,6 +535,118 @@ int cpsb_fermion_convert(const int dims[4], int ls, int order, int direction, do
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
     CK(launch_fconvert(out, in, dims, ls, order, direction, st));
     CK(cudaStreamSynchronize(st));
+    return CPSB_OK;
+  });
+}
+
+int cpsb_minresext(cpsb_gauge h, const cpsb_dirac_params *p, double *psi, const double *phi, double **v,
+                   double **vm, int degree, double *resid) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (!psi || !phi || degree < 0 || degree > 16 || (degree > 0 && (!v || !vm)))
+      throw Error{CPSB_ERR_ARG, "bad MinResExt arguments"};
+    for (int i = 0; i < degree; i++)
+      if (!v[i] || !vm[i]) throw Error{CPSB_ERR_ARG, "null previous solution"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    const long n = op.nsites();
+    const Geom &g = op.geom;
+    if (degree == 0) {  // minresext.C:57-61: no guess
+      memset(psi, 0, sizeof(double) * 24 * n);
+      if (resid) *resid = 1.0;
+      return CPSB_OK;
+    }
+    Field fphi(P64, n), fpsi(P64, n), fr(P64, n);
+    std::vector<Field> fv(degree), fvm(degree);
+    upload(fphi, &phi, 1, n, st);
+    for (int i = 0; i < degree; i++) {
+      fv[i].create(P64, n);
+      fvm[i].create(P64, n);
+      upload(fv[i], (const double *const *)&v[i], 1, n, st);
+    }
+    RedSlot rs;
+    DevBuf dres(sizeof(double) * 4);
+    double hres[2];
+    auto fetch = [&](int k) {
+      CK(cudaMemcpyAsync(hres, dres.p, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    };
+    auto cdot = [&](const Field &a, const Field &b) {
+      CK(launch_cdot(a.ptr(), b.ptr(), n, rs.r((double *)dres.p), st));
+      fetch(2);
+      return std::complex<double>(hres[0], hres[1]);
+    };
+    auto norm2 = [&](const Field &a) {
+      Geom g1 = g;
+      CK(launch_redot(P64, g1, a.ptr(), a.ptr(), rs.r((double *)dres.p), st));
+      fetch(1);
+      return hres[0];
+    };
+    auto scale = [&](const Field &a, double f) {
+      Scal2 c;
+      for (int q = 0; q < MAX_RHS; q++) {
+        c.a[q] = f;
+        c.b[q] = 0.0;
+      }
+      Reduce none;
+      memset(&none, 0, sizeof(none));
+      CK(launch_axpby(P64, a.ptr(), P64, a.ptr(), P64, SpinorPtr{}, g, c, nullptr, none, 0, st));
+    };
+    typedef std::complex<double> cplx_t;
+    std::vector<std::vector<cplx_t>> G(degree, std::vector<cplx_t>(degree));
+    std::vector<cplx_t> a(degree), b(degree);
+    // orthonormalise (minresext.C:84-93)
+    for (int i = 0; i < degree; i++) {
+      scale(fv[i], 1 / sqrt(norm2(fv[i])));
+      for (int j = i + 1; j < degree; j++) {
+        const cplx_t xp = cdot(fv[i], fv[j]);
+        CK(launch_caxpy(fv[j].ptr(), -xp.real(), -xp.imag(), fv[i].ptr(), fv[j].ptr(), n, st));
+      }
+    }
+    // right-hand side and the A-images (minresext.C:95-101)
+    for (int i = 0; i < degree; i++) {
+      b[i] = cdot(fv[i], fphi);
+      Reduce rd = rs.r((double *)dres.p);
+      op.mdagm(fvm[i], fv[i], &rd, nullptr, st);
+      fetch(1);
+      G[i][i] = cplx_t(hres[0], 0.0);
+    }
+    for (int j = 0; j < degree; j++)
+      for (int k = j + 1; k < degree; k++) {
+        G[j][k] = cdot(fv[j], fvm[k]);
+        G[k][j] = std::conj(G[j][k]);
+      }
+    // the reference's elimination with its diagonal pivot test (minresext.C:113-135)
+    for (int i = 0; i < degree; i++) {
+      int k = i;
+      for (int j = i + 1; j < degree; j++)
+        if (std::abs(G[j][j]) > std::abs(G[k][k])) k = j;
+      if (k != i) {
+        std::swap(b[k], b[i]);
+        std::swap(G[k], G[i]);
+      }
+      for (int j = i + 1; j < degree; j++) {
+        const cplx_t xp = G[j][i] / G[i][i];
+        b[j] -= xp * b[i];
+        for (int m = 0; m < degree; m++) G[j][m] -= xp * G[i][m];
+      }
+    }
+    CK(cudaMemsetAsync(fpsi.data.p, 0, fpsi.data.bytes, st));
+    CK(cudaMemcpyAsync(fr.data.p, fphi.data.p, fphi.data.bytes, cudaMemcpyDeviceToDevice, st));
+    for (int i = degree - 1; i >= 0; i--) {
+      a[i] = 0.0;
+      for (int j = i + 1; j < degree; j++) a[i] += G[i][j] * a[j];
+      a[i] = (b[i] - a[i]) / G[i][i];
+      CK(launch_caxpy(fpsi.ptr(), a[i].real(), a[i].imag(), fv[i].ptr(), fpsi.ptr(), n, st));
+      CK(launch_caxpy(fr.ptr(), -a[i].real(), -a[i].imag(), fvm[i].ptr(), fr.ptr(), n, st));
+    }
+    if (resid) *resid = sqrt(norm2(fr) / norm2(fphi));
+    download(&psi, 1, n, fpsi, st);
+    for (int i = 0; i < degree; i++) {
+      download(&v[i], 1, n, fv[i], st);
+      download(&vm[i], 1, n, fvm[i], st);
+    }
     return CPSB_OK;
   });
 }

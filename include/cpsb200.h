@@ -154,6 +154,15 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
 int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
                 cpsb_solve_result *res);
 
+/* DiracOp::MinResExt(psi, phi, v, vm, degree) (include/util/dirac_op.h;
+ * d_op_base/comsrc/minresext.C:32-156): the minimal-residual chronological
+ * initial guess from degree <= 16 previous solutions.  v[i] (host vectors) are
+ * orthonormalised in place, vm[i] receive MatPcDagMatPc v[i], psi the guess;
+ * resid (optional) receives |phi - MatPcDagMatPc psi| / |phi|.  The vector
+ * work runs on the device, the degree x degree elimination on the host. */
+int cpsb_minresext(cpsb_gauge h, const cpsb_dirac_params *p, double *psi, const double *phi, double **v,
+                   double **vm, int degree, double *resid);
+
 /* Lattice::Fconvert for fermion fields (include/util/lattice.h:1326;
  * lattice/convert/convert_func.C:429-495, convert.C:635-1010) on the device:
  * CANONICAL (slice s slowest, then site x+lx*(y+ly*(z+lz*t))) <-> the

@@ -17,6 +17,7 @@
  * field = sites x 24 reals, r+2*(colour+3*spin); a 5-D field is Ls consecutive
  * 4-D checkerboard slices.
  */
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -858,4 +859,89 @@ int orc_matinv(const orc_op *op, double *out, const double *in, double stop_rsd,
   free(t);
   free(src);
   return it;
+}
+
+/* ------------------------------------------------------------------ */
+/* DiracOp::MinResExt, d_op_base/comsrc/minresext.C:32-156             */
+/* ------------------------------------------------------------------ */
+/* Chronological guess: orthonormalise the previous solutions v[0..degree)
+ * in place (Gram-Schmidt with the complex dot conj(a).b), vm[i] =
+ * MatPcDagMatPc v[i], G = v^dag A v (diagonal from the fused |M v|^2), solve
+ * G a = v^dag phi by the reference's elimination (its pivot test compares
+ * diagonal magnitudes), psi = sum a_i v_i.  Complex arithmetic uses C99
+ * complex types, whose multiplication and division compile to the same
+ * runtime routines as the reference's std::complex<double>.  Returns
+ * |phi - A psi| / |phi|. */
+static void cdot_seq(const double *a, const double *b, long len, double *re, double *im) {
+  double r = 0.0, i = 0.0;
+  for (long k = 0; k < len; k += 2) {
+    r += a[k] * b[k] + a[k + 1] * b[k + 1];
+    i += a[k] * b[k + 1] - a[k + 1] * b[k];
+  }
+  *re = r;
+  *im = i;
+}
+static void caxpy_seq(double *a, double re, double im, const double *c, const double *d, long len) {
+  for (long k = 0; k < len; k += 2) {
+    const double c_re = c[k], c_im = c[k + 1];
+    a[k] = re * c_re - im * c_im + d[k];
+    a[k + 1] = re * c_im + im * c_re + d[k + 1];
+  }
+}
+double orc_minresext(const orc_op *op, double *psi, const double *phi, double **v, double **vm, int degree) {
+  const long n = orc_op_size(op);
+  if (degree == 0) {
+    memset(psi, 0, n * sizeof(double));
+    return 1.0;
+  }
+  double _Complex G[16][16], a[16], b[16], xp;
+  double re, im;
+  for (int i = 0; i < degree; i++) {
+    const double f = 1 / sqrt(dot_seq(v[i], v[i], n));
+    for (long k = 0; k < n; k++) v[i][k] *= f;
+    for (int j = i + 1; j < degree; j++) {
+      cdot_seq(v[i], v[j], n, &re, &im);
+      caxpy_seq(v[j], -re, -im, v[i], v[j], n);
+    }
+  }
+  for (int i = 0; i < degree; i++) {
+    cdot_seq(v[i], phi, n, &re, &im);
+    b[i] = CMPLX(re, im);
+    double dot = 0;
+    orc_mdagm(op, vm[i], v[i], &dot);
+    G[i][i] = CMPLX(dot, 0.0);
+  }
+  for (int j = 0; j < degree; j++)
+    for (int k = j + 1; k < degree; k++) {
+      cdot_seq(v[j], vm[k], n, &re, &im);
+      G[j][k] = CMPLX(re, im);
+      G[k][j] = conj(G[j][k]);
+    }
+  for (int i = 0; i < degree; i++) {
+    int k = i;
+    for (int j = i + 1; j < degree; j++)
+      if (cabs(G[j][j]) > cabs(G[k][k])) k = j;
+    if (k != i) {
+      xp = b[k]; b[k] = b[i]; b[i] = xp;
+      for (int j = 0; j < degree; j++) { xp = G[k][j]; G[k][j] = G[i][j]; G[i][j] = xp; }
+    }
+    for (int j = i + 1; j < degree; j++) {
+      xp = G[j][i] / G[i][i];
+      b[j] -= xp * b[i];
+      for (int m = 0; m < degree; m++) G[j][m] -= xp * G[i][m];
+    }
+  }
+  double *r = scratch(n);
+  memset(psi, 0, n * sizeof(double));
+  memcpy(r, phi, n * sizeof(double));
+  for (int i = degree - 1; i >= 0; i--) {
+    a[i] = CMPLX(0.0, 0.0);
+    for (int j = i + 1; j < degree; j++) a[i] += G[i][j] * a[j];
+    a[i] = (b[i] - a[i]) / G[i][i];
+    caxpy_seq(psi, creal(a[i]), cimag(a[i]), v[i], psi, n);
+    caxpy_seq(r, -creal(a[i]), -cimag(a[i]), vm[i], r, n);
+  }
+  const double err = sqrt(dot_seq(r, r, n) / dot_seq(phi, phi, n));
+  free(r);
+  return err;
 }

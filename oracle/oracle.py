@@ -161,6 +161,18 @@ class Op:
         return out, it, tr.value
 
 
+    def minresext(self, phi, prev):
+        """DiracOp::MinResExt: returns (psi, orthonormalised prev, MatPcDagMatPc of them, guess residual)."""
+        deg = len(prev)
+        v = [np.array(x, np.float64) for x in prev]
+        vm = [np.zeros(self.n) for _ in range(deg)]
+        psi = np.zeros(self.n)
+        vp = (_dp * max(deg, 1))(*[_p(x) for x in v]) if deg else (_dp * 1)()
+        vmp = (_dp * max(deg, 1))(*[_p(x) for x in vm]) if deg else (_dp * 1)()
+        err = lib().orc_minresext(C.byref(self.s), _p(psi), _p(self._v(phi)), vp, vmp, deg)
+        return psi, v, vm, err
+
+
 def _seqsum(x: np.ndarray) -> float:
     return float(np.cumsum(x * x)[-1])
 
@@ -170,6 +182,7 @@ def _setup():
     L.orc_dslash.restype = C.c_int
     L.orc_matpc.restype = C.c_int
     L.orc_matinv.restype = C.c_int
+    L.orc_minresext.restype = C.c_double
     L.orc_mdagm.restype = C.c_int
     L.orc_invcg.restype = C.c_int
     L.orc_invcg.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_double), _dp]

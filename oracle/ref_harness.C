@@ -19,6 +19,7 @@
 //   Lattice::FmatEvlMInv -> DiracOp::MInvCG         f_dwf_base.C:232-270, minvcg.C:47-353
 //   DiracOp*::MatInv (full-lattice solve)           d_op_wilson.C:257-334, d_op_dwf.C:316-507,
 //                                                   d_op_mobius.C:389-640
+//   DiracOp::MinResExt (chronological guess)        d_op_base/comsrc/minresext.C:32-156
 //   Lattice::Fconvert (fermion storage order)       lattice/convert/convert.C:444-570 (Wilson),
 //                                                   :635-1010 (DWF / Mobius)
 //   zmobius_m5inv / zmobius_dslash_4                d_op_zmobius/noarch/zmobius_m5inv.C:807-845,
@@ -34,7 +35,8 @@
 //        1 SINGLE), 12 zmobius pc type, 13 t boundary (0 periodic, 1 antiperiodic),
 //        14 repetitions (OP_BENCH: MatPcDagMatPc applied this many times),
 //        15 fermion order for OP_FCONVERT (0 WILSON, 1 DWF_4D_EOPREC_EE),
-//        16 OP_FCONVERT direction (0 CANONICAL -> order, 1 order -> CANONICAL)
+//        16 OP_FCONVERT direction (0 CANONICAL -> order, 1 order -> CANONICAL),
+//        17 OP_MINRESEXT degree (number of previous solutions)
 //   rpar[10] = wall seconds spent inside the timed CPS call(s) (MINVCG: rpar[42],
 //   since rpar[0..nshift) holds the per-shift residuals)
 //   par: 0 mass, 1 M5 (dwf_height), 2 a5_inv, 3 mobius b, 4 mobius c, 5 stop_rsd,
@@ -59,7 +61,8 @@
 USING_NAMESPACE_CPS
 
 enum { OP_DSLASH = 1, OP_MATPC = 2, OP_MDAGM = 3, OP_INVCG = 4, OP_MINVCG = 5,
-       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9, OP_FCONVERT = 10 };
+       OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9, OP_FCONVERT = 10,
+       OP_MINRESEXT = 11 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -253,6 +256,29 @@ int main(int argc, char **argv) {
     out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
     sfree(fin);
     sfree(fout);
+  } else if (op == OP_MINRESEXT) {
+    // phi, then degree previous solutions; returns psi, the orthonormalised
+    // solutions and their MatPcDagMatPc images.
+    const int degree = (int)hdr[17];
+    if (degree < 0 || degree > 16) die("degree out of range");
+    read_all(fi, in, fsz * sizeof(double));
+    std::vector<Vector *> v(degree > 0 ? degree : 1), vm(degree > 0 ? degree : 1);
+    for (int i = 0; i < degree; i++) {
+      v[i] = (Vector *)smalloc(fsz * sizeof(double));
+      vm[i] = (Vector *)smalloc(fsz * sizeof(double));
+      read_all(fi, v[i], fsz * sizeof(double));
+      memset(vm[i], 0, fsz * sizeof(double));
+    }
+    DiracOp *d = 0;
+    if (action == 0) d = new DiracOpWilson(lat, out, in, &cg_arg, CNV_FRM_NO);
+    else if (action == 1) d = new DiracOpDwf(lat, out, in, &cg_arg, CNV_FRM_NO);
+    else d = new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
+    d->MinResExt(out, in, v.data(), vm.data(), degree);
+    delete d;
+    out_payload.assign((double *)out, (double *)out + fsz);
+    for (int i = 0; i < degree; i++) out_payload.insert(out_payload.end(), (double *)v[i], (double *)v[i] + fsz);
+    for (int i = 0; i < degree; i++) out_payload.insert(out_payload.end(), (double *)vm[i], (double *)vm[i] + fsz);
+    for (int i = 0; i < degree; i++) { sfree(v[i]); sfree(vm[i]); }
   } else if (op == OP_FCONVERT) {
     const size_t full = 2 * fsz;  // both checkerboards
     Vector *f = (Vector *)smalloc(full * sizeof(double));

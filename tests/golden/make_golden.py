@@ -145,6 +145,45 @@ def gen_fconvert():
     return rec
 
 
+MINRESEXT_DEGREE = 4
+
+
+def minresext_inputs(rec):
+    """Source and previous solutions of the MinResExt fixtures (seed+600.. Gaussian)."""
+    dims = tuple(int(d) for d in rec["dims"])
+    n = int(np.prod(dims)) // 2 * int(rec.get("ls", 1))
+    seed = int(rec["seed"])
+    phi = fields.random_source(n, seed + 600)
+    prev = [fields.random_source(n, seed + 601 + i) for i in range(MINRESEXT_DEGREE)]
+    return phi, prev
+
+
+def gen_minresext(name, action, dims, ls, eps, seed, mass, extra):
+    """DiracOp::MinResExt: the guess psi in full, the orthonormalised previous
+    solutions and their MatPcDagMatPc images as SHA-256 digests."""
+    u = fields.random_gauge(dims, eps, seed)
+    base = {"dims": np.array(dims), "ls": ls, "seed": seed}
+    phi, prev = minresext_inputs(base)
+    _, _, pay = refrun.run(refrun.OP_MINRESEXT, action, dims, u, [phi] + prev, ls=ls, mass=mass,
+                           degree=MINRESEXT_DEGREE, threads=1, **extra)
+    n = phi.size
+    d = MINRESEXT_DEGREE
+    rec = {"gauge_sha": sha(u), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed, "mass": mass,
+           "psi": pay[:n], "v_sha": sha(pay[n:(1 + d) * n]), "vm_sha": sha(pay[(1 + d) * n:])}
+    for k, v in extra.items():
+        rec[k] = v
+    return rec
+
+
+def main_minresext():
+    for case in CASES:
+        if "bc_t" in case[7]:
+            continue
+        rec = gen_minresext(*case)
+        np.savez_compressed(os.path.join(OUT, "minresext_" + case[0] + ".npz"), **rec)
+        print("wrote minresext_" + case[0])
+
+
 def main():
     if not refrun.available():
         sys.exit("oracle/_ref/cpsref missing: run oracle/build_ref.sh first")
@@ -156,6 +195,7 @@ def main():
     print("wrote wilson_8x8x8x8_cg")
     main_matinv()
     main_fconvert()
+    main_minresext()
 
 
 def main_matinv():
@@ -177,5 +217,7 @@ if __name__ == "__main__":
         main_matinv()
     elif "--fconvert" in sys.argv:
         main_fconvert()
+    elif "--minresext" in sys.argv:
+        main_minresext()
     else:
         main()

@@ -108,3 +108,21 @@ def test_fermion_convert_matches_reference(action, order):
         perm = rec[f"{action}_dir{direction}"]
         np.testing.assert_array_equal(np.floor(out[:, 0]).astype(np.int32), perm)
         np.testing.assert_array_equal(out, coded_field(dims, ls).reshape(-1, 24)[perm])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_minresext_bitexact(name):
+    """DiracOp::MinResExt (chronological initial guess): the guess, the
+    orthonormalised previous solutions and their MatPcDagMatPc images."""
+    import os
+    from tests.golden.make_golden import minresext_inputs
+    from tests.golden_util import sha
+    rec = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"minresext_{name}.npz")))
+    from cps_public_b200 import fields
+    u = fields.random_gauge(tuple(int(d) for d in rec["dims"]), float(rec["eps"]), int(rec["seed"]))
+    assert sha(u) == str(rec["gauge_sha"])
+    op = make_op(rec, u, name.split("_")[0])
+    phi, prev = minresext_inputs(rec)
+    psi, v, vm, err = op.minresext(phi, prev)
+    np.testing.assert_array_equal(psi, rec["psi"])
+    assert sha(np.concatenate(v)) == str(rec["v_sha"]) and sha(np.concatenate(vm)) == str(rec["vm_sha"])
