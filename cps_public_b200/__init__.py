@@ -256,6 +256,35 @@ class Server:
         self._live[rid.value] = (xs, bs, xp, bp, op)  # keep the buffers alive until wait()
         return rid.value
 
+    def submit_minvcg(self, op: DiracOp, src, shifts, rsd, ms_type=MULTI, alpha=None, max_num_iter=5000,
+                      precision=F64) -> int:
+        """Queues a multishift solve (DiracOp::MInvCG); collect it with wait_minvcg."""
+        ns = len(shifts)
+        nvec = 1 if ms_type == SINGLE else ns
+        xs = [np.zeros(op.n) for _ in range(nvec)]
+        b = op._v(src)
+        rs = np.array(rsd, np.float64)
+        sh = np.array(shifts, np.float64)
+        al = np.ones(ns) if alpha is None else np.array(alpha, np.float64)
+        a = CgArg(float(np.min(rs)), max_num_iter, precision, 0.1, 0)
+        xp = (_lib._dp * nvec)(*[ptr(x) for x in xs])
+        rid = C.c_ulonglong()
+        check(_lib.load().cpsb_serve_submit_minvcg(self.h, op.gauge.h, C.byref(op.p), C.byref(a), xp, ptr(b), ptr(sh),
+                                                   ns, ptr(rs), ms_type, ptr(al), C.byref(rid)),
+              "cpsb_serve_submit_minvcg")
+        self._live[rid.value] = (xs, b, xp, rs, sh, al, op)
+        return rid.value
+
+    def wait_minvcg(self, rid: int):
+        """Returns (solutions, SolveResult, per-shift residuals, latency in ms)."""
+        xs, rs = self._live[rid][0], self._live[rid][3]
+        res = (SolveResult * 1)()
+        lat = C.c_double()
+        rc = _lib.load().cpsb_serve_wait(self.h, rid, res, C.byref(lat))
+        self._live.pop(rid, None)
+        check(rc, "cpsb_serve_wait")
+        return xs, res[0], rs, lat.value
+
     def done(self, rid: int) -> bool:
         d = C.c_int()
         check(_lib.load().cpsb_serve_poll(self.h, rid, C.byref(d)), "cpsb_serve_poll")

@@ -22,7 +22,7 @@ MULTI, SINGLE = 0, 1
 FERMION_CB, FERMION_4D_EE = 0, 1
 
 SYMBOLS = [
-    "cpsb_init", "cpsb_error_string", "cpsb_last_error", "cpsb_mem_info", "cpsb_gauge_load", "cpsb_gauge_free", "cpsb_dslash",
+    "cpsb_init", "cpsb_serve_submit_minvcg", "cpsb_error_string", "cpsb_last_error", "cpsb_mem_info", "cpsb_gauge_load", "cpsb_gauge_free", "cpsb_dslash",
     "cpsb_matpc", "cpsb_mdagm", "cpsb_invcg", "cpsb_invcg_multi", "cpsb_minvcg", "cpsb_matinv", "cpsb_invcg_dev",
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches",
@@ -98,6 +98,8 @@ def load():
     lib.cpsb_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_ulonglong]
     lib.cpsb_serve_submit.argtypes = [C.c_void_p, C.c_void_p, P, A, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
                                       C.POINTER(C.c_ulonglong)]
+    lib.cpsb_serve_submit_minvcg.argtypes = [C.c_void_p, C.c_void_p, P, A, C.POINTER(_dp), _dp, _dp, C.c_int, _dp,
+                                             C.c_int, _dp, C.POINTER(C.c_ulonglong)]
     lib.cpsb_serve_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
     lib.cpsb_serve_wait.argtypes = [C.c_void_p, C.c_ulonglong, R, _dp]
     lib.cpsb_serve_stats.argtypes = [C.c_void_p, C.POINTER(ServeStats)]

@@ -166,8 +166,10 @@ int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_
 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
 
+// refiner: the one-RHS solver for the per-shift refinement of reduced-precision
+// Krylov runs (nullptr: the library's cached one, taken under its lock).
 int multishift(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, Field &b64, std::vector<Field> &x,
                const double *shift, int nshift, double *rsd, int type, const double *alpha, cpsb_solve_result *res,
-               cudaStream_t st);
+               cudaStream_t st, CgSolver *refiner = nullptr);
 
 }  // namespace cpsb

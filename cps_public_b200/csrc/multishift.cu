@@ -243,7 +243,7 @@ Scal2 scal_all(double a, double b) {
 // one for SINGLE).  Returns the CPS iteration count in res->iters.
 int multishift(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, Field &chi, std::vector<Field> &x,
                const double *shift, int nshift, double *rsd, int type, const double *alpha, cpsb_solve_result *res,
-               cudaStream_t st) {
+               cudaStream_t st, CgSolver *refiner) {
   auto t0 = std::chrono::steady_clock::now();
   if (nshift < 1 || nshift > MAX_SHIFT) throw Error{CPSB_ERR_ARG, "nshift must be in [1, 32]"};
   for (int s = 1; s < nshift; s++)
@@ -366,8 +366,9 @@ int multishift(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, Field
   } else {
     // Refine every shift with mixed-precision CG on (A + shift_s) to its own
     // tolerance, checked with the FP64 true residual.
-    CgSolver *cg = get_solver(G, p, prec, 1);
-    std::lock_guard<std::mutex> lk(cg->busy);
+    CgSolver *cg = refiner ? refiner : get_solver(G, p, prec, 1);
+    std::unique_lock<std::mutex> lk(cg->busy, std::defer_lock);
+    if (!refiner) lk.lock();  // the cached solver may be shared between threads
     CK(launch_convert(P64, cg->b64.ptr(), P64, chi.ptr(), n, st));
     for (int s = 0; s < nshift; s++) {
       CK(launch_convert(P64, cg->x64.ptr(), px, psi[s].ptr(), n, st));

@@ -21,6 +21,9 @@
 //    arithmetic is the same whether it runs alone or in a mix: the result
 //    depends only on the request (and on the launch shapes the autotuner has
 //    cached for its operator shapes).
+//  * Multishift requests (cpsb_serve_submit_minvcg, DiracOp::MInvCG as the
+//    RHMC pseudofermion and pole solves issue them) are one work item each with
+//    their own refinement solver, so the solves of many pseudofermions overlap.
 //  * Latency is host time from submission to the completion of the last item.
 #include <string.h>
 
@@ -56,6 +59,18 @@ static size_t solve_footprint(const cpsb_dirac_params &p, long n, int sloppy, in
   return b + (size_t)(8u << 20);                         // reduction slots, state, graph
 }
 
+// Device bytes of one multishift solve (multishift.cu): FP64 source and
+// solutions, Krylov vectors in the Krylov precision, the operator's
+// temporaries, and the one-RHS refinement solver of reduced-precision runs.
+static size_t multishift_footprint(const cpsb_dirac_params &p, long n, int prec, int nshift, int nvec) {
+  const int op_tmp = p.action == CPSB_MOBIUS ? 3 : 2;
+  const int px = prec == P64 ? P64 : P32;
+  size_t b = field_bytes(P64, n) * (2 + nvec);                        // chi, staging, x[s]
+  b += field_bytes(prec, n) * (2 + nshift + op_tmp) + field_bytes(px, n) * nshift;  // r, Ap, p_s, temps; psi_s
+  if (prec != P64) b += solve_footprint(p, n, prec, 1);
+  return b + (size_t)(8u << 20);
+}
+
 struct ServeRequest {
   unsigned long long id = 0;
   cpsb_gauge h = nullptr;
@@ -65,6 +80,12 @@ struct ServeRequest {
   std::vector<double *> x;
   std::vector<const double *> b;
   std::vector<cpsb_solve_result> res;
+  // multishift requests (DiracOp::MInvCG): shifts, per-shift tolerances in and
+  // reported residuals out, type and weights
+  bool multishift = false;
+  std::vector<double> shift, alpha;
+  double *rsd = nullptr;
+  int ms_type = CPSB_MULTI;
   int items_left = 0;
   int status = CPSB_OK;
   std::string err;
@@ -122,6 +143,31 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
   Gauge *G = &r.h->g;
   const long n = cb_sites(r.h, &r.p);
   const size_t each = (size_t)n * 24 * sizeof(double);
+  if (r.multishift) {
+    const int nshift = (int)r.shift.size();
+    const int nvec = r.ms_type == CPSB_SINGLE ? 1 : nshift;
+    Field chi(P64, n);
+    DevBuf stage(each);
+    CK(cudaMemcpyAsync(stage.p, r.b[0], each, cudaMemcpyHostToDevice, st));
+    CK(launch_pack(P64, chi.ptr(), (const double *)stage.p, n, st));
+    std::vector<Field> xs(nvec);
+    for (int i = 0; i < nvec; i++) {
+      xs[i].create(P64, n);
+      CK(cudaMemsetAsync(xs[i].data.p, 0, xs[i].data.bytes, st));
+    }
+    // a private refinement solver: concurrent requests do not queue on the cached one
+    std::unique_ptr<CgSolver> refiner;
+    if (r.a.precision != P64) refiner.reset(new CgSolver(G, r.p, r.a.precision, 1));
+    const int rc = multishift(G, r.p, r.a, chi, xs, r.shift.data(), nshift, r.rsd, r.ms_type,
+                              r.alpha.empty() ? nullptr : r.alpha.data(), r.res.data(), st, refiner.get());
+    for (int i = 0; i < nvec; i++) {
+      CK(launch_unpack(P64, (double *)stage.p, xs[i].ptr(), n, st));
+      CK(cudaMemcpyAsync(r.x[i], stage.p, each, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (rc != CPSB_OK) throw Error{rc, "multishift solve did not converge"};
+    return;
+  }
   CgSolver s(G, r.p, r.a.precision, it.nrhs);
   DevBuf stage(each);
   for (int q = 0; q < it.nrhs; q++) {
@@ -274,6 +320,55 @@ int cpsb_serve_submit(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p,
         S.queue.push_back(ServeItem{r.get(), r0, m, solve_footprint(*p, n, a->precision, m)});
         r0 += m;
       }
+      *id = r->id;
+      S.reqs[r->id] = std::move(r);
+    }
+    S.cv_work.notify_all();
+    return CPSB_OK;
+  });
+}
+
+int cpsb_serve_submit_minvcg(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a,
+                             double **x, const double *b, const double *shift, int nshift, double *rsd, int type,
+                             const double *alpha, unsigned long long *id) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    if (!srv || !id || !x || !b || !shift || !rsd || nshift < 1 || nshift > 32)
+      throw Error{CPSB_ERR_ARG, "bad multishift submit arguments"};
+    if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE"};
+    if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
+    if (p->action == CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
+      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
+    const int nvec = type == CPSB_SINGLE ? 1 : nshift;
+    for (int i = 0; i < nvec; i++)
+      if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
+    Server &S = srv->s;
+    const long n = cb_sites(h, p);
+    const size_t bytes = multishift_footprint(*p, n, a->precision, nshift, nvec);
+    if (bytes > S.budget) throw Error{CPSB_ERR_OOM, "this multishift solve exceeds the server's HBM budget"};
+    std::unique_ptr<ServeRequest> r(new ServeRequest);
+    r->h = h;
+    r->p = *p;
+    r->a = *a;
+    r->nrhs = 1;
+    r->multishift = true;
+    r->x.assign(x, x + nvec);
+    r->b.assign(&b, &b + 1);
+    r->res.assign(1, cpsb_solve_result());
+    r->shift.assign(shift, shift + nshift);
+    if (alpha) r->alpha.assign(alpha, alpha + nshift);
+    r->rsd = rsd;
+    r->ms_type = type;
+    r->items_left = 1;
+    {
+      std::lock_guard<std::mutex> lk(S.mu);
+      if (S.stopping) throw Error{CPSB_ERR_BUSY, "server is shutting down"};
+      r->id = S.next_id++;
+      r->t_submit = now_ms();
+      if (S.t_first_submit < 0) S.t_first_submit = r->t_submit;
+      S.queue.push_back(ServeItem{r.get(), 0, 1, bytes});
       *id = r->id;
       S.reqs[r->id] = std::move(r);
     }

@@ -267,6 +267,14 @@ typedef struct {
 int cpsb_serve_create(cpsb_server *s, int slots, double hbm_fraction, unsigned long long hbm_bytes);
 int cpsb_serve_submit(cpsb_server s, cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nrhs,
                       double **x, const double *const *b, unsigned long long *id);
+/* Queues a multishift solve (the arguments and results of cpsb_minvcg; x[],
+ * b, shift, rsd and alpha must stay valid until cpsb_serve_wait returns, which
+ * fills one cpsb_solve_result).  RHMC callers submit the solves of all their
+ * pseudofermions (Lattice::FmatEvlMInv per pseudofermion,
+ * alg/alg_int/alg_action_rational.C:259-359) and they overlap on the device. */
+int cpsb_serve_submit_minvcg(cpsb_server s, cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a,
+                             double **x, const double *b, const double *shift, int nshift, double *rsd, int type,
+                             const double *alpha, unsigned long long *id);
 int cpsb_serve_poll(cpsb_server s, unsigned long long id, int *done);
 int cpsb_serve_wait(cpsb_server s, unsigned long long id, cpsb_solve_result *res, double *latency_ms);
 int cpsb_serve_stats(cpsb_server s, cpsb_serve_stats_t *st);

@@ -97,3 +97,27 @@ def test_request_larger_than_budget_is_refused(setup):
         srv.submit(op, srcs, stop_rsd=tol, precision=prec)
     assert e.value.code == -3
     srv.close()
+
+
+def test_multishift_requests_overlap_and_match(setup):
+    """RHMC-style batch: the multishift solves of several pseudofermions
+    submitted at once equal the same solves run one at a time (cpsb_minvcg),
+    bit for bit, for the FP64 and the FP32-Krylov-plus-refinement forms."""
+    cb, gauges, _ = setup
+    from cps_public_b200 import fields
+    op = cb.DiracOp(gauges[1], "dwf", mass=0.05, ls=8, m5=1.8)
+    shifts = [0.001, 0.01, 0.1, 1.0]
+    srcs = [fields.random_source(op.n // 24, 700 + i) for i in range(4)]
+    for prec in (cb.F64, cb.F32):
+        alone = [op.MInvCG(s, shifts, [1e-10] * 4, precision=prec) for s in srcs]
+        srv = cb.Server(slots=4)
+        ids = [srv.submit_minvcg(op, s, shifts, [1e-10] * 4, precision=prec) for s in srcs]
+        got = [srv.wait_minvcg(i) for i in ids]
+        st = srv.stats()
+        srv.close()
+        assert st["completed"] == 4 and st["peak_running"] >= 2
+        for (xa, ra, rsa), (xm, rm, rsm, _) in zip(alone, got):
+            assert rm.status == 0 and ra.iters == rm.iters
+            np.testing.assert_array_equal(rsa, rsm)
+            for k in range(len(shifts)):
+                np.testing.assert_array_equal(xa[k], xm[k])
