@@ -12,6 +12,8 @@ struct Reduce {
   double *result;
 };
 
+struct CgState;  // cg_state.h
+
 struct DslashArgs {
   Geom g;
   GaugePtr U;
@@ -27,6 +29,12 @@ struct DslashArgs {
   Reduce red;             // |out|^2 per RHS when requested
   const int *skip;        // per-RHS: nonzero skips that RHS (device memory), may be null
   int sl;                 // slice lanes per block (set by the launcher)
+  // Fused CG residual update (parity-class FP32 / 16-bit kernels only): when
+  // cg is set, out = x + a D in is not stored; instead r -= alpha (out +
+  // shift p) with alpha from cg, |r|^2 per RHS is reduced, and the last block
+  // advances the recurrence scalars as the r-update kernel of blas.cu does.
+  CgState *cg;
+  SpinorPtr cg_r, cg_p;
 };
 
 // Kernel-launch accounting (cpsb_kernel_launches): every launcher calls

@@ -260,6 +260,7 @@ static cudaError_t dslash_launch_v(DslashArgs A, int xpay, int norm, cudaStream_
 // Launch shapes the autotuner chooses from: (threads, min blocks/SM, link cache).
 template <int P>
 static cudaError_t dslash_launch_p(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
+  if (A.cg) return cudaErrorNotSupported;  // the fused residual update is FP32 / 16-bit only
   switch (variant) {
     case 1: return dslash_launch_v<P, 128, 4, false>(A, xpay, norm, st);
     case 2: return dslash_launch_v<P, 256, 2, false>(A, xpay, norm, st);

@@ -631,7 +631,7 @@ template <bool DAG> __device__ __forceinline__ HfX2 umul(const float2 *sh, int T
 // WG lanes that share a site read the same link words from shared memory
 // (one wavefront serves them) while each slice's sites stay one 16-byte-per-
 // site contiguous segment per chunk.
-template <int P, int NT, int MINB, int SL, int DEPTH, int WG, bool XPAY, bool NORM>
+template <int P, int NT, int MINB, int SL, int DEPTH, int WG, bool XPAY, bool NORM, bool CGR = false>
 __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
   constexpr int TX = NT / SL;
   static_assert(WG == 1 || WG == SL, "slice lanes are either all inside a warp or all across warps");
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
   const int ntiles = (g.n4cb + TX - 1) / TX;
   const int nclass = A.five_d ? 2 : 1;
   const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
-  if (NORM)
+  if (NORM || CGR)
     for (int q = 0; q < g.nrhs; q++) nrm_sh[q * NT + threadIdx.x] = 0;
   const float2 a2 = f2b((float)A.a);
   const float sdag = A.dag ? -1.f : 1.f;
@@ -759,11 +759,37 @@ __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
             o.im[p][cc] = mul2(a2, o.im[p][cc]);
           }
       }
-      const double n2 = store_x2<P>(A.out, (long)i, o);
-      if (NORM) nrm_sh[rhs * NT + threadIdx.x] += n2;
+      if (CGR) {
+        // r -= alpha (Ap + shift p), Ap = o held in registers (cg_r_update of blas.cu)
+        const CgState *S = A.cg;
+        const double sigma = S->shift;
+        const float alpha = (float)(S->rr[rhs] / (S->d[rhs] + sigma * S->pp[rhs]));
+        float rn;
+        SpX2 rv = load<P>(A.cg_r, i, &rn);
+        float pn = 0.f;
+        SpX2 pv;
+        if (sigma != 0.0) pv = load<P>(A.cg_p, i, &pn);
+        const float2 ma = f2b(-alpha), rs = f2b(rn), ps = f2b((float)sigma * pn);
+#pragma unroll
+        for (int p = 0; p < 2; p++)
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++) {
+            float2 are = o.re[p][cc], aim = o.im[p][cc];
+            if (sigma != 0.0) {
+              are = fma2(ps, pv.re[p][cc], are);
+              aim = fma2(ps, pv.im[p][cc], aim);
+            }
+            rv.re[p][cc] = fma2(ma, are, P == P16 ? mul2(rv.re[p][cc], rs) : rv.re[p][cc]);
+            rv.im[p][cc] = fma2(ma, aim, P == P16 ? mul2(rv.im[p][cc], rs) : rv.im[p][cc]);
+          }
+        nrm_sh[rhs * NT + threadIdx.x] += store_x2<P>(A.cg_r, (long)i, rv);
+      } else {
+        const double n2 = store_x2<P>(A.out, (long)i, o);
+        if (NORM) nrm_sh[rhs * NT + threadIdx.x] += n2;
+      }
     }
   }
-  if (NORM) {
+  if (NORM || CGR) {
     for (int q = 0; q < g.nrhs; q++) {
       const double bs = block_sum<NT>(nrm_sh[q * NT + threadIdx.x], red);
       if (threadIdx.x == 0) A.red.partial[q * gridDim.x + blockIdx.x] = bs;
@@ -771,7 +797,34 @@ __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
     if (last_block(A.red.ticket, gridDim.x)) {
       for (int q = 0; q < g.nrhs; q++) {
         double t = ordered_sum<NT>(A.red.partial + q * gridDim.x, gridDim.x, red);
-        if (threadIdx.x == 0 && !(A.skip && A.skip[q])) A.red.result[q] = t;
+        if (threadIdx.x == 0 && !(A.skip && A.skip[q])) {
+          if (!CGR) {
+            A.red.result[q] = t;
+          } else {
+            // the recurrence scalars and the halting decision of cg_r_update (blas.cu)
+            CgState *S = A.cg;
+            const double c = t;
+            const double rprev = S->rr[q];
+            const double d = S->d[q] + S->shift * S->pp[q];
+            S->alpha[q] = rprev / d;
+            S->rr_prev[q] = rprev;
+            S->rr[q] = c;
+            S->beta[q] = c / rprev;
+            S->iters[q] += 1;
+            int reason = HALT_NONE;
+            const double rn = sqrt(c);
+            if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
+            else if (c <= S->stp[q]) reason = HALT_CONVERGED;
+            else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
+            else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
+            if (rn > S->maxr[q]) S->maxr[q] = rn;
+            if (reason) {
+              S->halt[q] = 1;
+              S->reason[q] = reason;
+            }
+            if (A.red.result) A.red.result[q] = c;
+          }
+        }
         __syncthreads();
       }
     }
@@ -780,6 +833,23 @@ __global__ void __launch_bounds__(NT, MINB) kernel(DslashArgs A) {
 
 template <int P, int NT, int MINB, int SL, int DEPTH, int WG>
 static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
+  if (A.cg) {  // fused residual update: xpay hop whose output feeds r -= alpha Ap
+    if (!xpay) return cudaErrorInvalidValue;
+    constexpr int TX = NT / SL;
+    const long units = (long)((A.g.n4cb + TX - 1) / TX) * (A.five_d ? 2 : 1);
+    const long nb = units < 148L * 16 ? units : 148L * 16;
+    const size_t shm = (size_t)72 * TX * sizeof(float2) + sizeof(double) * NT * A.g.nrhs;
+    if (shm > 200 * 1024) return cudaErrorNotSupported;
+    static bool attr = false;
+    if (shm + 1024 > 48 * 1024 && !attr) {
+      const cudaError_t e = cudaFuncSetAttribute((const void *)kernel<P, NT, MINB, SL, DEPTH, WG, true, false, true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    kernel<P, NT, MINB, SL, DEPTH, WG, true, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
+    return launched();
+  }
   constexpr int TX = NT / SL;
   const int nclass = A.five_d ? 2 : 1;
   const int nsl = A.five_d ? (A.g.ls + 1) / 2 : A.g.ls;
@@ -814,6 +884,7 @@ static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
 // slice lanes per warp).
 template <int P>
 static cudaError_t dslash_fp32x2_launch(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
+  if (A.cg && variant < 7) variant = 7;  // the fused residual update exists in the parity-class kernel only
   switch (variant) {
     case 7: return x3::launch_v<P, 128, 4, 4, 8, 4>(A, xpay, norm, st);
     case 8: return x3::launch_v<P, 128, 4, 4, 8, 1>(A, xpay, norm, st);

@@ -121,6 +121,13 @@ struct Operator {
   void mdagm(const Field &out, const Field &in, const Reduce *red, const int *skip, cudaStream_t st) {
     mdagm(out.ptr(), in.ptr(), red, skip, st);
   }
+  // MatPcDagMatPc p with the CG residual update fused into its last hop
+  // (Wilson / DWF in FP32 or 16-bit): |MatPc p|^2 -> red_d, then
+  // r -= alpha (A p + shift p), |r|^2 and the recurrence scalars in S; A p is
+  // not stored (scratch receives it only while a launch shape is being tuned).
+  bool can_fuse_cg_r() const { return prec != P64 && p.action != CPSB_MOBIUS; }
+  void mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip, CgState *S,
+                  const SpinorPtr &r, const Reduce *red_r, cudaStream_t st);
   // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
   // (zmobius_m5inv, dag 0); out = D4(cb) in (zmobius_dslash_4, dag 0);
   // out = x + f H5 in (zmobius_kappa_dslash_5_plus_cmplx with factor f, dag 0).

@@ -19,6 +19,7 @@
 #include <atomic>
 
 #include "host.h"
+#include "cg_state.h"
 
 namespace cpsb {
 
@@ -309,6 +310,37 @@ void Operator::mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const 
   Reduce none;
   memset(&none, 0, sizeof(none));
   CK(launch_m5(prec, 0, geom, out, in, x, h, 1, 0, none, nullptr, st));
+}
+
+void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip,
+                          CgState *S, const SpinorPtr &r, const Reduce *red_r, cudaStream_t st) {
+  if (!can_fuse_cg_r()) throw Error{CPSB_ERR_UNSUPPORTED, "fused residual update needs Wilson / DWF in FP32 / 16-bit"};
+  matpc(t2.ptr(), in, 0, red_d, skip, st);  // |MatPc p|^2 -> d
+  hop(t1.ptr(), t2.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
+  // the last hop of MatPcDag: out = t2 - kappa^2 D t1 = A p, consumed in registers
+  DslashArgs A;
+  memset(&A, 0, sizeof(A));
+  A.g = geom;
+  A.U = G->ptr(prec);
+  A.in = t1.ptr();
+  A.out = scratch;
+  A.x = t2.ptr();
+  A.cb = 0;
+  A.dag = 1;
+  A.five_d = p.action == CPSB_DWF;
+  A.hop5 = p.action == CPSB_DWF;
+  A.hop5_fact = 2.0 * p.a5_inv;
+  A.hop5_wall = -2.0 * p.mass * p.a5_inv;
+  A.a = -kappa * kappa;
+  A.bc_t_sign = G->bc_t ? -1.0 : 1.0;
+  A.skip = skip;
+  // launch shape of the same hop without the fused update (tuned on the scratch output)
+  const int v = tuned_variant(A, prec, 1, 0, st);
+  A.red = *red_r;
+  A.cg = S;
+  A.cg_r = r;
+  A.cg_p = in;
+  CK(launch_dslash(prec, A, 1, 1, v, st));
 }
 
 void Operator::mdagm(const SpinorPtr &out, const SpinorPtr &in, const Reduce *red, const int *skip, cudaStream_t st) {

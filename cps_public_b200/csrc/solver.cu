@@ -77,9 +77,15 @@ void CgSolver::launch_batch(int k, cudaStream_t st) {
   Reduce rd = red_d.r(S->d);
   Reduce rr = red_r.r(nullptr);
   Reduce rp = red_p.r(nullptr);
+  const bool fused = op.can_fuse_cg_r();
   for (int j = 0; j < k; j++) {
-    op.mdagm(ApS, pS, &rd, S->halt, st);
-    CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), pS.ptr(), S, rr, st));
+    if (fused) {
+      // the residual update rides on the last hop of MatPcDagMatPc (A p stays in registers)
+      op.mdagm_cg_r(ApS.ptr(), pS.ptr(), &rd, S->halt, S, rS.ptr(), &rr, st);
+    } else {
+      op.mdagm(ApS, pS, &rd, S->halt, st);
+      CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), pS.ptr(), S, rr, st));
+    }
     CK(launch_cg_xp_update(px, op.prec, op.geom, xx.ptr(), pS.ptr(), rS.ptr(), S, rp, st));
   }
 }
