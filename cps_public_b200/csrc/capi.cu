@@ -4,7 +4,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
+#include <thread>
 #include <complex>
 
 #include "abi.h"
@@ -48,24 +50,56 @@ long cb_sites(cpsb_gauge h, const cpsb_dirac_params *p) {
 namespace {
 
 // Pinned staging buffer reused across calls (grown on demand).
+// Host <-> device staging of CPS-order vectors: two pinned buffers and two
+// device buffers of one vector each.  While vector i is copied by DMA (and
+// packed on the device), vector i+1 is copied into the other pinned buffer by
+// several host threads, so host copy and transfer overlap.
 struct Staging {
-  void *p = nullptr;
+  void *pin[2] = {nullptr, nullptr};
+  DevBuf dev[2];
+  cudaEvent_t done[2] = {nullptr, nullptr};  // last use of pin[k] by the device is over
   size_t bytes = 0;
   std::mutex mu;
-  void *get(size_t n) {
-    if (n > bytes) {
-      if (p) cudaFreeHost(p);
-      p = nullptr;
-      bytes = 0;
-      CK(cudaMallocHost(&p, n));
-      bytes = n;
+  void ensure(size_t n) {
+    if (!done[0]) {
+      CK(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
     }
-    return p;
+    if (n <= bytes) return;
+    for (int k = 0; k < 2; k++) {
+      if (pin[k]) cudaFreeHost(pin[k]);
+      pin[k] = nullptr;
+    }
+    bytes = 0;
+    for (int k = 0; k < 2; k++) {
+      CK(cudaMallocHost(&pin[k], n));
+      dev[k].alloc(n);
+    }
+    bytes = n;
   }
 };
 Staging &staging() {
   static Staging s;
   return s;
+}
+
+// memcpy of large vectors split over host threads.
+void par_copy(void *dst, const void *src, size_t n) {
+  const size_t chunk = 32u << 20;
+  const int nt = (int)std::min<size_t>(8, (n + chunk - 1) / chunk);
+  if (nt <= 1) {
+    memcpy(dst, src, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t part = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const size_t off = (size_t)t * part;
+    if (off >= n) break;
+    const size_t len = std::min(part, n - off);
+    th.emplace_back([=] { memcpy((char *)dst + off, (const char *)src + off, len); });
+  }
+  for (auto &x : th) x.join();
 }
 
 }  // namespace
@@ -191,36 +225,39 @@ namespace {
 // multi-RHS field f one right-hand side at a time through a pinned buffer and
 // a device buffer of one vector, packing each into its slice of f.
 void upload(Field &f, const double *const *host, int nvec, long nsites_each, cudaStream_t st) {
-  static DevBuf tmp;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> lk(mu);
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
-  if (tmp.bytes < each) tmp.alloc(each);
   Staging &sg = staging();
-  std::lock_guard<std::mutex> lk2(sg.mu);
-  void *pin = sg.get(each);
+  std::lock_guard<std::mutex> lk(sg.mu);
+  sg.ensure(each);
   for (int i = 0; i < nvec; i++) {
-    memcpy(pin, host[i], each);
-    CK(cudaMemcpyAsync(tmp.p, pin, each, cudaMemcpyHostToDevice, st));
-    CK(launch_pack(f.prec, f.view((long)i * nsites_each), (const double *)tmp.p, nsites_each, st));
-    CK(cudaStreamSynchronize(st));  // pin and tmp are reused by the next vector
+    const int k = i & 1;
+    CK(cudaEventSynchronize(sg.done[k]));  // the device is done with pin[k] / dev[k]
+    par_copy(sg.pin[k], host[i], each);
+    CK(cudaMemcpyAsync(sg.dev[k].p, sg.pin[k], each, cudaMemcpyHostToDevice, st));
+    CK(launch_pack(f.prec, f.view((long)i * nsites_each), (const double *)sg.dev[k].p, nsites_each, st));
+    CK(cudaEventRecord(sg.done[k], st));
   }
+  CK(cudaStreamSynchronize(st));
 }
 
 void download(double *const *host, int nvec, long nsites_each, const Field &f, cudaStream_t st) {
-  static DevBuf tmp;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> lk(mu);
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
-  if (tmp.bytes < each) tmp.alloc(each);
   Staging &sg = staging();
-  std::lock_guard<std::mutex> lk2(sg.mu);
-  void *pin = sg.get(each);
-  for (int i = 0; i < nvec; i++) {
-    CK(launch_unpack(f.prec, (double *)tmp.p, f.view((long)i * nsites_each), nsites_each, st));
-    CK(cudaMemcpyAsync(pin, tmp.p, each, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    memcpy(host[i], pin, each);
+  std::lock_guard<std::mutex> lk(sg.mu);
+  sg.ensure(each);
+  // vector i is unpacked and transferred while vector i-1 is copied out on the host
+  for (int i = 0; i <= nvec; i++) {
+    if (i < nvec) {
+      const int k = i & 1;
+      CK(launch_unpack(f.prec, (double *)sg.dev[k].p, f.view((long)i * nsites_each), nsites_each, st));
+      CK(cudaMemcpyAsync(sg.pin[k], sg.dev[k].p, each, cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(sg.done[k], st));
+    }
+    if (i > 0) {
+      const int k = (i - 1) & 1;
+      CK(cudaEventSynchronize(sg.done[k]));
+      par_copy(host[i - 1], sg.pin[k], each);
+    }
   }
 }
 
