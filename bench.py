@@ -239,12 +239,16 @@ def run_ours(args):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         infos = []
         torch.cuda.synchronize()
+        # NVTX range "timed_<arm>": lets a profiler select one arm's timed solves
+        # (ncu --nvtx --nvtx-include "timed_f16_mixed_x12/").
+        torch.cuda.nvtx.range_push("timed_" + name)
         for k in range(args.steps):
             batch(args.warmup + k, nrhs)
             ev[k][0].record(stream)
             infos += solve_on_device(nrhs, prec)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if head:
             lib.cpsb_kernel_launches(C.byref(launches1))
             clocks = sampler.stop()
