@@ -175,6 +175,30 @@ class DiracOp:
         r.rc = rc
         return out, r
 
+    def Dminus(self, x_full):
+        """DiracOpMobius::Dminus on a full vector (4-D-even half first)."""
+        x = np.ascontiguousarray(x_full, np.float64)
+        if x.size != 2 * self.n:
+            raise ValueError(f"full vector has {x.size} reals, expected {2 * self.n}")
+        out = np.empty(2 * self.n)
+        check(_lib.load().cpsb_dminus(self.gauge.h, C.byref(self.p), ptr(out), ptr(x)), "cpsb_dminus")
+        return out
+
+    def FmatInv(self, src_full, guess_full=None, dminus=0, stop_rsd=1e-10, max_num_iter=5000, precision=F64,
+                reliable_delta=0.1, batch=0):
+        """Lattice::FmatInv(..., dminus): for Mobius with dminus the source is
+        replaced by Dminus(source) before MatInv; other actions ignore dminus."""
+        src = np.ascontiguousarray(src_full, np.float64)
+        if src.size != 2 * self.n:
+            raise ValueError(f"full vector has {src.size} reals, expected {2 * self.n}")
+        out = np.zeros(2 * self.n) if guess_full is None else np.array(guess_full, np.float64)
+        a = CgArg(stop_rsd, max_num_iter, precision, reliable_delta, batch)
+        r = SolveResult()
+        rc = check(_lib.load().cpsb_fmatinv(self.gauge.h, C.byref(self.p), C.byref(a), ptr(out), ptr(src),
+                                            int(dminus), C.byref(r)), "cpsb_fmatinv")
+        r.rc = rc
+        return out, r
+
     def MinResExt(self, phi, prev):
         """DiracOp::MinResExt: chronological guess from previous solutions.
         Returns (psi, orthonormalised prev, MatPcDagMatPc of them, |phi - A psi|/|phi|)."""
@@ -212,10 +236,11 @@ def fmat_evl_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
     return r.iters, x, r.true_rsd
 
 
-def fmat_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
-    """Lattice::FmatInv (lattice.h:1114): full-lattice solve; returns (iterations, f_out, true_res)."""
-    out, r = op.MatInv(f_in, f_out, cg_arg.get("stop_rsd", 1e-10), cg_arg.get("max_num_iter", 5000),
-                       cg_arg.get("precision", F64))
+def fmat_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None, dminus=0):
+    """Lattice::FmatInv (lattice.h:1114, dminus form :1127): full-lattice solve;
+    returns (iterations, f_out, true_res)."""
+    out, r = op.FmatInv(f_in, f_out, dminus, cg_arg.get("stop_rsd", 1e-10), cg_arg.get("max_num_iter", 5000),
+                        cg_arg.get("precision", F64))
     return r.iters, out, r.true_rsd
 
 

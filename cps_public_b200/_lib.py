@@ -23,7 +23,7 @@ FERMION_CB, FERMION_4D_EE = 0, 1
 
 SYMBOLS = [
     "cpsb_init", "cpsb_serve_submit_minvcg", "cpsb_error_string", "cpsb_last_error", "cpsb_mem_info", "cpsb_gauge_load", "cpsb_gauge_free", "cpsb_dslash",
-    "cpsb_matpc", "cpsb_mdagm", "cpsb_invcg", "cpsb_invcg_multi", "cpsb_minvcg", "cpsb_matinv", "cpsb_invcg_dev",
+    "cpsb_matpc", "cpsb_mdagm", "cpsb_invcg", "cpsb_invcg_multi", "cpsb_minvcg", "cpsb_matinv", "cpsb_fmatinv", "cpsb_dminus", "cpsb_invcg_dev",
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches",
     "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
@@ -88,6 +88,8 @@ def load():
     lib.cpsb_invcg_multi.argtypes = [C.c_void_p, P, A, C.c_int, C.POINTER(_dp), C.POINTER(_dp), R]
     lib.cpsb_minvcg.argtypes = [C.c_void_p, P, A, C.POINTER(_dp), _dp, _dp, C.c_int, _dp, C.c_int, _dp, R]
     lib.cpsb_matinv.argtypes = [C.c_void_p, P, A, _dp, _dp, R]
+    lib.cpsb_fmatinv.argtypes = [C.c_void_p, P, A, _dp, _dp, C.c_int, R]
+    lib.cpsb_dminus.argtypes = [C.c_void_p, P, _dp, _dp]
     lib.cpsb_invcg_dev.argtypes = [C.c_void_p, P, A, C.c_void_p, C.c_void_p, R, C.c_void_p]
     lib.cpsb_invcg_multi_dev.argtypes = [C.c_void_p, P, A, C.c_int, C.c_void_p, C.c_void_p, R, C.c_void_p]
     lib.cpsb_mdagm_dev.argtypes = [C.c_void_p, P, C.c_void_p, C.c_void_p, _dp, C.c_void_p]

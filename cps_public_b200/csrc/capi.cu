@@ -489,8 +489,35 @@ int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg 
   });
 }
 
-int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
-                cpsb_solve_result *res) {
+// out = fa x + fb y (y optional) on FP64 fields of one right-hand side.
+static void lin64(const Geom &g, const Field &o, double fa, const Field &x, double fb, const Field *y,
+                  cudaStream_t st) {
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  Scal2 c;
+  for (int i = 0; i < MAX_RHS; i++) {
+    c.a[i] = fa;
+    c.b[i] = fb;
+  }
+  CK(launch_axpby(P64, o.ptr(), P64, x.ptr(), P64, y ? y->ptr() : SpinorPtr{}, g, c, nullptr, none, 0, st));
+}
+
+// DiracOpMobius::Dminus (d_op_mobius.C:745-777): mobius_dminus (mobius_dminus.C:
+// 29-86) hops each checkerboard into the other on every s slice with the fixed
+// 4-D parity of the input, on -c/2 times the input; then out = -(k in + out),
+// k = c(4 - M5) - a5_inv.  Here: out_x = (c/2) D_W in_y - k in_x.
+static void mobius_dminus_dev(Operator &op, const cpsb_dirac_params &p, const Field &out_e, const Field &out_o,
+                              const Field &in_e, const Field &in_o, cudaStream_t st) {
+  const double c = p.mobius_c;
+  const double k = 0.5 * (2 * (c * (4 - p.m5) - p.a5_inv));
+  op.hop(out_e.ptr(), in_o.ptr(), 1, 0, 1.0, nullptr, nullptr, nullptr, st);
+  op.hop(out_o.ptr(), in_e.ptr(), 0, 0, 1.0, nullptr, nullptr, nullptr, st);
+  lin64(op.geom, out_e, 0.5 * c, out_e, -k, &in_e, st);
+  lin64(op.geom, out_o, 0.5 * c, out_o, -k, &in_o, st);
+}
+
+static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out,
+                       const double *in, int dminus, cpsb_solve_result *res) {
   return guarded([&] {
     need_init();
     check_params(h, p);
@@ -508,15 +535,14 @@ int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
     upload(fin_c, &in_c, 1, n, st);
     upload(fin_e, &in_e, 1, n, st);
     upload(fout_c, (const double *const *)&out_c, 1, n, st);
-    Reduce none;
-    memset(&none, 0, sizeof(none));
+    if (mob && dminus) {
+      // f_mobius.C:45-117: the source becomes Dminus(source) before MatInv
+      mobius_dminus_dev(op, *p, t, t2, fin_e, fin_c, st);
+      CK(cudaMemcpyAsync(fin_e.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(fin_c.data.p, t2.data.p, t2.data.bytes, cudaMemcpyDeviceToDevice, st));
+    }
     auto lin = [&](const Field &o, double fa, const Field &x, double fb, const Field *y) {
-      Scal2 c;
-      for (int i = 0; i < MAX_RHS; i++) {
-        c.a[i] = fa;
-        c.b[i] = fb;
-      }
-      CK(launch_axpby(P64, o.ptr(), P64, x.ptr(), P64, y ? y->ptr() : SpinorPtr{}, g, c, nullptr, none, 0, st));
+      lin64(g, o, fa, x, fb, y, st);
     };
     double kb = 0;
     if (!mob) {
@@ -556,6 +582,38 @@ int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
     download(&out_c, 1, n, fout_c, st);
     download(&out_e, 1, n, fout_e, st);
     return rc;
+  });
+}
+
+int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
+                cpsb_solve_result *res) {
+  return matinv_impl(h, p, a, out, in, 0, res);
+}
+
+int cpsb_fmatinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
+                 int dminus, cpsb_solve_result *res) {
+  return matinv_impl(h, p, a, out, in, dminus, res);
+}
+
+int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (p->action != CPSB_MOBIUS) throw Error{CPSB_ERR_ARG, "Dminus is a Mobius operator"};
+    if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = ctx().stream;
+    Operator op(&h->g, *p, P64, 1);
+    const long n = op.nsites();
+    if (out < in + 48 * n && in < out + 48 * n) throw Error{CPSB_ERR_ARG, "out and in overlap"};
+    const double *in_e = in, *in_o = in + 24 * n;
+    double *out_e = out, *out_o = out + 24 * n;
+    Field fe(P64, n), fo(P64, n), ge(P64, n), go(P64, n);
+    upload(fe, &in_e, 1, n, st);
+    upload(fo, &in_o, 1, n, st);
+    mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
+    download(&out_e, 1, n, ge, st);
+    download(&out_o, 1, n, go, st);
+    return CPSB_OK;
   });
 }
 

@@ -154,6 +154,20 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
 int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
                 cpsb_solve_result *res);
 
+/* Lattice::FmatInv(f_out, f_in, cg_arg, true_res, CNV_FRM_NO, PRESERVE_YES, dminus)
+ * (lattice.h:1127-1132; Fmobius override f_mobius.C:45-117): for Mobius with
+ * dminus != 0 the source is first replaced by DiracOpMobius::Dminus of it (on the
+ * device; in is not modified), then the solve is cpsb_matinv's.  Wilson and DWF
+ * ignore dminus, as the reference's default FmatInv does. */
+int cpsb_fmatinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
+                 int dminus, cpsb_solve_result *res);
+
+/* DiracOpMobius::Dminus(out, in) (d_op_mobius.C:745-777, mobius_dminus.C:29-86) on
+ * full Mobius vectors (4-D-even half first): out = -(c(4 - M5) - a5_inv) in
+ * + (c/2) D_W in, D_W the 4-D hop of every s slice into the other checkerboard.
+ * Mobius only (CPSB_ERR_ARG otherwise); out and in must not overlap. */
+int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in);
+
 /* DiracOp::MinResExt(psi, phi, v, vm, degree) (include/util/dirac_op.h;
  * d_op_base/comsrc/minresext.C:32-156): the minimal-residual chronological
  * initial guess from degree <= 16 previous solutions.  v[i] (host vectors) are

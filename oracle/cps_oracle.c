@@ -861,6 +861,30 @@ int orc_matinv(const orc_op *op, double *out, const double *in, double stop_rsd,
   return it;
 }
 
+/* DiracOpMobius::Dminus, d_op_mobius.C:745-777, on a full Mobius vector
+ * (4-D-even half first) with mobius_dminus (mobius_dminus.C:29-86):
+ *   out_e = D_W(odd -> even)(-c/2 in_o),  out_o = D_W(even -> odd)(-c/2 in_e)
+ * on every s slice (fixed 4-D parity), then out = -((c (4 - M5) - a5_inv) in + out). */
+int orc_mobius_dminus(const orc_op *op, double *out, const double *in) {
+  if (op->action != 2) return -1;
+  const long n = orc_op_size(op);
+  const int ls = op->mob.ls;
+  const long n4 = n / ls;
+  const double c = op->mob.c[0][0];
+  const double k = 0.5 * (2 * (c * (4 - op->m5) - op->a5_inv));
+  double *t = scratch(n);
+  for (int half = 0; half < 2; half++) {
+    const double *src = in + (half ? 0 : n);   /* out_e from in_o, out_o from in_e */
+    double *dst = out + (half ? n : 0);
+    const int cb = half ? 0 : 1;               /* checkerboard of the input */
+    for (long i = 0; i < n; i++) t[i] = src[i] * (-0.5 * c);
+    for (int s = 0; s < ls; s++) orc_wilson_dslash(dst + s * n4, op->u, t + s * n4, cb, 0, op->dims);
+  }
+  for (long i = 0; i < 2 * n; i++) out[i] = -(k * in[i] + out[i]);
+  free(t);
+  return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* DiracOp::MinResExt, d_op_base/comsrc/minresext.C:32-156             */
 /* ------------------------------------------------------------------ */

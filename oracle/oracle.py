@@ -161,6 +161,21 @@ class Op:
         return out, it, tr.value
 
 
+    def dminus(self, x_full):
+        """DiracOpMobius::Dminus on a full vector (4-D-even half first)."""
+        x = np.ascontiguousarray(x_full, np.float64)
+        assert self.action == 2 and x.size == 2 * self.n
+        out = np.zeros(2 * self.n)
+        rc = lib().orc_mobius_dminus(C.byref(self.s), _p(out), _p(x))
+        assert rc == 0
+        return out
+
+    def fmatinv(self, src_full, guess_full=None, dminus=0, stop_rsd=1e-10, max_iter=5000):
+        """Lattice::FmatInv(..., dminus): Fmobius applies Dminus to the source
+        before MatInv (f_mobius.C:45-117); the other actions ignore the flag."""
+        src = self.dminus(src_full) if (dminus and self.action == 2) else src_full
+        return self.matinv(src, guess_full, stop_rsd, max_iter)
+
     def minresext(self, phi, prev):
         """DiracOp::MinResExt: returns (psi, orthonormalised prev, MatPcDagMatPc of them, guess residual)."""
         deg = len(prev)
@@ -183,6 +198,7 @@ def _setup():
     L.orc_matpc.restype = C.c_int
     L.orc_matinv.restype = C.c_int
     L.orc_minresext.restype = C.c_double
+    L.orc_mobius_dminus.restype = C.c_int
     L.orc_mdagm.restype = C.c_int
     L.orc_invcg.restype = C.c_int
     L.orc_invcg.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_double), _dp]

@@ -15,11 +15,13 @@
 //   DiracOp::InvCgShift                             d_op_base/comsrc/inv_cg.C:84-447
 //     (exactly what Lattice::FmatEvlInv reaches through InvCg(&true_res); the
 //      4-argument InvCg wrapper at inv_cg.C:449-454 has no return statement, so
-//      it is bypassed here -- see DESIGN.md)
+//      it is bypassed here)
 //   Lattice::FmatEvlMInv -> DiracOp::MInvCG         f_dwf_base.C:232-270, minvcg.C:47-353
 //   DiracOp*::MatInv (full-lattice solve)           d_op_wilson.C:257-334, d_op_dwf.C:316-507,
 //                                                   d_op_mobius.C:389-640
 //   DiracOp::MinResExt (chronological guess)        d_op_base/comsrc/minresext.C:32-156
+//   DiracOpMobius::Dminus                           d_op_mobius/d_op_mobius.C:745-777
+//   Fmobius::FmatInv(..., dminus)                   lattice/f_mobius/f_mobius.C:45-117
 //   Lattice::Fconvert (fermion storage order)       lattice/convert/convert.C:444-570 (Wilson),
 //                                                   :635-1010 (DWF / Mobius)
 //   zmobius_m5inv / zmobius_dslash_4                d_op_zmobius/noarch/zmobius_m5inv.C:807-845,
@@ -36,7 +38,8 @@
 //        14 repetitions (OP_BENCH: MatPcDagMatPc applied this many times),
 //        15 fermion order for OP_FCONVERT (0 WILSON, 1 DWF_4D_EOPREC_EE),
 //        16 OP_FCONVERT direction (0 CANONICAL -> order, 1 order -> CANONICAL),
-//        17 OP_MINRESEXT degree (number of previous solutions)
+//        17 OP_MINRESEXT degree (number of previous solutions),
+//        18 OP_FMATINV dminus flag
 //   rpar[10] = wall seconds spent inside the timed CPS call(s) (MINVCG: rpar[42],
 //   since rpar[0..nshift) holds the per-shift residuals)
 //   par: 0 mass, 1 M5 (dwf_height), 2 a5_inv, 3 mobius b, 4 mobius c, 5 stop_rsd,
@@ -62,7 +65,7 @@ USING_NAMESPACE_CPS
 
 enum { OP_DSLASH = 1, OP_MATPC = 2, OP_MDAGM = 3, OP_INVCG = 4, OP_MINVCG = 5,
        OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9, OP_FCONVERT = 10,
-       OP_MINRESEXT = 11 };
+       OP_MINRESEXT = 11, OP_DMINUS = 12, OP_FMATINV = 13 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -252,6 +255,36 @@ int main(int argc, char **argv) {
     d->MatInv(fout, fin, &true_res, PRESERVE_YES);
     rpar[10] = now_s() - t0;
     delete d;
+    rpar[0] = true_res;
+    out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
+    sfree(fin);
+    sfree(fout);
+  } else if (op == OP_DMINUS) {
+    // Mobius only: one full vector (4-D-even half first) in, Dminus of it out.
+    if (action != 2) die("Dminus is a Mobius operator");
+    Vector *fin = (Vector *)smalloc(2 * fsz * sizeof(double));
+    Vector *fout = (Vector *)smalloc(2 * fsz * sizeof(double));
+    read_all(fi, fin, 2 * fsz * sizeof(double));
+    memset(fout, 0, 2 * fsz * sizeof(double));
+    {
+      DiracOpMobius d(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+      d.Dminus(fout, fin);
+    }
+    out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
+    sfree(fin);
+    sfree(fout);
+  } else if (op == OP_FMATINV) {
+    // Lattice::FmatInv with the source preserved and the dminus flag of hdr[18]
+    // (only Fmobius overrides the dminus form; the others ignore the flag,
+    // lattice.h:1127-1132).  Full source and initial guess in.
+    Vector *fin = (Vector *)smalloc(2 * fsz * sizeof(double));
+    Vector *fout = (Vector *)smalloc(2 * fsz * sizeof(double));
+    read_all(fi, fin, 2 * fsz * sizeof(double));
+    read_all(fi, fout, 2 * fsz * sizeof(double));
+    Float true_res = 0;
+    double t0 = now_s();
+    rhdr[0] = lat.FmatInv(fout, fin, &cg_arg, &true_res, CNV_FRM_NO, PRESERVE_YES, (int)hdr[18]);
+    rpar[10] = now_s() - t0;
     rpar[0] = true_res;
     out_payload.assign((double *)fout, (double *)fout + 2 * fsz);
     sfree(fin);

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CPSREF = os.path.join(HERE, "_ref", "cpsref")
 
 OP_DSLASH, OP_MATPC, OP_MDAGM, OP_INVCG, OP_MINVCG, OP_M5INV, OP_MOBIUS_D4, OP_BENCH, OP_MATINV, OP_FCONVERT, \
-    OP_MINRESEXT = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+    OP_MINRESEXT, OP_DMINUS, OP_FMATINV = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13
 ACTIONS = {"wilson": 0, "dwf": 1, "mobius": 2}
 
 
@@ -26,7 +26,7 @@ def available() -> bool:
 
 def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8, a5_inv=1.0,
         b=1.5, c=0.5, stop_rsd=1e-10, max_iter=5000, shifts=(), ms_type=0, pc_type=2,
-        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0):
+        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0, dminus=0):
     """Run one reference operation; returns (iters, rpar[64], payload array)."""
     if not available():
         raise RuntimeError("reference oracle not built (run oracle/build_ref.sh)")
@@ -47,6 +47,7 @@ def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8
     hdr[15] = order
     hdr[16] = direction
     hdr[17] = degree
+    hdr[18] = dminus
     par[0] = mass
     par[1] = m5
     par[2] = a5_inv

@@ -198,6 +198,31 @@ def main():
     main_minresext()
 
 
+DMINUS_CASES = [("mobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 31, 0.05, 1.5, 0.5),
+                ("mobius_b2c1_4x4x4x4_ls6", (4, 4, 4, 4), 6, 0.2, 33, 0.02, 2.0, 1.0)]
+
+
+def gen_dminus(name, dims, ls, eps, seed, mass, b, c):
+    """DiracOpMobius::Dminus of the MatInv source, and Lattice::FmatInv with
+    dminus = 1 (Dminus applied to the source, then MatInv) from the MatInv guess."""
+    u = fields.random_gauge(dims, eps, seed)
+    base = {"dims": np.array(dims), "ls": ls, "seed": seed}
+    src, guess = matinv_inputs(base)
+    kw = dict(ls=ls, mass=mass, m5=1.8, b=b, c=c, threads=1)
+    _, _, dm = refrun.run(refrun.OP_DMINUS, "mobius", dims, u, [src], **kw)
+    it, rp, sol = refrun.run(refrun.OP_FMATINV, "mobius", dims, u, [src, guess], stop_rsd=1e-10, max_iter=5000,
+                             dminus=1, **kw)
+    return {"gauge_sha": sha(u), "matinv_src_sha": sha(src), "matinv_guess_sha": sha(guess),
+            "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed, "mass": mass, "m5": 1.8, "b": b, "c": c,
+            "dminus_out": dm, "fmatinv_sol": sol, "fmatinv_true_res": rp[0], "fmatinv_iters": it}
+
+
+def main_dminus():
+    for case in DMINUS_CASES:
+        np.savez_compressed(os.path.join(OUT, "dminus_" + case[0] + ".npz"), **gen_dminus(*case))
+        print("wrote dminus_" + case[0])
+
+
 def main_matinv():
     for case in CASES:
         if "bc_t" in case[7]:
@@ -219,5 +244,7 @@ if __name__ == "__main__":
         main_fconvert()
     elif "--minresext" in sys.argv:
         main_minresext()
+    elif "--dminus" in sys.argv:
+        main_dminus()
     else:
         main()

@@ -39,3 +39,15 @@ def load_matinv(name):
     assert sha(u) == str(rec["gauge_sha"]), "gauge generator drifted from the fixture"
     assert sha(src) == str(rec["matinv_src_sha"]) and sha(guess) == str(rec["matinv_guess_sha"])
     return rec, u, src, guess
+
+
+def load_dminus(name):
+    """Dminus / FmatInv(dminus = 1) fixture: (record, gauge, full source, full initial guess)."""
+    from tests.golden.make_golden import matinv_inputs
+    rec = dict(np.load(os.path.join(GOLDEN, "dminus_" + name + ".npz")))
+    dims = tuple(int(d) for d in rec["dims"])
+    u = fields.random_gauge(dims, float(rec["eps"]), int(rec["seed"]))
+    src, guess = matinv_inputs(rec)
+    assert sha(u) == str(rec["gauge_sha"]), "gauge generator drifted from the fixture"
+    assert sha(src) == str(rec["matinv_src_sha"]) and sha(guess) == str(rec["matinv_guess_sha"])
+    return rec, u, src, guess

@@ -203,3 +203,35 @@ def test_matinv_vs_reference(name, action, prec):
     out, r = op.MatInv(src, guess, stop_rsd=1e-10, precision=getattr(cb, prec))
     assert r.status == 0 and r.true_rsd <= 1e-10
     assert rel(out, rec["matinv_sol"]) < (1e-9 if prec == "F64" else 1e-8)
+
+
+@pytest.mark.parametrize("name", ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls6"])
+@pytest.mark.parametrize("prec", ["F64", "F32"])
+def test_dminus_fmatinv_vs_reference(name, prec):
+    """DiracOpMobius::Dminus on the device against the compiled CPS (FP64, within
+    1e-13 relative), and Lattice::FmatInv with dminus = 1 against CPS's
+    Fmobius::FmatInv from a nonzero guess: FP64 within 1e-9 relative, mixed FP32
+    within 1e-8, the preconditioned CG reaching FP64 true residual 1e-10."""
+    import cps_public_b200 as cb
+    from tests.golden_util import load_dminus
+    rec, u, src, guess = load_dminus(name)
+    op = device_op(rec, u, "mobius")
+    assert rel(op.Dminus(src), rec["dminus_out"]) < 1e-13
+    out, r = op.FmatInv(src, guess, dminus=1, stop_rsd=1e-10, precision=getattr(cb, prec))
+    assert r.status == 0 and r.true_rsd <= 1e-10
+    assert rel(out, rec["fmatinv_sol"]) < (1e-9 if prec == "F64" else 1e-8)
+    if prec == "F64":
+        assert abs(r.iters - int(rec["fmatinv_iters"])) <= 1
+
+
+def test_fmatinv_dminus_ignored_outside_mobius():
+    """Lattice::FmatInv's dminus form falls back to the plain solve for Wilson
+    and DWF (lattice.h:1127-1132): the same solution bit for bit."""
+    from tests.golden_util import load_matinv
+    rec, u, src, guess = load_matinv("dwf_4x4x4x4_ls4")
+    op = device_op(rec, u, "dwf")
+    a, _ = op.MatInv(src, guess, stop_rsd=1e-10)
+    b, _ = op.FmatInv(src, guess, dminus=1, stop_rsd=1e-10)
+    np.testing.assert_array_equal(a, b)
+    with pytest.raises(Exception):
+        op.Dminus(src)

@@ -93,6 +93,22 @@ def test_matinv_bitexact(name):
     assert tr == float(rec["matinv_true_res"])
 
 
+DMINUS_CASES = ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls6"]
+
+
+@pytest.mark.parametrize("name", DMINUS_CASES)
+def test_dminus_fmatinv_bitexact(name):
+    """DiracOpMobius::Dminus, and Lattice::FmatInv with dminus = 1 (Dminus of
+    the source, then MatInv) from a nonzero initial guess."""
+    from tests.golden_util import load_dminus
+    rec, u, src, guess = load_dminus(name)
+    op = make_op(rec, u, "mobius")
+    np.testing.assert_array_equal(op.dminus(src), rec["dminus_out"])
+    out, it, tr = op.fmatinv(src, guess, dminus=1, stop_rsd=1e-10, max_iter=5000)
+    np.testing.assert_array_equal(out, rec["fmatinv_sol"])
+    assert tr == float(rec["fmatinv_true_res"]) and it == int(rec["fmatinv_iters"])
+
+
 @pytest.mark.parametrize("action,order", [("wilson", "wilson"), ("dwf", "wilson"), ("mobius", "4d_ee")])
 def test_fermion_convert_matches_reference(action, order):
     """Lattice::Fconvert (CANONICAL <-> WILSON / 5-D checkerboard /
