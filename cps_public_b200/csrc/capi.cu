@@ -550,14 +550,20 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
       op.dslash(t, fin_e, 0, 0, st);
       lin(t, op.kappa, t, 1.0, &fin_c);        // t = kappa D in_e + in_o
     } else {
-      // d_op_mobius.C:389-640, ZMOB_PC_SYM2
+      // d_op_mobius.C:389-640 (ZMOB_PC_ORIG, SYM1, SYM2)
       kb = op.kappa_b;
       op.mobius_m5inv(t.ptr(), fin_e.ptr(), st);
       op.mobius_d4(t2.ptr(), t.ptr(), 0, st);
       lin(t, kb, t2, 1.0, &fin_c);             // t = kappa_b D4 M5^-1 in_e + in_o
-      CK(cudaMemcpyAsync(t2.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
-      const double kappa_c = 1.0 / (2 * (p->mobius_c * (4 - p->m5) - p->a5_inv));
-      op.mobius_hop5_add(fout_c.ptr(), t2.ptr(), t2.ptr(), kb / kappa_c, st);  // SYM2 guess
+      if (p->pc_type == 2) {                   // SYM2: guess = M5 guess
+        CK(cudaMemcpyAsync(t2.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
+        const double kappa_c = 1.0 / (2 * (p->mobius_c * (4 - p->m5) - p->a5_inv));
+        op.mobius_hop5_add(fout_c.ptr(), t2.ptr(), t2.ptr(), kb / kappa_c, st);
+      }
+      if (p->pc_type == 1) {                   // SYM1: source = M5^-1 source
+        op.mobius_m5inv(t2.ptr(), t.ptr(), st);
+        CK(cudaMemcpyAsync(t.data.p, t2.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      }
     }
     CgSolver *s = get_solver(&h->g, *p, a->precision, 1);
     std::lock_guard<std::mutex> lk(s->busy);
@@ -569,8 +575,10 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
       op.dslash(t, fout_c, 1, 0, st);
       lin(fout_e, op.kappa, t, 1.0, &fin_e);   // out_e = kappa D out_o + in_e
     } else {
-      op.mobius_m5inv(t.ptr(), fout_c.ptr(), st);
-      CK(cudaMemcpyAsync(fout_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      if (p->pc_type == 2) {                   // SYM2: the solution is M5 out_o
+        op.mobius_m5inv(t.ptr(), fout_c.ptr(), st);
+        CK(cudaMemcpyAsync(fout_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      }
       op.mobius_d4(t.ptr(), fout_c.ptr(), 1, st);
       lin(t2, kb, t, 0.0, nullptr);            // kappa_b D4 out_o
       op.mobius_m5inv(fout_e.ptr(), t2.ptr(), st);

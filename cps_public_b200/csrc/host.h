@@ -131,6 +131,8 @@ struct Operator {
   // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
   // (zmobius_m5inv, dag 0); out = D4(cb) in (zmobius_dslash_4, dag 0);
   // out = x + f H5 in (zmobius_kappa_dslash_5_plus_cmplx with factor f, dag 0).
+  void matpc_orig_sym1(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
+                       cudaStream_t st);
   void mobius_m5inv(const SpinorPtr &out, const SpinorPtr &in, cudaStream_t st);
   void mobius_d4(const SpinorPtr &out, const SpinorPtr &in, int cb, cudaStream_t st);
   void mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const SpinorPtr &x, double f, cudaStream_t st);

@@ -167,7 +167,8 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
   if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
   if (p.action == CPSB_MOBIUS) {
-    if (p.pc_type != 2) throw Error{CPSB_ERR_UNSUPPORTED, "only the ZMOB_PC_SYM2 Mobius preconditioner is implemented"};
+    if (p.pc_type < 0 || p.pc_type > 2)
+      throw Error{CPSB_ERR_UNSUPPORTED, "Mobius preconditioners: ZMOB_PC_ORIG (0), ZMOB_PC_SYM1 (1), ZMOB_PC_SYM2 (2)"};
     if (prec == P16) throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
     const int ok[] = {4, 8, 12, 16, 20, 24, 32};
     bool found = false;
@@ -258,6 +259,10 @@ void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const R
   }
   Reduce none;
   memset(&none, 0, sizeof(none));
+  if (p.pc_type != 2) {
+    matpc_orig_sym1(out, in, dag, red, skip, st);
+    return;
+  }
   if (!dag) {
     CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
     hop(t3.ptr(), t1.ptr(), 1, 0, kappa_b, nullptr, nullptr, skip, st);
@@ -271,6 +276,72 @@ void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const R
     hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
     CK(launch_m5(prec, 1, geom, out, t1.ptr(), in, m5c[1], 1, red != nullptr, red ? *red : none, skip,
                  st));
+  }
+}
+
+// ZMOB_PC_ORIG (zmobius_m-orig.h:3-126, zmobius_mdag-orig.h) and ZMOB_PC_SYM1
+// (zmobius_m-sym1.h, zmobius_mdag-sym1.h) from the same kernels as SYM2: the m5
+// kernel with K = 0 is the D4 prefix b in + c H5 in (or, with b = 0, the
+// 5th-direction hop alone), with b = 1, c = 0 it is M5^-1 alone.
+//   ORIG  M    = in - kb D4(0) M5^-1 kb D4(1) in + (kb/kc) H5 in
+//         M^dag = in + D4^dag(0) kb M5^-dag D4^dag(1) (-kb in) + (kb/kc) H5^dag in
+//   SYM1  M    = in - M5^-1 kb D4(0) M5^-1 kb D4(1) in
+//         M^dag = in + D4^dag(0) kb M5^-dag D4^dag(1) (-kb M5^-dag in)
+// D4(cb) = hop(cb) (b + c H5) and D4^dag(cb) = (b + c H5)^dag hop^dag(cb)
+// (zmobius_dslash_4.C:90-121, :176-202).
+void Operator::matpc_orig_sym1(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red,
+                               const int *skip, cudaStream_t st) {
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  const bool orig = p.pc_type == 0;
+  const double kc = 1.0 / (2 * (p.mobius_c * (4 - p.m5) - p.a5_inv));
+  M5Coef mix;  // K = 0: identity sweeps, then the b/c mixing
+  memset(&mix, 0, sizeof(mix));
+  mix.invd = 1.0;
+  mix.b = p.mobius_b;
+  mix.c = p.mobius_c;
+  mix.mass = p.mass;
+  mix.scale = 1.0;
+  M5Coef h5 = mix;  // (kb/kc) H5
+  h5.b = 0.0;
+  h5.c = kappa_b / kc;
+  const Reduce rd = red ? *red : none;
+  if (!dag) {
+    CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, mix, 0, 0, none, skip, st));
+    hop(t3.ptr(), t1.ptr(), 1, 0, kappa_b, nullptr, nullptr, skip, st);
+    CK(launch_m5(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
+    if (orig) {
+      hop(out, t1.ptr(), 0, 0, -kappa_b, &in, nullptr, skip, st);
+      CK(launch_m5(prec, 0, geom, out, in, out, h5, 1, red != nullptr, rd, skip, st));
+    } else {
+      hop(t3.ptr(), t1.ptr(), 0, 0, -kappa_b, nullptr, nullptr, skip, st);
+      M5Coef inv = m5c[0];
+      inv.b = 1.0;
+      inv.c = 0.0;
+      inv.scale = 1.0;
+      CK(launch_m5(prec, 0, geom, out, t3.ptr(), in, inv, 1, red != nullptr, rd, skip, st));
+    }
+    return;
+  }
+  if (orig) {
+    hop(t1.ptr(), in, 1, 1, -kappa_b, nullptr, nullptr, skip, st);
+  } else {
+    M5Coef inv = m5c[1];
+    inv.b = 1.0;
+    inv.c = 0.0;
+    inv.scale = -kappa_b;
+    CK(launch_m5(prec, 1, geom, t3.ptr(), in, SpinorPtr{}, inv, 0, 0, none, skip, st));
+    hop(t1.ptr(), t3.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
+  }
+  M5Coef c = m5c[1];
+  c.scale = kappa_b;
+  CK(launch_m5(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, c, 0, 0, none, skip, st));
+  hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+  if (orig) {
+    CK(launch_m5(prec, 1, geom, out, t1.ptr(), in, mix, 1, 0, none, skip, st));
+    CK(launch_m5(prec, 1, geom, out, in, out, h5, 1, red != nullptr, rd, skip, st));
+  } else {
+    CK(launch_m5(prec, 1, geom, out, t1.ptr(), in, mix, 1, red != nullptr, rd, skip, st));
   }
 }
 

@@ -47,8 +47,10 @@ typedef struct cpsb_gauge_s *cpsb_gauge;
  *   m5      GJP.DwfHeight() (include/util/gjp.h:579)
  *   a5_inv  GJP.DwfA5Inv() (gjp.h:587)
  *   mobius_b, mobius_c   GJP.Mobius_b/c() (gjp.h:594-601)
- *   pc_type GJP.ZMobius_PC_Type(): only ZMOB_PC_SYM2 (= 2), the CPS default
- *           (src/util/gjp/gjp.C:129), is implemented on the device. */
+ *   pc_type GJP.ZMobius_PC_Type() (include/util/dwf.h:42-48): ZMOB_PC_ORIG (0),
+ *           ZMOB_PC_SYM1 (1) and ZMOB_PC_SYM2 (2, the CPS default, src/util/gjp/
+ *           gjp.C:129) are implemented; the MIT and SYM3 forms (which read the
+ *           zMobius coefficient arrays) return CPSB_ERR_UNSUPPORTED. */
 typedef struct {
   int action;
   int ls;

@@ -306,7 +306,7 @@ typedef struct {
   int ls;
   double mass, m5, a5_inv;
   double b[64][2], c[64][2];  /* per-s b_s, c_s as (re, im) */
-  int pc_type;                 /* 0 = ZMOB_PC_ORIG, 2 = ZMOB_PC_SYM2 */
+  int pc_type;                 /* 0 ZMOB_PC_ORIG, 1 ZMOB_PC_SYM1, 2 ZMOB_PC_SYM2 */
 } orc_mobius_params;
 
 /* kappa_b(s) = 1/(2(b_s(4-M5)+a5_inv)), kappa_c(s) = 1/(2(c_s(4-M5)-a5_inv)),
@@ -515,17 +515,92 @@ static void mobius_mdag_sym2(double *out, const double *u, const double *in, con
   free(t2);
 }
 
-/* zmobius_m-orig.h:3-126 and zmobius_mdag-orig.h: the original preconditioner
- * out = in + (kb/kc) 1/2 D5 in - kb D4(0) M5^-1 kb D4(1) in is not restated
- * here; only SYM2 (the CPS default, gjp.C:129) is. */
+/* zmobius_m-orig.h:3-126: out = in - kb D4(0) M5^-1 kb D4(1) in + kr H5 in
+ * (M5 - kb^2 D4 M5^-1 D4 with M5 = 1 + kr H5). */
+static void mobius_m_orig(double *out, const double *u, const double *in, const int *dims,
+                          const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  orc_mobius_dslash_4(out, u, in, 1, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, kb[s], n);
+  orc_mobius_m5inv(out, 0, dims, p);
+  orc_mobius_dslash_4(t2, u, out, 0, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cneg(kb[s]), n);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (long i = 0; i < n * ls; i++) out[i] += t2[i];
+  orc_zmobius_dslash_5_plus(out, in, p->mass, 0, dims, ls, kr);
+  free(t2);
+}
+
+/* zmobius_mdag-orig.h */
+static void mobius_mdag_orig(double *out, const double *u, const double *in, const int *dims,
+                             const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, cneg(cconj(kb[s])), n);
+  orc_mobius_dslash_4(t2, u, out, 1, 1, dims, p);
+  orc_mobius_m5inv(t2, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cconj(kb[s]), n);
+  orc_mobius_dslash_4(out, u, t2, 0, 1, dims, p);
+  for (long i = 0; i < n * ls; i++) out[i] += in[i];
+  orc_zmobius_dslash_5_plus(out, in, p->mass, 1, dims, ls, kr);
+  free(t2);
+}
+
+/* zmobius_m-sym1.h: out = in - M5^-1 kb D4(0) M5^-1 kb D4(1) in. */
+static void mobius_m_sym1(double *out, const double *u, const double *in, const int *dims,
+                          const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  orc_mobius_dslash_4(out, u, in, 1, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, kb[s], n);
+  orc_mobius_m5inv(out, 0, dims, p);
+  orc_mobius_dslash_4(t2, u, out, 0, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cneg(kb[s]), n);
+  orc_mobius_m5inv(t2, 0, dims, p);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (long i = 0; i < n * ls; i++) out[i] += t2[i];
+  free(t2);
+}
+
+/* zmobius_mdag-sym1.h */
+static void mobius_mdag_sym1(double *out, const double *u, const double *in, const int *dims,
+                             const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(out, in, sizeof(double) * n * ls);
+  orc_mobius_m5inv(out, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, cneg(cconj(kb[s])), n);
+  orc_mobius_dslash_4(t2, u, out, 1, 1, dims, p);
+  orc_mobius_m5inv(t2, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cconj(kb[s]), n);
+  orc_mobius_dslash_4(out, u, t2, 0, 1, dims, p);
+  for (long i = 0; i < n * ls; i++) out[i] += in[i];
+  free(t2);
+}
 
 /* mobius_m.C:28-42 -> zmobius_m.C:40-74 (pc dispatch); mobius_mdag.C:35-55. */
 int orc_mobius_m(double *out, const double *u, const double *in, int dag, const int *dims,
                  const orc_mobius_params *p) {
-  if (p->pc_type != 2) return -1;
-  if (dag) mobius_mdag_sym2(out, u, in, dims, p);
-  else mobius_m_sym2(out, u, in, dims, p);
-  return 0;
+  switch (p->pc_type) {  /* ZMOB_PC_ORIG, ZMOB_PC_SYM1, ZMOB_PC_SYM2 (util/dwf.h:42-48) */
+    case 0: if (dag) mobius_mdag_orig(out, u, in, dims, p); else mobius_m_orig(out, u, in, dims, p); return 0;
+    case 1: if (dag) mobius_mdag_sym1(out, u, in, dims, p); else mobius_m_sym1(out, u, in, dims, p); return 0;
+    case 2: if (dag) mobius_mdag_sym2(out, u, in, dims, p); else mobius_m_sym2(out, u, in, dims, p); return 0;
+    default: return -1;
+  }
 }
 
 /* mobius_mdagm.C:33-60 */
@@ -838,13 +913,20 @@ int orc_matinv(const orc_op *op, double *out, const double *in, double stop_rsd,
         t[s * n4 + 2 * i + 1] = r.im + in_o[s * n4 + 2 * i + 1];
       }
     }
-    memcpy(t2, out_o, n * sizeof(double));                       /* SYM2: guess transform */
-    orc_zmobius_dslash_5_plus(out_o, t2, p.mass, 0, op->dims, ls, kr);
+    if (p.pc_type == 2) {                                         /* SYM2: guess transform */
+      memcpy(t2, out_o, n * sizeof(double));
+      orc_zmobius_dslash_5_plus(out_o, t2, p.mass, 0, op->dims, ls, kr);
+    }
+    if (p.pc_type == 1) {                                         /* SYM1: source M5^-1 */
+      orc_mobius_m5inv(t, 0, op->dims, &p);
+    }
     orc_matpc(op, src, t, 1);
     it = orc_invcg(op, out_o, src, stop_rsd, max_num_iter, true_res, NULL);
-    memcpy(t, out_o, n * sizeof(double));
-    orc_mobius_m5inv(t, 0, op->dims, &p);
-    memcpy(out_o, t, n * sizeof(double));
+    if (p.pc_type == 2) {
+      memcpy(t, out_o, n * sizeof(double));
+      orc_mobius_m5inv(t, 0, op->dims, &p);
+      memcpy(out_o, t, n * sizeof(double));
+    }
     orc_mobius_dslash_4(t, op->u, out_o, 1, 0, op->dims, &p);
     for (int s = 0; s < ls; s++) zscale(t + s * n4, kb[s], n4);   /* zmobius_zvectTimesEquComplex */
     memcpy(out_e, t, n * sizeof(double));

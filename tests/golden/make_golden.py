@@ -196,6 +196,24 @@ def main():
     main_matinv()
     main_fconvert()
     main_minresext()
+    main_pc()
+    main_dminus()
+
+
+# Mobius with the non-default preconditioners ZMOB_PC_ORIG (0) and ZMOB_PC_SYM1 (1)
+PC_CASES = [
+    ("mobius_orig_4x4x4x4_ls4", "mobius", (4, 4, 4, 4), 4, 0.2, 35, 0.05, {"m5": 1.8, "b": 1.5, "c": 0.5, "pc_type": 0}),
+    ("mobius_sym1_4x4x4x4_ls6", "mobius", (4, 4, 4, 4), 6, 0.2, 36, 0.03, {"m5": 1.8, "b": 2.0, "c": 1.0, "pc_type": 1}),
+]
+
+
+def main_pc():
+    for case in PC_CASES:
+        # the hop, M5^-1 and D4 do not depend on the preconditioner: not stored again
+        rec = {k: v for k, v in gen_case(*case).items() if not k.startswith(("dslash_", "m5inv_", "d4_"))}
+        np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **rec)
+        np.savez_compressed(os.path.join(OUT, "matinv_" + case[0] + ".npz"), **gen_matinv(*case))
+        print("wrote", case[0], "and matinv_" + case[0])
 
 
 DMINUS_CASES = [("mobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 31, 0.05, 1.5, 0.5),
@@ -246,5 +264,7 @@ if __name__ == "__main__":
         main_minresext()
     elif "--dminus" in sys.argv:
         main_dminus()
+    elif "--pc" in sys.argv:
+        main_pc()
     else:
         main()

@@ -18,6 +18,8 @@ pytestmark = pytest.mark.gpu
 
 OP_TOL = 1e-13
 CASES = [("wilson_4x4x4x4", "wilson"), ("dwf_4x4x4x4_ls4", "dwf"), ("mobius_4x4x4x4_ls4", "mobius")]
+# Mobius with the ZMOB_PC_ORIG and ZMOB_PC_SYM1 preconditioners
+PC_CASES = [("mobius_orig_4x4x4x4_ls4", "mobius"), ("mobius_sym1_4x4x4x4_ls6", "mobius")]
 
 
 def device_op(rec, u, action):
@@ -28,6 +30,8 @@ def device_op(rec, u, action):
     for k in ("m5", "b", "c"):
         if k in rec:
             kw[k] = float(rec[k])
+    if "pc_type" in rec:
+        kw["pc_type"] = int(rec["pc_type"])
     return cb.DiracOp(g, action, **kw)
 
 
@@ -40,7 +44,7 @@ def test_dslash_vs_reference(name, action):
         assert rel(op.Dslash(src, cb_, dag), rec[k]) < OP_TOL, k
 
 
-@pytest.mark.parametrize("name,action", CASES)
+@pytest.mark.parametrize("name,action", CASES + PC_CASES)
 def test_matpc_mdagm_vs_reference(name, action):
     rec, u, src = load(name)
     op = device_op(rec, u, action)
@@ -51,7 +55,7 @@ def test_matpc_mdagm_vs_reference(name, action):
     assert abs(dot - float(rec["mdagm_dot"])) < OP_TOL * abs(float(rec["mdagm_dot"]))
 
 
-@pytest.mark.parametrize("name,action", CASES)
+@pytest.mark.parametrize("name,action", CASES + PC_CASES)
 def test_fp64_cg_vs_reference(name, action):
     import cps_public_b200 as cb
     rec, u, src = load(name)
@@ -63,7 +67,7 @@ def test_fp64_cg_vs_reference(name, action):
 
 
 @pytest.mark.parametrize("prec", ["F32", "F16"])
-@pytest.mark.parametrize("name,action", CASES)
+@pytest.mark.parametrize("name,action", CASES + PC_CASES)
 def test_mixed_cg_reaches_fp64_true_residual(name, action, prec):
     import cps_public_b200 as cb
     if action == "mobius" and prec == "F16":
@@ -190,7 +194,7 @@ def test_max_rhs_batch(prec):
 
 
 @pytest.mark.parametrize("prec", ["F64", "F32"])
-@pytest.mark.parametrize("name,action", CASES)
+@pytest.mark.parametrize("name,action", CASES + PC_CASES)
 def test_matinv_vs_reference(name, action, prec):
     """DiracOp*::MatInv on the device (source preparation, MatPcDag, CG,
     reconstruction of the other checkerboard) against the compiled CPS MatInv

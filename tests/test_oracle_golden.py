@@ -8,13 +8,16 @@ from oracle import oracle
 from tests.golden_util import load
 
 CASES = ["wilson_4x4x4x4", "dwf_4x4x4x4_ls4", "mobius_4x4x4x4_ls4"]
+# Mobius with ZMOB_PC_ORIG and ZMOB_PC_SYM1 (no hop fixtures: the hop does not
+# depend on the preconditioner)
+PC_CASES = ["mobius_orig_4x4x4x4_ls4", "mobius_sym1_4x4x4x4_ls6"]
 
 
 def make_op(rec, u, action):
     kw = dict(ls=int(rec["ls"]), mass=float(rec["mass"]))
-    for k in ("m5", "b", "c", "bc_t"):
+    for k in ("m5", "b", "c", "bc_t", "pc_type"):
         if k in rec:
-            kw[k] = float(rec[k]) if k != "bc_t" else int(rec[k])
+            kw[k] = float(rec[k]) if k in ("m5", "b", "c") else int(rec[k])
     return oracle.Op(action, tuple(rec["dims"]), u, **kw)
 
 
@@ -29,7 +32,7 @@ def test_dslash_bitexact(name):
         np.testing.assert_array_equal(op.dslash(src, cb, dag), rec[k], err_msg=k)
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_matpc_mdagm_bitexact(name):
     rec, u, src = load(name)
     op = make_op(rec, u, name.split("_")[0])
@@ -40,7 +43,7 @@ def test_matpc_mdagm_bitexact(name):
     assert dot == float(rec["mdagm_dot"])
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_invcg_bitexact(name):
     rec, u, src = load(name)
     op = make_op(rec, u, name.split("_")[0])
@@ -50,7 +53,7 @@ def test_invcg_bitexact(name):
     np.testing.assert_array_equal(sol, rec["cg_sol"])
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_minvcg_bitexact(name):
     rec, u, src = load(name)
     op = make_op(rec, u, name.split("_")[0])
@@ -81,7 +84,7 @@ def test_wilson_8x8x8x8_cg_config():
     np.testing.assert_array_equal(sol, rec["cg_sol"])
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_matinv_bitexact(name):
     """DiracOp*::MatInv (full-lattice solve with source preparation and
     even/odd reconstruction) from a nonzero initial guess."""
