@@ -32,7 +32,7 @@
 //              order: site x+lx*(y+ly*(z+lz*t)), link mu, row-major 3x3 complex),
 //              then op-specific doubles (see below).
 //   response = int64 rhdr[8], double rpar[64], then op-specific doubles.
-//   hdr: 0 op, 1 action (0 Wilson, 1 DWF, 2 Mobius), 2..5 lx ly lz lt, 6 ls,
+//   hdr: 0 op, 1 action (0 Wilson, 1 DWF, 2 Mobius, 3 zMobius), 2..5 lx ly lz lt, 6 ls,
 //        7 cb, 8 dag, 9 max_iter, 10 nshift, 11 multishift type (0 MULTI,
 //        1 SINGLE), 12 zmobius pc type, 13 t boundary (0 periodic, 1 antiperiodic),
 //        14 repetitions (OP_BENCH: MatPcDagMatPc applied this many times),
@@ -44,6 +44,9 @@
 //   since rpar[0..nshift) holds the per-shift residuals)
 //   par: 0 mass, 1 M5 (dwf_height), 2 a5_inv, 3 mobius b, 4 mobius c, 5 stop_rsd,
 //        8.. shifts[nshift], 24.. unused
+//   zMobius (action 3) only: 4*ls doubles right after par, before the gauge:
+//        b_s as (re, im) pairs for s = 0..ls-1, then c_s likewise
+//        (DoArgExt zmobius_b_coeff / zmobius_c_coeff, src/util/gjp/gjp.C:167-178)
 #include <config.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -91,6 +94,18 @@ static double apply_op(D &d, int op, Vector *out, Vector *in, int cb, int dag) {
   return dot;
 }
 
+// DiracOpZMobius's constructor (d_op_zmobius.C:315-368) resets the kappa arrays
+// but never fills Dwf::zmobius_b / zmobius_c, which zmobius_dslash_4 reads
+// (zmobius_dslash_4.C:61-62, :151-152); only DiracOpMobius fills them
+// (d_op_mobius.C:111-118).  The harness copies GJP's zMobius coefficients there
+// (what the disabled branch at zmobius_dslash_4.C:64-65 reads), so the
+// reference's zMobius kernels run on the coefficients the job set.
+static void fill_zmobius_coefficients(Lattice &lat, int ls) {
+  Dwf *arg = (Dwf *)lat.FdiracOpInitPtr();
+  arg->zmobius_b.assign(GJP.ZMobius_b(), GJP.ZMobius_b() + ls);
+  arg->zmobius_c.assign(GJP.ZMobius_c(), GJP.ZMobius_c() + ls);
+}
+
 int main(int argc, char **argv) {
   if (argc != 3) { fprintf(stderr, "usage: cpsref request.bin response.bin\n"); return 2; }
   FILE *fi = fopen(argv[1], "rb");
@@ -126,21 +141,32 @@ int main(int argc, char **argv) {
   ext.mobius_b_coeff = par[3];
   ext.mobius_c_coeff = par[4];
   // DoArgExt's constructor leaves the zMobius coefficient arrays uninitialised
-  // (src/alg/alg_arg/do_arg_init.C:75-93); empty them so InitializeExt skips them.
+  // (src/alg/alg_arg/do_arg_init.C:75-93); empty them so InitializeExt skips them,
+  // except for zMobius, which reads its b_s, c_s from them.
   ext.zmobius_b_coeff.zmobius_b_coeff_len = 0;
   ext.zmobius_b_coeff.zmobius_b_coeff_val = 0;
   ext.zmobius_c_coeff.zmobius_c_coeff_len = 0;
   ext.zmobius_c_coeff.zmobius_c_coeff_val = 0;
+  std::vector<double> zb(2 * ls), zc(2 * ls);
+  if (action == 3) {
+    read_all(fi, zb.data(), zb.size() * sizeof(double));
+    read_all(fi, zc.data(), zc.size() * sizeof(double));
+    ext.zmobius_b_coeff.zmobius_b_coeff_len = 2 * ls;
+    ext.zmobius_b_coeff.zmobius_b_coeff_val = zb.data();
+    ext.zmobius_c_coeff.zmobius_c_coeff_len = 2 * ls;
+    ext.zmobius_c_coeff.zmobius_c_coeff_val = zc.data();
+  }
   trace("gjp");
   GJP.Initialize(do_arg);
   GJP.InitializeExt(ext);
   VRB.Level(VERBOSE_NONE_LEVEL);
-  if (action == 2) GJP.ZMobius_PC_Type((ZMobiusPCType)hdr[12]);
+  if (action >= 2) GJP.ZMobius_PC_Type((ZMobiusPCType)hdr[12]);
 
   Lattice *latp = 0;
   if (action == 0) latp = new GwilsonFwilson;
   else if (action == 1) latp = new GwilsonFdwf;
   else if (action == 2) latp = new GwilsonFmobius;
+  else if (action == 3) latp = new GwilsonFzmobius;
   else die("bad action");
   Lattice &lat = *latp;
   trace("lattice");
@@ -164,13 +190,26 @@ int main(int argc, char **argv) {
       op == OP_MOBIUS_D4) {
     read_all(fi, in, fsz * sizeof(double));
     if (op == OP_M5INV || op == OP_MOBIUS_D4) {
-      if (action != 2) die("M5INV / MOBIUS_D4 need the Mobius action");
-      DiracOpMobius d(lat, out, in, &cg_arg, CNV_FRM_NO);
+      if (action < 2) die("M5INV / MOBIUS_D4 need the Mobius or zMobius action");
+      DiracOp *dp = action == 2 ? (DiracOp *)new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO)
+                                : (DiracOp *)new DiracOpZMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
+      if (action == 3) fill_zmobius_coefficients(lat, ls);
       Dwf *arg = (Dwf *)lat.FdiracOpInitPtr();
       if (op == OP_M5INV)
         zmobius_m5inv(out, in, cg_arg.mass, dag, arg, arg->zmobius_kappa_ratio.data());
       else
         zmobius_dslash_4(out, (Matrix *)lat.GaugeField(), in, cb, dag, arg, cg_arg.mass);
+      delete dp;
+    } else if (action == 3) {
+      // DiracOpZMobius::Dslash is the unpreconditioned operator on full
+      // vectors; only MatPc / MatPcDag / MatPcDagMatPc are checkerboard operators.
+      if (op == OP_DSLASH) die("zMobius Dslash is not a checkerboard operator");
+      trace("zmobius ctor");
+      DiracOpZMobius d(lat, out, in, &cg_arg, CNV_FRM_NO);
+      fill_zmobius_coefficients(lat, ls);
+      trace("zmobius op");
+      rpar[0] = apply_op(d, op, out, in, cb, dag);
+      trace("zmobius done");
     } else if (action == 0) {
       DiracOpWilson d(lat, out, in, &cg_arg, CNV_FRM_NO);
       rpar[0] = apply_op(d, op, out, in, cb, dag);
@@ -205,7 +244,9 @@ int main(int argc, char **argv) {
     DiracOp *d = 0;
     if (action == 0) d = new DiracOpWilson(lat, out, in, &cg_arg, CNV_FRM_NO);
     else if (action == 1) d = new DiracOpDwf(lat, out, in, &cg_arg, CNV_FRM_NO);
-    else d = new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
+    else if (action == 2) d = new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
+    else d = new DiracOpZMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
+    if (action == 3) fill_zmobius_coefficients(lat, ls);
     Float true_res = 0;
     double t0 = now_s();
     int iters = d->InvCgShift(out, in, 0.0, &true_res, NULL);

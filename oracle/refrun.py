@@ -17,7 +17,7 @@ CPSREF = os.path.join(HERE, "_ref", "cpsref")
 
 OP_DSLASH, OP_MATPC, OP_MDAGM, OP_INVCG, OP_MINVCG, OP_M5INV, OP_MOBIUS_D4, OP_BENCH, OP_MATINV, OP_FCONVERT, \
     OP_MINRESEXT, OP_DMINUS, OP_FMATINV = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13
-ACTIONS = {"wilson": 0, "dwf": 1, "mobius": 2}
+ACTIONS = {"wilson": 0, "dwf": 1, "mobius": 2, "zmobius": 3}
 
 
 def available() -> bool:
@@ -26,8 +26,9 @@ def available() -> bool:
 
 def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8, a5_inv=1.0,
         b=1.5, c=0.5, stop_rsd=1e-10, max_iter=5000, shifts=(), ms_type=0, pc_type=2,
-        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0, dminus=0):
-    """Run one reference operation; returns (iters, rpar[64], payload array)."""
+        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0, dminus=0, zb=None, zc=None):
+    """Run one reference operation; returns (iters, rpar[64], payload array).
+    zMobius (action "zmobius") takes the complex per-slice coefficients zb, zc (ls each)."""
     if not available():
         raise RuntimeError("reference oracle not built (run oracle/build_ref.sh)")
     hdr = np.zeros(32, np.int64)
@@ -65,6 +66,11 @@ def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8
         with open(req, "wb") as f:
             f.write(hdr.tobytes())
             f.write(par.tobytes())
+            if hdr[1] == 3:
+                for z in (zb, zc):
+                    z = np.asarray(z, np.complex128)
+                    assert z.size == ls
+                    f.write(np.ascontiguousarray(np.stack([z.real, z.imag], 1).reshape(-1), np.float64).tobytes())
             f.write(np.ascontiguousarray(gauge, np.float64).tobytes())
             for v in vectors:
                 f.write(np.ascontiguousarray(v, np.float64).tobytes())
