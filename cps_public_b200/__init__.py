@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DWF, F16, F32, F64, MOBIUS, MULTI, ORDER_CANONICAL, ORDER_WILSON, SINGLE,  # noqa: F401
-                   WILSON, CgArg, CpsbError, DiracParams, SolveResult, check, ptr)
+                   WILSON, ZMOBIUS, CgArg, CpsbError, DiracParams, SolveResult, check, ptr)
 
 _initialised = None
 
@@ -67,7 +67,7 @@ class Gauge:
             pass
 
 
-ACTION_NAMES = {"wilson": WILSON, "dwf": DWF, "mobius": MOBIUS}
+ACTION_NAMES = {"wilson": WILSON, "dwf": DWF, "mobius": MOBIUS, "zmobius": ZMOBIUS}
 
 
 class DiracOp:
@@ -78,7 +78,8 @@ class DiracOp:
     """
 
     def __init__(self, gauge: Gauge, action="wilson", mass=0.1, ls=1, m5=1.8, a5_inv=1.0, b=1.5, c=0.5,
-                 pc_type=2):
+                 pc_type=2, bs=None, cs=None):
+        """zMobius ('zmobius') takes the complex per-slice coefficients bs, cs (ls each)."""
         self.gauge = gauge
         self.p = DiracParams()
         self.p.action = ACTION_NAMES[action] if isinstance(action, str) else int(action)
@@ -89,6 +90,14 @@ class DiracOp:
         self.p.mobius_b = b
         self.p.mobius_c = c
         self.p.pc_type = pc_type
+        if self.p.action == ZMOBIUS:
+            if bs is None or cs is None or len(bs) != self.p.ls or len(cs) != self.p.ls:
+                raise ValueError("zmobius needs bs and cs with ls entries each")
+            # (re, im) pairs, kept alive with the operator
+            self._zb = np.ascontiguousarray(np.stack([np.real(bs), np.imag(bs)], 1).reshape(-1), np.float64)
+            self._zc = np.ascontiguousarray(np.stack([np.real(cs), np.imag(cs)], 1).reshape(-1), np.float64)
+            self.p.zmobius_b = ptr(self._zb)
+            self.p.zmobius_c = ptr(self._zc)
         self.n = gauge.n4cb * self.p.ls * 24
 
     def _v(self, x):

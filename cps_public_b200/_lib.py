@@ -15,7 +15,7 @@ LIBPATH = os.path.join(HERE, "libcpsb200.so")
 
 CPSB_OK = 0
 CPSB_NOT_CONVERGED = 1
-WILSON, DWF, MOBIUS = 0, 1, 2
+WILSON, DWF, MOBIUS, ZMOBIUS = 0, 1, 2, 3
 F64, F32, F16 = 0, 1, 2
 ORDER_CANONICAL, ORDER_WILSON = 0, 1
 MULTI, SINGLE = 0, 1
@@ -34,7 +34,7 @@ SYMBOLS = [
 class DiracParams(C.Structure):
     _fields_ = [("action", C.c_int), ("ls", C.c_int), ("mass", C.c_double), ("m5", C.c_double),
                 ("a5_inv", C.c_double), ("mobius_b", C.c_double), ("mobius_c", C.c_double),
-                ("pc_type", C.c_int)]
+                ("pc_type", C.c_int), ("zmobius_b", C.POINTER(C.c_double)), ("zmobius_c", C.POINTER(C.c_double))]
 
 
 class CgArg(C.Structure):

@@ -35,4 +35,29 @@ struct M5Coef {
 cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
                       int xpay, int norm, Reduce red, const int *skip, cudaStream_t st);
 
+// zMobius form (complex per-slice coefficients, zmobius_m5inv.C:247-400 and
+// :403-686, zmobius_dslash_5_plus.C:125-376): one table per launch shape, in
+// device memory.  The kernel applies, per 4-D site and chirality half h
+// (0: spins 0,1; 1: spins 2,3) to the column v[0..Ls) of one component:
+//   pre:   v_s *= pre_s
+//   dag 1: v_s <- bb_s v_s + cc[h]_s v_nb          (mixing before the sweeps)
+//   sweep: walls first:  v_last *= invd[h]; v_last += w[h]_s v_s (s ascending);
+//                        v_s += a[h]_s v_{s+1} (s descending)
+//          chain first:  v_{s+1} += a[h]_s v_s (s ascending);
+//                        v_s += w[h]_s v_last (s descending); v_last *= invd[h]
+//   dag 0: v_s <- bb_s v_s + cc[h]_s v_nb          (mixing after the sweeps)
+//   post:  v_s *= post_s, then out = [x +] v
+// with nb = s-1 / s+1 (cyclic) for the upper / lower half at dag 0 and the
+// reverse at dag 1 (the wall terms carry -m_f in cc).
+struct ZM5Tab {
+  double2 a[2][64], w[2][64];
+  double2 invd[2];
+  int walls_first[2];
+  double2 bb[64], cc[2][64];
+  double2 pre[64], post[64];
+  int sweep, mix, pre_on, post_on;
+};
+cudaError_t launch_m5z(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
+                       const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip, cudaStream_t st);
+
 }  // namespace cpsb

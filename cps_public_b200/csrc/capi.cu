@@ -31,7 +31,9 @@ void need_init() {
 
 void check_params(cpsb_gauge h, const cpsb_dirac_params *p) {
   if (!h || !p) throw Error{CPSB_ERR_ARG, "null gauge handle or parameters"};
-  if (p->action < CPSB_WILSON || p->action > CPSB_MOBIUS) throw Error{CPSB_ERR_ARG, "unknown action"};
+  if (p->action < CPSB_WILSON || p->action > CPSB_ZMOBIUS) throw Error{CPSB_ERR_ARG, "unknown action"};
+  if (p->action == CPSB_ZMOBIUS && (!p->zmobius_b || !p->zmobius_c))
+    throw Error{CPSB_ERR_ARG, "zMobius needs the zmobius_b and zmobius_c coefficient arrays"};
   if (p->action != CPSB_WILSON && (p->ls < 2 || p->ls > 64)) throw Error{CPSB_ERR_ARG, "ls must be in [2, 64]"};
 }
 
@@ -523,6 +525,8 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     check_params(h, p);
     check_cg(a);
     if (!out || !in || !res) throw Error{CPSB_ERR_ARG, "null vector or result"};
+    if (p->action == CPSB_ZMOBIUS)
+      throw Error{CPSB_ERR_UNSUPPORTED, "zMobius MatInv (DiracOpZMobius::MatInv) is not implemented"};
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     const long n = op.nsites();

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <complex>
+
 #include <map>
 #include <memory>
 #include <mutex>
@@ -92,6 +94,11 @@ struct Operator {
   double kappa = 0;        // Wilson / DWF
   double kappa_b = 0;      // Mobius
   M5Coef m5c[2];           // Mobius M5^-1 coefficient sets (dag 0, dag 1)
+  // zMobius: the per-slice coefficients (copied from the parameters) and the
+  // four m5z tables of MatPc (dag 0: kb and -kb stages; dag 1: the scaled and
+  // the xpay stage), in device memory
+  std::vector<std::complex<double>> zb, zc;
+  DevBuf ztab;
   Field t1, t2, t3;
   RedSlot red_inner;
 
@@ -125,7 +132,10 @@ struct Operator {
   // (Wilson / DWF in FP32 or 16-bit): |MatPc p|^2 -> red_d, then
   // r -= alpha (A p + shift p), |r|^2 and the recurrence scalars in S; A p is
   // not stored (scratch receives it only while a launch shape is being tuned).
-  bool can_fuse_cg_r() const { return prec != P64 && p.action != CPSB_MOBIUS; }
+  bool can_fuse_cg_r() const { return prec != P64 && (p.action == CPSB_WILSON || p.action == CPSB_DWF); }
+  bool mobius_like() const { return p.action == CPSB_MOBIUS || p.action == CPSB_ZMOBIUS; }
+  void matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
+                     cudaStream_t st);
   void mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip, CgState *S,
                   const SpinorPtr &r, const Reduce *red_r, cudaStream_t st);
   // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
@@ -168,7 +178,8 @@ struct CgSolver {
  private:
   void launch_batch(int k, cudaStream_t st);
   void run_batches(int batch, cudaStream_t st, const bool *done, bool any);
-  void true_residual(double *rr_out, const double *bnorm, cudaStream_t st);
+  void true_residual(double *rr_out, const double *bnorm, cudaStream_t st, const int *skip_h = nullptr,
+                     const int *skip_d = nullptr);
 };
 
 int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_t st);

@@ -191,4 +191,147 @@ cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr
   return cudaErrorInvalidValue;  // FP16 Mobius storage is not supported by this kernel
 }
 
+// ----------------------------------------------------------------- zMobius
+template <typename T> __device__ __forceinline__ cplx<T> ldz(const double2 *p) {
+  const double2 v = __ldg(p);
+  return mk((T)v.x, (T)v.y);
+}
+#define ZAXPYC(dst, f, src)                                  \
+  _Pragma("unroll") for (int q = 0; q < NC; q++) (dst)[q] = (dst)[q] + cmul((f), (src)[q]);
+#define ZSCALC(dst, f)                                       \
+  _Pragma("unroll") for (int q = 0; q < NC; q++) (dst)[q] = cmul((f), (dst)[q]);
+
+template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
+__global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv,
+                                                 const ZM5Tab *tab, Reduce red, const int *skip) {
+  typedef typename ChunkT<P>::T T;
+  const int NCH = ChunkT<P>::NCH, NC = ChunkT<P>::NC;
+  __shared__ double sh[NT / 32];
+  const int rhs = blockIdx.y;
+  const long per = (long)g.n4cb * LS;
+  const long work = (long)g.n4cb * NCH;
+  double acc = 0;
+  const bool sk = skip && skip[rhs];
+  const int sweep = tab->sweep, mix = tab->mix, pre_on = tab->pre_on, post_on = tab->post_on;
+  for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
+    const int x = (int)(w % g.n4cb);
+    const int k = (int)(w / g.n4cb);
+    const int h = (k < NCH / 2) ? 0 : 1;
+    const long base = rhs * per + x;
+    cplx<T> v[LS][NC], y[LS][NC];
+#pragma unroll
+    for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
+    if (pre_on) {
+#pragma unroll
+      for (int s = 0; s < LS; s++) { ZSCALC(v[s], ldz<T>(&tab->pre[s])); }
+    }
+    // upper half at dag 0 and lower half at dag 1 take slice s-1, the others s+1
+    const bool from_below = (DAG == 0) == (h == 0);
+    if (DAG == 1 && mix) {
+#pragma unroll
+      for (int s = 0; s < LS; s++) {
+        const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
+        const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
+      }
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
+    }
+    if (sweep) {
+      if (tab->walls_first[h]) {
+        ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
+#pragma unroll
+        for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[LS - 1], ldz<T>(&tab->w[h][s]), v[s]); }
+#pragma unroll
+        for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->a[h][s]), v[s + 1]); }
+      } else {
+#pragma unroll
+        for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[s + 1], ldz<T>(&tab->a[h][s]), v[s]); }
+#pragma unroll
+        for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->w[h][s]), v[LS - 1]); }
+        ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
+      }
+    }
+    if (DAG == 0 && mix) {
+#pragma unroll
+      for (int s = 0; s < LS; s++) {
+        const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
+        const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
+    }
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      if (post_on) { ZSCALC(y[s], ldz<T>(&tab->post[s])); }
+      cplx<T> o[NC];
+      if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
+#pragma unroll
+      for (int q = 0; q < NC; q++) {
+        o[q] = XPAY ? o[q] + y[s][q] : y[s][q];
+        if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
+      }
+      st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
+    }
+  }
+  if (NORM) {
+    double bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bs;
+    if (last_block(red.ticket, gridDim.x * gridDim.y)) {
+      for (int q = 0; q < g.nrhs; q++) {
+        double t = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
+        if (threadIdx.x == 0 && !(skip && skip[q])) red.result[q] = t;
+        __syncthreads();
+      }
+    }
+  }
+}
+
+template <int P, int LS>
+static cudaError_t m5z_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
+                                 const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip,
+                                 cudaStream_t st) {
+  const int NT = 128;
+  dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
+#define M5ZL(D, XP, NR)                                                                             \
+  if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
+    m5z_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, tab, red, skip);           \
+    return launched();                                                                              \
+  }
+  M5ZL(0, false, false) M5ZL(1, false, false) M5ZL(1, true, false) M5ZL(1, true, true)
+#undef M5ZL
+  return cudaErrorInvalidValue;
+}
+
+template <int P>
+static cudaError_t m5z_launch_p(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
+                                const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip,
+                                cudaStream_t st) {
+  switch (g.ls) {
+    case 4: return m5z_launch_ls<P, 4>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 8: return m5z_launch_ls<P, 8>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 12: return m5z_launch_ls<P, 12>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 16: return m5z_launch_ls<P, 16>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 20: return m5z_launch_ls<P, 20>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 24: return m5z_launch_ls<P, 24>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 32: return m5z_launch_ls<P, 32>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_m5z(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
+                       const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  if (prec == P64) return m5z_launch_p<P64>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+  if (prec == P32) return m5z_launch_p<P32>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace cpsb

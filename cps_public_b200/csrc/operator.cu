@@ -150,8 +150,130 @@ static void m5_coefficients(double K, double mass, int ls, M5Coef *c0, M5Coef *c
   c1->invd = invd1;
 }
 
+// zMobius (DiracOpZMobius with complex b_s, c_s): kappa_b(s) = 1/(2(b_s(4-M5)+a5_inv)),
+// kappa_c(s) = 1/(2(c_s(4-M5)-a5_inv)), K_s = kappa_b(s)/kappa_c(s) (reset_mobius_arg,
+// d_op_zmobius.C:246-295), and the four m5z tables of MatPc / MatPcDag (SYM2,
+// zmobius_m-sym2.h, zmobius_mdag-sym2.h) in the step order of zmobius_m5inv.C:
+//   dag 0  t1 = kb  . mix(M5^-1 in);  t3 = D_W(1) t1;
+//          t1 = -kb . mix(M5^-1 t3);  out = in + D_W(0) t1
+//   dag 1  t1 = D_W^dag(1) in;  t3 = conj(kb) . M5^-dag(mix^dag(-conj(kb) . t1));
+//          t1 = D_W^dag(0) t3;  out = in + M5^-dag(mix^dag(t1))
+// (the per-slice factors commute with the 4-D hop, which acts slice by slice).
+typedef std::complex<double> zc_t;
+static double2 d2(zc_t z) { return make_double2(z.real(), z.imag()); }
+
+static void zmobius_sweeps(ZM5Tab &t, int dag, int ls, double m, const zc_t *K) {
+  const zc_t one(1.0, 0.0);
+  if (!dag) {
+    zc_t prod = one;
+    for (int i = 0; i < ls; i++) prod *= -K[i];
+    prod *= m;
+    const zc_t invd = one / (one + prod);
+    // upper: chain first (v_{s+1} += -K_{s+1} v_s), walls from the last slice
+    t.walls_first[0] = 0;
+    for (int s = 0; s <= ls - 2; s++) t.a[0][s] = d2(-K[s + 1]);
+    zc_t pr = one;
+    for (int i = 0; i < ls - 1; i++) pr *= -K[i];
+    zc_t fr = -(m * pr) * invd;
+    for (int s = ls - 2; s >= 0; s--) {
+      t.w[0][s] = d2(fr);
+      fr /= -K[s];
+    }
+    t.invd[0] = d2(invd);
+    // lower: walls first (v_last += f v_s), then v_s += -K_s v_{s+1}
+    t.walls_first[1] = 1;
+    zc_t fl = m * K[ls - 1] * invd;
+    for (int s = 0; s <= ls - 2; s++) {
+      t.w[1][s] = d2(fl);
+      fl *= -K[s];
+    }
+    for (int s = 0; s <= ls - 2; s++) t.a[1][s] = d2(-K[s]);
+    t.invd[1] = d2(invd);
+  } else {
+    zc_t prod = one;
+    for (int i = 0; i < ls; i++) prod *= K[i];
+    prod *= m;
+    const zc_t invd = std::conj(one / (one + prod));
+    // upper: walls first, then v_s += -conj(K_{s+1}) v_{s+1}
+    t.walls_first[0] = 1;
+    zc_t fr = m * std::conj(K[0]) * invd;
+    for (int s = 0; s <= ls - 2; s++) {
+      t.w[0][s] = d2(fr);
+      fr *= -std::conj(K[s + 1]);
+    }
+    for (int s = 0; s <= ls - 2; s++) t.a[0][s] = d2(-std::conj(K[s + 1]));
+    t.invd[0] = d2(invd);
+    // lower: chain first (v_{s+1} += -conj(K_s) v_s), walls from the last slice
+    t.walls_first[1] = 0;
+    for (int s = 0; s <= ls - 2; s++) t.a[1][s] = d2(-std::conj(K[s]));
+    zc_t pr = one;
+    for (int i = 0; i < ls - 2; i++) pr *= -K[i];
+    pr *= -K[ls - 1];
+    zc_t fl = -(m * std::conj(pr)) * invd;
+    for (int s = ls - 2; s >= 0; s--) {
+      t.w[1][s] = d2(fl);
+      if (s > 0) fl /= -std::conj(K[s - 1]);
+    }
+    t.invd[1] = d2(invd);
+  }
+  t.sweep = 1;
+}
+
+// b_s v_s + c-hop (zmobius_dslash_4.C:90-121 with zmobius_dslash_5_plus.C:125-376,
+// dag 0) or its adjoint (dag 1: conj(b_s), conjugated and index-shifted c).
+static void zmobius_mix(ZM5Tab &t, int dag, int ls, double m, const zc_t *b, const zc_t *c) {
+  for (int s = 0; s < ls; s++) t.bb[s] = d2(dag ? std::conj(b[s]) : b[s]);
+  if (!dag) {
+    for (int s = 0; s < ls; s++) {
+      t.cc[0][s] = d2(s == 0 ? -m * c[0] : c[s]);             // upper: from s-1
+      t.cc[1][s] = d2(s == ls - 1 ? -m * c[ls - 1] : c[s]);   // lower: from s+1
+    }
+  } else {
+    for (int s = 0; s < ls; s++) {
+      t.cc[0][s] = d2(s == ls - 1 ? -m * std::conj(c[0]) : std::conj(c[s + 1]));  // upper: from s+1
+      t.cc[1][s] = d2(s == 0 ? -m * std::conj(c[ls - 1]) : std::conj(c[s - 1]));  // lower: from s-1
+    }
+  }
+  t.mix = 1;
+}
+
+static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
+  const int ls = op.geom.ls;
+  if (pp.pc_type != 2) throw Error{CPSB_ERR_UNSUPPORTED, "zMobius: only the ZMOB_PC_SYM2 preconditioner is implemented"};
+  if (!pp.zmobius_b || !pp.zmobius_c) throw Error{CPSB_ERR_ARG, "zMobius needs zmobius_b and zmobius_c"};
+  op.zb.resize(ls);
+  op.zc.resize(ls);
+  std::vector<zc_t> kb(ls), K(ls);
+  for (int s = 0; s < ls; s++) {
+    op.zb[s] = zc_t(pp.zmobius_b[2 * s], pp.zmobius_b[2 * s + 1]);
+    op.zc[s] = zc_t(pp.zmobius_c[2 * s], pp.zmobius_c[2 * s + 1]);
+    kb[s] = 1.0 / (2.0 * (op.zb[s] * (4 - pp.m5) + pp.a5_inv));
+    const zc_t kc = 1.0 / (2.0 * (op.zc[s] * (4 - pp.m5) - pp.a5_inv));
+    K[s] = kb[s] / kc;
+  }
+  std::vector<ZM5Tab> t(4);
+  memset(t.data(), 0, sizeof(ZM5Tab) * 4);
+  for (int k = 0; k < 4; k++) {
+    const int dag = k >= 2;
+    zmobius_sweeps(t[k], dag, ls, pp.mass, K.data());
+    zmobius_mix(t[k], dag, ls, pp.mass, op.zb.data(), op.zc.data());
+  }
+  for (int s = 0; s < ls; s++) {
+    t[0].post[s] = d2(kb[s]);
+    t[1].post[s] = d2(-kb[s]);
+    t[2].pre[s] = d2(-std::conj(kb[s]));
+    t[2].post[s] = d2(std::conj(kb[s]));
+  }
+  t[0].post_on = t[1].post_on = 1;
+  t[2].pre_on = t[2].post_on = 1;
+  op.ztab.alloc(sizeof(ZM5Tab) * 4);
+  CK(cudaMemcpy(op.ztab.p, t.data(), sizeof(ZM5Tab) * 4, cudaMemcpyHostToDevice));
+  op.kappa_b = kb[0].real();
+}
+
 Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g), p(pp), prec(pr), nrhs(nr) {
-  if (p.action < 0 || p.action > 2) throw Error{CPSB_ERR_ARG, "unknown action"};
+  if (p.action < 0 || p.action > 3) throw Error{CPSB_ERR_ARG, "unknown action"};
+  p.zmobius_b = p.zmobius_c = nullptr;  // the caller's arrays are read here only (zb, zc keep copies)
   const int ls = p.action == CPSB_WILSON ? 1 : p.ls;
   if (ls < 1 || ls > 64) throw Error{CPSB_ERR_ARG, "ls out of range"};
   if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
@@ -166,14 +288,18 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   geom.nsites = (long)geom.n4cb * ls * nrhs;
   if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
   if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
-  if (p.action == CPSB_MOBIUS) {
-    if (p.pc_type < 0 || p.pc_type > 2)
-      throw Error{CPSB_ERR_UNSUPPORTED, "Mobius preconditioners: ZMOB_PC_ORIG (0), ZMOB_PC_SYM1 (1), ZMOB_PC_SYM2 (2)"};
-    if (prec == P16) throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
+  if (mobius_like()) {
+    if (prec == P16) throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     const int ok[] = {4, 8, 12, 16, 20, 24, 32};
     bool found = false;
     for (int v : ok) found |= (v == ls);
     if (!found) throw Error{CPSB_ERR_UNSUPPORTED, "Mobius Ls must be one of 4,8,12,16,20,24,32"};
+    t3.create(prec, geom.nsites);
+  }
+  if (p.action == CPSB_ZMOBIUS) zmobius_setup(*this, pp);
+  if (p.action == CPSB_MOBIUS) {
+    if (p.pc_type < 0 || p.pc_type > 2)
+      throw Error{CPSB_ERR_UNSUPPORTED, "Mobius preconditioners: ZMOB_PC_ORIG (0), ZMOB_PC_SYM1 (1), ZMOB_PC_SYM2 (2)"};
     kappa_b = 1.0 / (2 * (p.mobius_b * (4 - p.m5) + p.a5_inv));
     const double kappa_c = 1.0 / (2 * (p.mobius_c * (4 - p.m5) - p.a5_inv));
     m5_coefficients(kappa_b / kappa_c, p.mass, ls, &m5c[0], &m5c[1]);
@@ -183,7 +309,6 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
       m5c[d].mass = p.mass;
       m5c[d].scale = 1.0;
     }
-    t3.create(prec, geom.nsites);
   }
   t1.create(prec, geom.nsites);
   t2.create(prec, geom.nsites);
@@ -219,6 +344,9 @@ void Operator::hop(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, d
 }
 
 void Operator::dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, cudaStream_t st) {
+  if (p.action == CPSB_ZMOBIUS)
+    throw Error{CPSB_ERR_UNSUPPORTED,
+                "zMobius Dslash: DiracOpZMobius::Dslash is the unpreconditioned operator on full vectors"};
   if (p.action != CPSB_MOBIUS) {
     hop(out, in, cb, dag, 1.0, nullptr, nullptr, nullptr, st);
     return;
@@ -252,6 +380,10 @@ void Operator::dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag
 
 void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
                      cudaStream_t st) {
+  if (p.action == CPSB_ZMOBIUS) {
+    matpc_zmobius(out, in, dag, red, skip, st);
+    return;
+  }
   if (p.action != CPSB_MOBIUS) {
     hop(t1.ptr(), in, 1, dag, 1.0, nullptr, nullptr, skip, st);
     hop(out, t1.ptr(), 0, dag, -kappa * kappa, &in, red, skip, st);
@@ -342,6 +474,24 @@ void Operator::matpc_orig_sym1(const SpinorPtr &out, const SpinorPtr &in, int da
     CK(launch_m5(prec, 1, geom, out, in, out, h5, 1, red != nullptr, rd, skip, st));
   } else {
     CK(launch_m5(prec, 1, geom, out, t1.ptr(), in, mix, 1, red != nullptr, rd, skip, st));
+  }
+}
+
+void Operator::matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red,
+                             const int *skip, cudaStream_t st) {
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  const ZM5Tab *t = (const ZM5Tab *)ztab.p;
+  if (!dag) {
+    CK(launch_m5z(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, t + 0, 0, 0, none, skip, st));
+    hop(t3.ptr(), t1.ptr(), 1, 0, 1.0, nullptr, nullptr, skip, st);
+    CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 1, 0, 0, none, skip, st));
+    hop(out, t1.ptr(), 0, 0, 1.0, &in, red, skip, st);
+  } else {
+    hop(t1.ptr(), in, 1, 1, 1.0, nullptr, nullptr, skip, st);
+    CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 2, 0, 0, none, skip, st));
+    hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+    CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 3, 1, red != nullptr, red ? *red : none, skip, st));
   }
 }
 

@@ -48,7 +48,7 @@ static double now_ms() {
 // plus the one-vector CPS-order FP64 staging buffer of the work item.
 static size_t solve_footprint(const cpsb_dirac_params &p, long n, int sloppy, int nrhs) {
   const long N = n * nrhs;
-  const int op_tmp = p.action == CPSB_MOBIUS ? 3 : 2;   // Operator::t1, t2 (t3 for Mobius)
+  const int op_tmp = p.action >= CPSB_MOBIUS ? 3 : 2;   // Operator::t1, t2 (t3 for Mobius / zMobius)
   size_t b = field_bytes(P64, N) * 3 + field_bytes(P64, n);  // x, b, r; staging
   if (sloppy == P64) {
     b += field_bytes(P64, N) * (3 + op_tmp);             // r, p, Ap; temporaries of the FP64 operator
@@ -63,7 +63,7 @@ static size_t solve_footprint(const cpsb_dirac_params &p, long n, int sloppy, in
 // solutions, Krylov vectors in the Krylov precision, the operator's
 // temporaries, and the one-RHS refinement solver of reduced-precision runs.
 static size_t multishift_footprint(const cpsb_dirac_params &p, long n, int prec, int nshift, int nvec) {
-  const int op_tmp = p.action == CPSB_MOBIUS ? 3 : 2;
+  const int op_tmp = p.action >= CPSB_MOBIUS ? 3 : 2;
   const int px = prec == P64 ? P64 : P32;
   size_t b = field_bytes(P64, n) * (2 + nvec);                        // chi, staging, x[s]
   b += field_bytes(prec, n) * (2 + nshift + op_tmp) + field_bytes(px, n) * nshift;  // r, Ap, p_s, temps; psi_s
@@ -75,6 +75,7 @@ struct ServeRequest {
   unsigned long long id = 0;
   cpsb_gauge h = nullptr;
   cpsb_dirac_params p;
+  std::vector<double> zb, zc;  // zMobius coefficients owned by the request (p points here)
   cpsb_cg_arg a;
   int nrhs = 0;
   std::vector<double *> x;
@@ -290,8 +291,8 @@ int cpsb_serve_submit(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p,
     if (!srv || !id || !x || !b || nrhs < 1 || nrhs > 4096) throw Error{CPSB_ERR_ARG, "bad submit arguments"};
     for (int i = 0; i < nrhs; i++)
       if (!x[i] || !b[i]) throw Error{CPSB_ERR_ARG, "null vector"};
-    if (p->action == CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
-      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
+    if (p->action >= CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
+      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     Server &S = srv->s;
     const long n = cb_sites(h, p);
     int g = std::min(nrhs, MAX_RHS);
@@ -300,6 +301,12 @@ int cpsb_serve_submit(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p,
     std::unique_ptr<ServeRequest> r(new ServeRequest);
     r->h = h;
     r->p = *p;
+    if (p->action == CPSB_ZMOBIUS) {
+      r->zb.assign(p->zmobius_b, p->zmobius_b + 2 * p->ls);
+      r->zc.assign(p->zmobius_c, p->zmobius_c + 2 * p->ls);
+      r->p.zmobius_b = r->zb.data();
+      r->p.zmobius_c = r->zc.data();
+    }
     r->a = *a;
     r->nrhs = nrhs;
     r->x.assign(x, x + nrhs);
@@ -339,8 +346,8 @@ int cpsb_serve_submit_minvcg(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_par
       throw Error{CPSB_ERR_ARG, "bad multishift submit arguments"};
     if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE"};
     if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
-    if (p->action == CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
-      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius"};
+    if (p->action >= CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
+      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     const int nvec = type == CPSB_SINGLE ? 1 : nshift;
     for (int i = 0; i < nvec; i++)
       if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
@@ -351,6 +358,12 @@ int cpsb_serve_submit_minvcg(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_par
     std::unique_ptr<ServeRequest> r(new ServeRequest);
     r->h = h;
     r->p = *p;
+    if (p->action == CPSB_ZMOBIUS) {
+      r->zb.assign(p->zmobius_b, p->zmobius_b + 2 * p->ls);
+      r->zc.assign(p->zmobius_c, p->zmobius_c + 2 * p->ls);
+      r->p.zmobius_b = r->zb.data();
+      r->p.zmobius_c = r->zc.data();
+    }
     r->a = *a;
     r->nrhs = 1;
     r->multishift = true;

@@ -50,6 +50,7 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
   }
   state.alloc(sizeof(CgState));
   CK(cudaMallocHost((void **)&hstate, sizeof(CgState)));
+  p.zmobius_b = p.zmobius_c = nullptr;  // the operators hold copies of the zMobius coefficients
   scal.alloc(sizeof(double) * MAX_RHS * 8);
 }
 
@@ -136,28 +137,35 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
   }
 }
 
-// rr_out[q] = |b - (A + shift) x64|^2 (FP64), leaves r64 = b - (A + shift) x64.
-void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t st) {
+// rr_out[q] = |b - (A + shift) x64|^2 (FP64), leaves r64 = b - (A + shift) x64,
+// for every right-hand side q not masked by skip_h (host) / skip_d (the same
+// mask on the device); masked entries of rr_out and r64 are left as they were.
+void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t st, const int *skip_h,
+                             const int *skip_d) {
   (void)bnorm;
   double *dres = (double *)scal.p;
   // r = b - (A + shift) x, formed in place in r (no separate A x vector)
   if (op64->nrhs == nrhs) {
-    op64->mdagm(r64, x64, nullptr, nullptr, st);
+    op64->mdagm(r64, x64, nullptr, skip_d, st);
   } else {
     const long n1 = op64->nsites();
-    for (int q = 0; q < nrhs; q++) op64->mdagm(r64.view(q * n1), x64.view(q * n1), nullptr, nullptr, st);
+    for (int q = 0; q < nrhs; q++)
+      if (!(skip_h && skip_h[q])) op64->mdagm(r64.view(q * n1), x64.view(q * n1), nullptr, nullptr, st);
   }
   Reduce rm = red_misc.r(dres);
   if (shift != 0.0) {
     Reduce none;
     memset(&none, 0, sizeof(none));
-    CK(launch_axpby(P64, r64.ptr(), P64, r64.ptr(), P64, x64.ptr(), geom, sc2(nrhs, 1.0, shift), nullptr,
+    CK(launch_axpby(P64, r64.ptr(), P64, r64.ptr(), P64, x64.ptr(), geom, sc2(nrhs, 1.0, shift), skip_d,
                     none, 0, st));
   }
-  CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, r64.ptr(), geom, sc2(nrhs, 1.0, -1.0), nullptr, rm, 1,
+  CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, r64.ptr(), geom, sc2(nrhs, 1.0, -1.0), skip_d, rm, 1,
                   st));
-  CK(cudaMemcpyAsync(rr_out, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+  double rr[MAX_RHS];
+  CK(cudaMemcpyAsync(rr, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  for (int q = 0; q < nrhs; q++)
+    if (!(skip_h && skip_h[q])) rr_out[q] = rr[q];
 }
 
 int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma) {
@@ -207,6 +215,10 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   CK(cudaMemcpyAsync(pS.data.p, rS.data.p, rS.data.bytes, cudaMemcpyDeviceToDevice, st));
   if (pS.norm.p) CK(cudaMemcpyAsync(pS.norm.p, rS.norm.p, rS.norm.bytes, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(state.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st));
+  // The host mirror starts from this solve's state: a right-hand side that has
+  // converged before the first iteration reports it (CPS: itr + 1 = 1), not
+  // the state the previous solve left behind.
+  *hstate = hs;
 
   int batch = a.batch > 0 ? a.batch : 16;
   int status = CPSB_OK;
@@ -230,7 +242,8 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
     memset(&none, 0, sizeof(none));
     CK(launch_axpby(P64, x64.ptr(), P64, x64.ptr(), P32, xS.ptr(), gg, sc2(nrhs, 1.0, 1.0), dskip, none, 0, st));
     CK(launch_axpby(P32, xS.ptr(), P32, xS.ptr(), P32, SpinorPtr{}, gg, sc2(nrhs, 0.0, 0.0), dskip, none, 0, st));
-    true_residual(rr, bnorm, st);
+    // only the right-hand sides that paused need their FP64 residual
+    true_residual(rr, bnorm, st, skip_h, dskip);
     Scal2 beta = sc2(nrhs, 1.0, 0.0);
     for (int q = 0; q < nrhs; q++) {
       if (skip_h[q]) continue;
@@ -302,6 +315,7 @@ struct SolverKey {
   Gauge *G;
   int action, ls, sloppy, nrhs, pc;
   double mass, m5, a5, b, c;
+  double zb[128], zc[128];  // zMobius b_s, c_s (re, im) by value
   bool operator<(const SolverKey &o) const {
     return memcmp(this, &o, sizeof(SolverKey)) < 0;
   }
@@ -326,6 +340,11 @@ CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs)
   k.a5 = p.a5_inv;
   k.b = p.mobius_b;
   k.c = p.mobius_c;
+  if (p.action == CPSB_ZMOBIUS)
+    for (int i = 0; i < 2 * k.ls && i < 128; i++) {
+      k.zb[i] = p.zmobius_b[i];
+      k.zc[i] = p.zmobius_c[i];
+    }
   std::lock_guard<std::mutex> lk(solvers_mu);
   auto &m = solvers();
   auto it = m.find(k);

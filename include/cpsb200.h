@@ -32,7 +32,7 @@ extern "C" {
 #define CPSB_ERR_NO_DEVICE (-6)
 #define CPSB_ERR_BUSY (-7)
 
-enum cpsb_action { CPSB_WILSON = 0, CPSB_DWF = 1, CPSB_MOBIUS = 2 };
+enum cpsb_action { CPSB_WILSON = 0, CPSB_DWF = 1, CPSB_MOBIUS = 2, CPSB_ZMOBIUS = 3 };
 enum cpsb_precision { CPSB_PREC_F64 = 0, CPSB_PREC_F32 = 1, CPSB_PREC_F16 = 2 };
 enum cpsb_gauge_order { CPSB_ORDER_CANONICAL = 0, CPSB_ORDER_WILSON = 1 };
 enum cpsb_multishift_type { CPSB_MULTI = 0, CPSB_SINGLE = 1 };
@@ -49,8 +49,13 @@ typedef struct cpsb_gauge_s *cpsb_gauge;
  *   mobius_b, mobius_c   GJP.Mobius_b/c() (gjp.h:594-601)
  *   pc_type GJP.ZMobius_PC_Type() (include/util/dwf.h:42-48): ZMOB_PC_ORIG (0),
  *           ZMOB_PC_SYM1 (1) and ZMOB_PC_SYM2 (2, the CPS default, src/util/gjp/
- *           gjp.C:129) are implemented; the MIT and SYM3 forms (which read the
- *           zMobius coefficient arrays) return CPSB_ERR_UNSUPPORTED. */
+ *           gjp.C:129) are implemented for Mobius, SYM2 for zMobius; the MIT and
+ *           SYM3 forms return CPSB_ERR_UNSUPPORTED.
+ *   zmobius_b, zmobius_c   zMobius (CPSB_ZMOBIUS) only: the complex per-slice
+ *           coefficients b_s, c_s as ls (re, im) pairs each, the layout of
+ *           DoArgExt::zmobius_b_coeff / zmobius_c_coeff (GJP.ZMobius_b/c(),
+ *           src/util/gjp/gjp.C:167-178).  Read during the call only (solvers
+ *           and the request loop keep copies); ignored for the other actions. */
 typedef struct {
   int action;
   int ls;
@@ -60,6 +65,8 @@ typedef struct {
   double mobius_b;
   double mobius_c;
   int pc_type;
+  const double *zmobius_b;
+  const double *zmobius_c;
 } cpsb_dirac_params;
 
 /* Solver controls: CgArg::stop_rsd / max_num_iter plus the precision forms.

@@ -97,9 +97,11 @@ static double apply_op(D &d, int op, Vector *out, Vector *in, int cb, int dag) {
 // DiracOpZMobius's constructor (d_op_zmobius.C:315-368) resets the kappa arrays
 // but never fills Dwf::zmobius_b / zmobius_c, which zmobius_dslash_4 reads
 // (zmobius_dslash_4.C:61-62, :151-152); only DiracOpMobius fills them
-// (d_op_mobius.C:111-118).  The harness copies GJP's zMobius coefficients there
-// (what the disabled branch at zmobius_dslash_4.C:64-65 reads), so the
-// reference's zMobius kernels run on the coefficients the job set.
+// (d_op_mobius.C:111-118), so as shipped every zMobius checkerboard operator
+// dereferences empty arrays.  The harness copies GJP's zMobius coefficients
+// into the lattice's Dwf struct once (what the disabled branch at
+// zmobius_dslash_4.C:64-65 reads), so the reference's zMobius kernels run on
+// the coefficients the job set.
 static void fill_zmobius_coefficients(Lattice &lat, int ls) {
   Dwf *arg = (Dwf *)lat.FdiracOpInitPtr();
   arg->zmobius_b.assign(GJP.ZMobius_b(), GJP.ZMobius_b() + ls);
@@ -169,6 +171,7 @@ int main(int argc, char **argv) {
   else if (action == 3) latp = new GwilsonFzmobius;
   else die("bad action");
   Lattice &lat = *latp;
+  if (action == 3) fill_zmobius_coefficients(lat, ls);  // kept by the lattice's Dwf struct
   trace("lattice");
   read_all(fi, (void *)lat.GaugeField(), vol * 4 * 18 * sizeof(double));
 
@@ -193,7 +196,6 @@ int main(int argc, char **argv) {
       if (action < 2) die("M5INV / MOBIUS_D4 need the Mobius or zMobius action");
       DiracOp *dp = action == 2 ? (DiracOp *)new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO)
                                 : (DiracOp *)new DiracOpZMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
-      if (action == 3) fill_zmobius_coefficients(lat, ls);
       Dwf *arg = (Dwf *)lat.FdiracOpInitPtr();
       if (op == OP_M5INV)
         zmobius_m5inv(out, in, cg_arg.mass, dag, arg, arg->zmobius_kappa_ratio.data());
@@ -206,7 +208,6 @@ int main(int argc, char **argv) {
       if (op == OP_DSLASH) die("zMobius Dslash is not a checkerboard operator");
       trace("zmobius ctor");
       DiracOpZMobius d(lat, out, in, &cg_arg, CNV_FRM_NO);
-      fill_zmobius_coefficients(lat, ls);
       trace("zmobius op");
       rpar[0] = apply_op(d, op, out, in, cb, dag);
       trace("zmobius done");
@@ -246,7 +247,6 @@ int main(int argc, char **argv) {
     else if (action == 1) d = new DiracOpDwf(lat, out, in, &cg_arg, CNV_FRM_NO);
     else if (action == 2) d = new DiracOpMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
     else d = new DiracOpZMobius(lat, out, in, &cg_arg, CNV_FRM_NO);
-    if (action == 3) fill_zmobius_coefficients(lat, ls);
     Float true_res = 0;
     double t0 = now_s();
     int iters = d->InvCgShift(out, in, 0.0, &true_res, NULL);
@@ -272,8 +272,20 @@ int main(int argc, char **argv) {
       args[s] = cg_arg; args[s].stop_rsd = rsd[s]; argp[s] = &args[s];
     }
     double t0 = now_s();
-    int iters = lat.FmatEvlMInv(sol.data(), in, par + 8, nshift, 0, argp.data(), CNV_FRM_NO,
-                                type == 1 ? SINGLE : MULTI, alpha.data());
+    int iters = 0;
+    if (action == 3) {
+      // Fzmobius inherits FdwfBase::FmatEvlMInv (f_dwf_base.C:232-270), which
+      // builds a DiracOpDwf: the zMobius multishift is DiracOp::MInvCG on a
+      // DiracOpZMobius, called here as FmatEvlMInv calls it.
+      DiracOpZMobius d(lat, sol[0], in, argp[0], CNV_FRM_NO);
+      const Float dot = in->NormSqGlbSum(fsz);
+      iters = d.MInvCG(sol.data(), in, dot, par + 8, nshift, 0, rsd.data(), type == 1 ? SINGLE : MULTI,
+                       alpha.data());
+      for (int s = 0; s < nshift; s++) args[s].true_rsd = rsd[s];
+    } else {
+      iters = lat.FmatEvlMInv(sol.data(), in, par + 8, nshift, 0, argp.data(), CNV_FRM_NO,
+                              type == 1 ? SINGLE : MULTI, alpha.data());
+    }
     rpar[10 + 32] = now_s() - t0;
     rhdr[0] = iters;
     for (int s = 0; s < nshift; s++) rpar[s] = args[s].true_rsd;

@@ -198,12 +198,13 @@ def main():
     main_minresext()
     main_pc()
     main_dminus()
+    main_zmobius()
 
 
 # Mobius with the non-default preconditioners ZMOB_PC_ORIG (0) and ZMOB_PC_SYM1 (1)
 PC_CASES = [
     ("mobius_orig_4x4x4x4_ls4", "mobius", (4, 4, 4, 4), 4, 0.2, 35, 0.05, {"m5": 1.8, "b": 1.5, "c": 0.5, "pc_type": 0}),
-    ("mobius_sym1_4x4x4x4_ls6", "mobius", (4, 4, 4, 4), 6, 0.2, 36, 0.03, {"m5": 1.8, "b": 2.0, "c": 1.0, "pc_type": 1}),
+    ("mobius_sym1_4x4x4x4_ls8", "mobius", (4, 4, 4, 4), 8, 0.2, 36, 0.03, {"m5": 1.8, "b": 2.0, "c": 1.0, "pc_type": 1}),
 ]
 
 
@@ -216,8 +217,56 @@ def main_pc():
         print("wrote", case[0], "and matinv_" + case[0])
 
 
+# zMobius (complex per-slice b_s, c_s: b_s = b + 0.3 z, c_s = c + 0.2 z' with
+# complex Gaussian z, z' from the case seed), SYM2
+ZMOBIUS_CASES = [("zmobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 37, 0.04, 1.5, 0.5)]
+
+
+def zmobius_coefficients(ls, seed, b, c):
+    rng = np.random.default_rng(seed + 900)
+    zb = b + 0.3 * (rng.standard_normal(ls) + 1j * rng.standard_normal(ls))
+    zc = c + 0.2 * (rng.standard_normal(ls) + 1j * rng.standard_normal(ls))
+    return zb, zc
+
+
+def gen_zmobius(name, dims, ls, eps, seed, mass, b, c):
+    """DiracOpZMobius MatPc / MatPcDag / MatPcDagMatPc, InvCg, FmatEvlMInv and the
+    zmobius_m5inv / zmobius_dslash_4 kernels on complex coefficients."""
+    u = fields.random_gauge(dims, eps, seed)
+    src = fields.random_source(int(np.prod(dims)) // 2 * ls, seed)
+    zb, zc = zmobius_coefficients(ls, seed, b, c)
+    kw = dict(ls=ls, mass=mass, m5=1.8, b=b, c=c, zb=zb, zc=zc, threads=1)
+    rec = {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
+           "mass": mass, "m5": 1.8, "zb": zb, "zc": zc}
+    for dag in (0, 1):
+        _, _, rec[f"matpc_dag{dag}"] = refrun.run(refrun.OP_MATPC, "zmobius", dims, u, [src], dag=dag, **kw)
+        _, _, rec[f"m5inv_dag{dag}"] = refrun.run(refrun.OP_M5INV, "zmobius", dims, u, [src], dag=dag, **kw)
+    for cb, dag in [(1, 0), (0, 1)]:
+        _, _, rec[f"d4_cb{cb}_dag{dag}"] = refrun.run(refrun.OP_MOBIUS_D4, "zmobius", dims, u, [src], cb=cb,
+                                                      dag=dag, **kw)
+    _, rp, rec["mdagm"] = refrun.run(refrun.OP_MDAGM, "zmobius", dims, u, [src], **kw)
+    rec["mdagm_dot"] = rp[0]
+    it, rp, rec["cg_sol"] = refrun.run(refrun.OP_INVCG, "zmobius", dims, u, [src, np.zeros_like(src)],
+                                       stop_rsd=1e-10, max_iter=5000, **kw)
+    rec["cg_iters"], rec["cg_true_res"] = it, rp[0]
+    ns = 2
+    it, rp, r = refrun.run(refrun.OP_MINVCG, "zmobius", dims, u, [src], shifts=SHIFTS[:ns],
+                           extra=[np.full(ns, 1e-9), np.ones(ns)], max_iter=5000, **kw)
+    rec["minvcg_shifts"] = np.array(SHIFTS[:ns])
+    rec["minvcg_sol"] = r.reshape(ns, -1)
+    rec["minvcg_iters"] = it
+    rec["minvcg_rsd"] = rp[:ns].copy()
+    return rec
+
+
+def main_zmobius():
+    for case in ZMOBIUS_CASES:
+        np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **gen_zmobius(*case))
+        print("wrote", case[0])
+
+
 DMINUS_CASES = [("mobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 31, 0.05, 1.5, 0.5),
-                ("mobius_b2c1_4x4x4x4_ls6", (4, 4, 4, 4), 6, 0.2, 33, 0.02, 2.0, 1.0)]
+                ("mobius_b2c1_4x4x4x4_ls8", (4, 4, 4, 4), 8, 0.2, 33, 0.02, 2.0, 1.0)]
 
 
 def gen_dminus(name, dims, ls, eps, seed, mass, b, c):
@@ -266,5 +315,7 @@ if __name__ == "__main__":
         main_dminus()
     elif "--pc" in sys.argv:
         main_pc()
+    elif "--zmobius" in sys.argv:
+        main_zmobius()
     else:
         main()

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 OP_TOL = 1e-13
 CASES = [("wilson_4x4x4x4", "wilson"), ("dwf_4x4x4x4_ls4", "dwf"), ("mobius_4x4x4x4_ls4", "mobius")]
 # Mobius with the ZMOB_PC_ORIG and ZMOB_PC_SYM1 preconditioners
-PC_CASES = [("mobius_orig_4x4x4x4_ls4", "mobius"), ("mobius_sym1_4x4x4x4_ls6", "mobius")]
+PC_CASES = [("mobius_orig_4x4x4x4_ls4", "mobius"), ("mobius_sym1_4x4x4x4_ls8", "mobius")]
 
 
 def device_op(rec, u, action):
@@ -209,7 +209,7 @@ def test_matinv_vs_reference(name, action, prec):
     assert rel(out, rec["matinv_sol"]) < (1e-9 if prec == "F64" else 1e-8)
 
 
-@pytest.mark.parametrize("name", ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls6"])
+@pytest.mark.parametrize("name", ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls8"])
 @pytest.mark.parametrize("prec", ["F64", "F32"])
 def test_dminus_fmatinv_vs_reference(name, prec):
     """DiracOpMobius::Dminus on the device against the compiled CPS (FP64, within
@@ -239,3 +239,74 @@ def test_fmatinv_dminus_ignored_outside_mobius():
     np.testing.assert_array_equal(a, b)
     with pytest.raises(Exception):
         op.Dminus(src)
+
+
+def zmobius_op(rec, u):
+    import cps_public_b200 as cb
+    cb.init(0)
+    g = cb.Gauge(u, tuple(int(d) for d in rec["dims"]))
+    return cb.DiracOp(g, "zmobius", mass=float(rec["mass"]), ls=int(rec["ls"]), m5=float(rec["m5"]),
+                      bs=list(rec["zb"]), cs=list(rec["zc"]))
+
+
+def test_zmobius_operators_vs_reference():
+    """zMobius (complex b_s, c_s; SYM2) MatPc, MatPcDag and MatPcDagMatPc on the
+    device against the compiled CPS DiracOpZMobius, FP64, within 1e-13."""
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    assert rel(op.MatPc(src), rec["matpc_dag0"]) < OP_TOL
+    assert rel(op.MatPcDag(src), rec["matpc_dag1"]) < OP_TOL
+    out, dot = op.MatPcDagMatPc(src)
+    assert rel(out, rec["mdagm"]) < OP_TOL
+    assert abs(dot - float(rec["mdagm_dot"])) < OP_TOL * abs(float(rec["mdagm_dot"]))
+
+
+@pytest.mark.parametrize("prec", ["F64", "F32"])
+def test_zmobius_cg_vs_reference(prec):
+    """zMobius CG: FP64 follows CPS's InvCg (iterations within 1, solution within
+    1e-9); mixed FP32 reaches the FP64 true residual 1e-10 (solution within 1e-8)."""
+    import cps_public_b200 as cb
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    x, r = op.InvCg(src, stop_rsd=1e-10, max_num_iter=5000, precision=getattr(cb, prec))
+    assert r.status == 0 and r.true_rsd <= 1e-10, r.as_dict()
+    if prec == "F64":
+        assert abs(r.iters - int(rec["cg_iters"])) <= 1
+        assert rel(x, rec["cg_sol"]) < 1e-9
+    else:
+        assert rel(x, rec["cg_sol"]) < 1e-8
+
+
+def test_zmobius_minvcg_vs_reference():
+    """zMobius FmatEvlMInv (MULTI) on the device against the compiled CPS."""
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    shifts = list(rec["minvcg_shifts"])
+    xs, r, rsd = op.MInvCG(src, shifts, [1e-9] * len(shifts))
+    assert abs(r.iters - int(rec["minvcg_iters"])) <= 1
+    for i in range(len(shifts)):
+        assert rel(xs[i], rec["minvcg_sol"][i]) < 1e-9
+
+
+def test_zmobius_constant_coefficients_equal_mobius():
+    """zMobius with b_s = b, c_s = c is Mobius: both device paths agree."""
+    import cps_public_b200 as cb
+    rec, u, src = load("mobius_4x4x4x4_ls4")
+    m = device_op(rec, u, "mobius")
+    ls = int(rec["ls"])
+    z = cb.DiracOp(m.gauge, "zmobius", mass=float(rec["mass"]), ls=ls, m5=float(rec["m5"]),
+                   bs=[complex(float(rec["b"]))] * ls, cs=[complex(float(rec["c"]))] * ls)
+    a, da = m.MatPcDagMatPc(src)
+    b, db = z.MatPcDagMatPc(src)
+    assert rel(b, a) < 1e-13 and abs(db - da) < 1e-13 * da
+
+
+def test_zmobius_unsupported_forms_refused():
+    """DiracOpZMobius::Dslash (unpreconditioned, full vectors) and MatInv are not
+    built on the device: the ABI says so instead of computing something else."""
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    with pytest.raises(Exception, match="unsupported"):
+        op.Dslash(src, 0, 0)
+    with pytest.raises(Exception, match="unsupported"):
+        op.MatInv(np.concatenate([src, src]))

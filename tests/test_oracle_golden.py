@@ -10,7 +10,7 @@ from tests.golden_util import load
 CASES = ["wilson_4x4x4x4", "dwf_4x4x4x4_ls4", "mobius_4x4x4x4_ls4"]
 # Mobius with ZMOB_PC_ORIG and ZMOB_PC_SYM1 (no hop fixtures: the hop does not
 # depend on the preconditioner)
-PC_CASES = ["mobius_orig_4x4x4x4_ls4", "mobius_sym1_4x4x4x4_ls6"]
+PC_CASES = ["mobius_orig_4x4x4x4_ls4", "mobius_sym1_4x4x4x4_ls8"]
 
 
 def make_op(rec, u, action):
@@ -96,7 +96,7 @@ def test_matinv_bitexact(name):
     assert tr == float(rec["matinv_true_res"])
 
 
-DMINUS_CASES = ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls6"]
+DMINUS_CASES = ["mobius_4x4x4x4_ls4", "mobius_b2c1_4x4x4x4_ls8"]
 
 
 @pytest.mark.parametrize("name", DMINUS_CASES)
@@ -145,3 +145,28 @@ def test_minresext_bitexact(name):
     psi, v, vm, err = op.minresext(phi, prev)
     np.testing.assert_array_equal(psi, rec["psi"])
     assert sha(np.concatenate(v)) == str(rec["v_sha"]) and sha(np.concatenate(vm)) == str(rec["vm_sha"])
+
+
+def test_zmobius_bitexact():
+    """zMobius with complex per-slice b_s, c_s (DiracOpZMobius, SYM2): the
+    zmobius_m5inv / zmobius_dslash_4 kernels, MatPc, MatPcDag, MatPcDagMatPc,
+    InvCg and FmatEvlMInv against the compiled reference."""
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = oracle.Op("mobius", tuple(rec["dims"]), u, ls=int(rec["ls"]), mass=float(rec["mass"]),
+                   m5=float(rec["m5"]), bs=list(rec["zb"]), cs=list(rec["zc"]))
+    for dag in (0, 1):
+        np.testing.assert_array_equal(op.m5inv(src, dag), rec[f"m5inv_dag{dag}"])
+        np.testing.assert_array_equal(op.matpc(src, dag), rec[f"matpc_dag{dag}"])
+    for cb, dag in [(1, 0), (0, 1)]:
+        np.testing.assert_array_equal(op.mobius_d4(src, cb, dag), rec[f"d4_cb{cb}_dag{dag}"])
+    out, dot = op.mdagm(src)
+    np.testing.assert_array_equal(out, rec["mdagm"])
+    assert dot == float(rec["mdagm_dot"])
+    sol, it, tr = op.invcg(src, 1e-10, 5000)
+    assert it == int(rec["cg_iters"]) and tr == float(rec["cg_true_res"])
+    np.testing.assert_array_equal(sol, rec["cg_sol"])
+    shifts = list(rec["minvcg_shifts"])
+    sols, it, rsd = op.minvcg(src, shifts, [1e-9] * len(shifts))
+    assert it == int(rec["minvcg_iters"])
+    for i in range(len(shifts)):
+        np.testing.assert_array_equal(sols[i], rec["minvcg_sol"][i])
