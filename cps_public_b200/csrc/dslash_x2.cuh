@@ -835,6 +835,9 @@ template <int P, int NT, int MINB, int SL, int DEPTH, int WG>
 static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
   if (A.cg) {  // fused residual update: xpay hop whose output feeds r -= alpha Ap
     if (!xpay) return cudaErrorInvalidValue;
+    // The update epilogue needs more registers than the plain hop: above 4
+    // blocks/SM (<= 128 registers) it spills, so those shapes run it at 4.
+    constexpr int MB = MINB > 4 ? 4 : MINB;
     constexpr int TX = NT / SL;
     const long units = (long)((A.g.n4cb + TX - 1) / TX) * (A.five_d ? 2 : 1);
     const long nb = units < 148L * 16 ? units : 148L * 16;
@@ -842,12 +845,12 @@ static cudaError_t launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
     if (shm > 200 * 1024) return cudaErrorNotSupported;
     static bool attr = false;
     if (shm + 1024 > 48 * 1024 && !attr) {
-      const cudaError_t e = cudaFuncSetAttribute((const void *)kernel<P, NT, MINB, SL, DEPTH, WG, true, false, true>,
+      const cudaError_t e = cudaFuncSetAttribute((const void *)kernel<P, NT, MB, SL, DEPTH, WG, true, false, true>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       if (e != cudaSuccess) return e;
       attr = true;
     }
-    kernel<P, NT, MINB, SL, DEPTH, WG, true, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
+    kernel<P, NT, MB, SL, DEPTH, WG, true, false, true><<<(unsigned)nb, NT, shm, st>>>(A);
     return launched();
   }
   constexpr int TX = NT / SL;

@@ -95,8 +95,8 @@ struct Operator {
   double kappa_b = 0;      // Mobius
   M5Coef m5c[2];           // Mobius M5^-1 coefficient sets (dag 0, dag 1)
   // zMobius: the per-slice coefficients (copied from the parameters) and the
-  // four m5z tables of MatPc (dag 0: kb and -kb stages; dag 1: the scaled and
-  // the xpay stage), in device memory
+  // m5z tables of the MatPc / MatPcDag stages of the three preconditioners, in
+  // device memory
   std::vector<std::complex<double>> zb, zc;
   DevBuf ztab;
   Field t1, t2, t3;

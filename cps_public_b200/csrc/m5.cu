@@ -306,7 +306,8 @@ static cudaError_t m5z_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPt
     m5z_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, tab, red, skip);           \
     return launched();                                                                              \
   }
-  M5ZL(0, false, false) M5ZL(1, false, false) M5ZL(1, true, false) M5ZL(1, true, true)
+  M5ZL(0, false, false) M5ZL(0, true, false) M5ZL(0, true, true)
+  M5ZL(1, false, false) M5ZL(1, true, false) M5ZL(1, true, true)
 #undef M5ZL
   return cudaErrorInvalidValue;
 }

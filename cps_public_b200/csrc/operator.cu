@@ -239,7 +239,8 @@ static void zmobius_mix(ZM5Tab &t, int dag, int ls, double m, const zc_t *b, con
 
 static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   const int ls = op.geom.ls;
-  if (pp.pc_type != 2) throw Error{CPSB_ERR_UNSUPPORTED, "zMobius: only the ZMOB_PC_SYM2 preconditioner is implemented"};
+  if (pp.pc_type < 0 || pp.pc_type > 2)
+    throw Error{CPSB_ERR_UNSUPPORTED, "zMobius preconditioners: ZMOB_PC_ORIG (0), ZMOB_PC_SYM1 (1), ZMOB_PC_SYM2 (2)"};
   if (!pp.zmobius_b || !pp.zmobius_c) throw Error{CPSB_ERR_ARG, "zMobius needs zmobius_b and zmobius_c"};
   op.zb.resize(ls);
   op.zc.resize(ls);
@@ -251,23 +252,33 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
     const zc_t kc = 1.0 / (2.0 * (op.zc[s] * (4 - pp.m5) - pp.a5_inv));
     K[s] = kb[s] / kc;
   }
-  std::vector<ZM5Tab> t(4);
-  memset(t.data(), 0, sizeof(ZM5Tab) * 4);
-  for (int k = 0; k < 4; k++) {
-    const int dag = k >= 2;
-    zmobius_sweeps(t[k], dag, ls, pp.mass, K.data());
-    zmobius_mix(t[k], dag, ls, pp.mass, op.zb.data(), op.zc.data());
+  // Tables (the stage each one applies; kb, K per slice):
+  //   0 dag0 kb . mix(M5^-1 .)        1 dag0 -kb . mix(M5^-1 .)     4 dag0 kb . mix(.)
+  //   5 dag0 K-weighted H5 (b = 0)    6 dag0 M5^-1 alone
+  //   2 dag1 conj(kb) . M5^-dag(mix^dag(-conj(kb) .))              3 dag1 M5^-dag(mix^dag(.))
+  //   7 dag1 mix^dag alone            8 dag1 K-weighted H5^dag       9 dag1 -conj(kb) . M5^-dag(.)
+  //  10 dag1 conj(kb) . M5^-dag(mix^dag(.))
+  const int NT = 11;
+  std::vector<ZM5Tab> t(NT);
+  memset(t.data(), 0, sizeof(ZM5Tab) * NT);
+  const std::vector<zc_t> zero(ls, zc_t(0.0, 0.0));
+  auto dag_of = [](int k) { return (k == 0 || k == 1 || k == 4 || k == 5 || k == 6) ? 0 : 1; };
+  for (int k = 0; k < NT; k++) {
+    const int dag = dag_of(k);
+    if (k != 4 && k != 5 && k != 7 && k != 8) zmobius_sweeps(t[k], dag, ls, pp.mass, K.data());
+    if (k == 5 || k == 8) zmobius_mix(t[k], dag, ls, pp.mass, zero.data(), K.data());
+    else if (k != 6 && k != 9) zmobius_mix(t[k], dag, ls, pp.mass, op.zb.data(), op.zc.data());
   }
   for (int s = 0; s < ls; s++) {
-    t[0].post[s] = d2(kb[s]);
+    t[0].post[s] = t[4].post[s] = d2(kb[s]);
     t[1].post[s] = d2(-kb[s]);
-    t[2].pre[s] = d2(-std::conj(kb[s]));
-    t[2].post[s] = d2(std::conj(kb[s]));
+    t[2].pre[s] = t[9].post[s] = d2(-std::conj(kb[s]));
+    t[2].post[s] = t[10].post[s] = d2(std::conj(kb[s]));
   }
-  t[0].post_on = t[1].post_on = 1;
+  t[0].post_on = t[1].post_on = t[4].post_on = t[9].post_on = t[10].post_on = 1;
   t[2].pre_on = t[2].post_on = 1;
-  op.ztab.alloc(sizeof(ZM5Tab) * 4);
-  CK(cudaMemcpy(op.ztab.p, t.data(), sizeof(ZM5Tab) * 4, cudaMemcpyHostToDevice));
+  op.ztab.alloc(sizeof(ZM5Tab) * NT);
+  CK(cudaMemcpy(op.ztab.p, t.data(), sizeof(ZM5Tab) * NT, cudaMemcpyHostToDevice));
   op.kappa_b = kb[0].real();
 }
 
@@ -482,16 +493,44 @@ void Operator::matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag,
   Reduce none;
   memset(&none, 0, sizeof(none));
   const ZM5Tab *t = (const ZM5Tab *)ztab.p;
+  const Reduce rd = red ? *red : none;
+  const int nr = red != nullptr;
+  const int pc = p.pc_type;
   if (!dag) {
-    CK(launch_m5z(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, t + 0, 0, 0, none, skip, st));
+    // SYM2 (zmobius_m-sym2.h): in - kb D4(0) M5^-1 kb D4(1) M5^-1 in
+    // ORIG (zmobius_m-orig.h): in - kb D4(0) M5^-1 kb D4(1) in + K H5 in
+    // SYM1 (zmobius_m-sym1.h): in - M5^-1 kb D4(0) M5^-1 kb D4(1) in
+    CK(launch_m5z(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, t + (pc == 2 ? 0 : 4), 0, 0, none, skip, st));
     hop(t3.ptr(), t1.ptr(), 1, 0, 1.0, nullptr, nullptr, skip, st);
     CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 1, 0, 0, none, skip, st));
-    hop(out, t1.ptr(), 0, 0, 1.0, &in, red, skip, st);
+    if (pc == 2) {
+      hop(out, t1.ptr(), 0, 0, 1.0, &in, red, skip, st);
+    } else if (pc == 0) {
+      hop(out, t1.ptr(), 0, 0, 1.0, &in, nullptr, skip, st);
+      CK(launch_m5z(prec, 0, geom, out, in, out, t + 5, 1, nr, rd, skip, st));
+    } else {
+      hop(t3.ptr(), t1.ptr(), 0, 0, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 0, geom, out, t3.ptr(), in, t + 6, 1, nr, rd, skip, st));
+    }
   } else {
-    hop(t1.ptr(), in, 1, 1, 1.0, nullptr, nullptr, skip, st);
-    CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 2, 0, 0, none, skip, st));
+    // the adjoints (zmobius_mdag-sym2.h, -orig.h, -sym1.h)
+    if (pc == 1) {
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), in, SpinorPtr{}, t + 9, 0, 0, none, skip, st));
+      hop(t1.ptr(), t3.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 10, 0, 0, none, skip, st));
+    } else {
+      hop(t1.ptr(), in, 1, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 2, 0, 0, none, skip, st));
+    }
     hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
-    CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 3, 1, red != nullptr, red ? *red : none, skip, st));
+    if (pc == 2) {
+      CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 3, 1, nr, rd, skip, st));
+    } else if (pc == 0) {
+      CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 7, 1, 0, none, skip, st));
+      CK(launch_m5z(prec, 1, geom, out, in, out, t + 8, 1, nr, rd, skip, st));
+    } else {
+      CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 7, 1, nr, rd, skip, st));
+    }
   }
 }
 

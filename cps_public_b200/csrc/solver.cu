@@ -220,7 +220,12 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   // the state the previous solve left behind.
   *hstate = hs;
 
-  int batch = a.batch > 0 ? a.batch : 16;
+  // Iterations per graph launch.  The host looks at the state between
+  // launches, so a right-hand side that pauses for a reliable update idles
+  // until its launch ends; with many right-hand sides an iteration is long
+  // (milliseconds) and a host round trip every couple of iterations costs
+  // little, so the batch shrinks as the right-hand sides grow.
+  int batch = a.batch > 0 ? a.batch : (nrhs >= 8 ? 2 : nrhs >= 2 ? 4 : 16);
   int status = CPSB_OK;
   for (;;) {
     bool all = true;

@@ -219,7 +219,9 @@ def main_pc():
 
 # zMobius (complex per-slice b_s, c_s: b_s = b + 0.3 z, c_s = c + 0.2 z' with
 # complex Gaussian z, z' from the case seed), SYM2
-ZMOBIUS_CASES = [("zmobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 37, 0.04, 1.5, 0.5)]
+ZMOBIUS_CASES = [("zmobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 37, 0.04, 1.5, 0.5),
+                 ("zmobius_orig_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 38, 0.04, 1.5, 0.5, 0),
+                 ("zmobius_sym1_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 39, 0.04, 1.5, 0.5, 1)]
 
 
 def zmobius_coefficients(ls, seed, b, c):
@@ -229,19 +231,20 @@ def zmobius_coefficients(ls, seed, b, c):
     return zb, zc
 
 
-def gen_zmobius(name, dims, ls, eps, seed, mass, b, c):
-    """DiracOpZMobius MatPc / MatPcDag / MatPcDagMatPc, InvCg, FmatEvlMInv and the
-    zmobius_m5inv / zmobius_dslash_4 kernels on complex coefficients."""
+def gen_zmobius(name, dims, ls, eps, seed, mass, b, c, pc_type=2):
+    """DiracOpZMobius MatPc / MatPcDag / MatPcDagMatPc, InvCg, FmatEvlMInv and (for
+    SYM2) the zmobius_m5inv / zmobius_dslash_4 kernels on complex coefficients."""
     u = fields.random_gauge(dims, eps, seed)
     src = fields.random_source(int(np.prod(dims)) // 2 * ls, seed)
     zb, zc = zmobius_coefficients(ls, seed, b, c)
-    kw = dict(ls=ls, mass=mass, m5=1.8, b=b, c=c, zb=zb, zc=zc, threads=1)
+    kw = dict(ls=ls, mass=mass, m5=1.8, b=b, c=c, zb=zb, zc=zc, pc_type=pc_type, threads=1)
     rec = {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
-           "mass": mass, "m5": 1.8, "zb": zb, "zc": zc}
+           "mass": mass, "m5": 1.8, "zb": zb, "zc": zc, "pc_type": pc_type}
     for dag in (0, 1):
         _, _, rec[f"matpc_dag{dag}"] = refrun.run(refrun.OP_MATPC, "zmobius", dims, u, [src], dag=dag, **kw)
-        _, _, rec[f"m5inv_dag{dag}"] = refrun.run(refrun.OP_M5INV, "zmobius", dims, u, [src], dag=dag, **kw)
-    for cb, dag in [(1, 0), (0, 1)]:
+        if pc_type == 2:
+            _, _, rec[f"m5inv_dag{dag}"] = refrun.run(refrun.OP_M5INV, "zmobius", dims, u, [src], dag=dag, **kw)
+    for cb, dag in ([(1, 0), (0, 1)] if pc_type == 2 else []):
         _, _, rec[f"d4_cb{cb}_dag{dag}"] = refrun.run(refrun.OP_MOBIUS_D4, "zmobius", dims, u, [src], cb=cb,
                                                       dag=dag, **kw)
     _, rp, rec["mdagm"] = refrun.run(refrun.OP_MDAGM, "zmobius", dims, u, [src], **kw)

@@ -241,18 +241,23 @@ def test_fmatinv_dminus_ignored_outside_mobius():
         op.Dminus(src)
 
 
+ZMOBIUS_CASES = ["zmobius_4x4x4x4_ls4", "zmobius_orig_4x4x4x4_ls4", "zmobius_sym1_4x4x4x4_ls4"]
+
+
 def zmobius_op(rec, u):
     import cps_public_b200 as cb
     cb.init(0)
     g = cb.Gauge(u, tuple(int(d) for d in rec["dims"]))
     return cb.DiracOp(g, "zmobius", mass=float(rec["mass"]), ls=int(rec["ls"]), m5=float(rec["m5"]),
-                      bs=list(rec["zb"]), cs=list(rec["zc"]))
+                      bs=list(rec["zb"]), cs=list(rec["zc"]), pc_type=int(rec.get("pc_type", 2)))
 
 
-def test_zmobius_operators_vs_reference():
-    """zMobius (complex b_s, c_s; SYM2) MatPc, MatPcDag and MatPcDagMatPc on the
-    device against the compiled CPS DiracOpZMobius, FP64, within 1e-13."""
-    rec, u, src = load("zmobius_4x4x4x4_ls4")
+@pytest.mark.parametrize("name", ZMOBIUS_CASES)
+def test_zmobius_operators_vs_reference(name):
+    """zMobius (complex b_s, c_s; SYM2, ORIG, SYM1) MatPc, MatPcDag and
+    MatPcDagMatPc on the device against the compiled CPS DiracOpZMobius, FP64,
+    within 1e-13."""
+    rec, u, src = load(name)
     op = zmobius_op(rec, u)
     assert rel(op.MatPc(src), rec["matpc_dag0"]) < OP_TOL
     assert rel(op.MatPcDag(src), rec["matpc_dag1"]) < OP_TOL
@@ -261,12 +266,13 @@ def test_zmobius_operators_vs_reference():
     assert abs(dot - float(rec["mdagm_dot"])) < OP_TOL * abs(float(rec["mdagm_dot"]))
 
 
+@pytest.mark.parametrize("name", ZMOBIUS_CASES)
 @pytest.mark.parametrize("prec", ["F64", "F32"])
-def test_zmobius_cg_vs_reference(prec):
+def test_zmobius_cg_vs_reference(name, prec):
     """zMobius CG: FP64 follows CPS's InvCg (iterations within 1, solution within
     1e-9); mixed FP32 reaches the FP64 true residual 1e-10 (solution within 1e-8)."""
     import cps_public_b200 as cb
-    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    rec, u, src = load(name)
     op = zmobius_op(rec, u)
     x, r = op.InvCg(src, stop_rsd=1e-10, max_num_iter=5000, precision=getattr(cb, prec))
     assert r.status == 0 and r.true_rsd <= 1e-10, r.as_dict()
@@ -277,9 +283,11 @@ def test_zmobius_cg_vs_reference(prec):
         assert rel(x, rec["cg_sol"]) < 1e-8
 
 
-def test_zmobius_minvcg_vs_reference():
-    """zMobius FmatEvlMInv (MULTI) on the device against the compiled CPS."""
-    rec, u, src = load("zmobius_4x4x4x4_ls4")
+@pytest.mark.parametrize("name", ZMOBIUS_CASES)
+def test_zmobius_minvcg_vs_reference(name):
+    """zMobius multishift (DiracOp::MInvCG on DiracOpZMobius, MULTI) on the device
+    against the compiled CPS."""
+    rec, u, src = load(name)
     op = zmobius_op(rec, u)
     shifts = list(rec["minvcg_shifts"])
     xs, r, rsd = op.MInvCG(src, shifts, [1e-9] * len(shifts))
