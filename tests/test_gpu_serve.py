@@ -121,3 +121,24 @@ def test_multishift_requests_overlap_and_match(setup):
             np.testing.assert_array_equal(rsa, rsm)
             for k in range(len(shifts)):
                 np.testing.assert_array_equal(xa[k], xm[k])
+
+
+def test_zmobius_request_owns_coefficients(setup):
+    """A zMobius request copies its complex b_s, c_s at submission: clearing the
+    caller's arrays afterwards does not change the solve, which equals InvCg."""
+    cb, gauges, _ = setup
+    from cps_public_b200 import fields
+    ls = 4
+    zb = [1.5 + 0.1j * (s - 1.5) for s in range(ls)]
+    zc = [0.5 - 0.05j * s for s in range(ls)]
+    op = cb.DiracOp(gauges[0], "zmobius", mass=0.05, ls=ls, m5=1.8, bs=zb, cs=zc)
+    src = fields.random_source(op.n // 24, 4242)
+    x_ref, r_ref = op.InvCg(src, stop_rsd=1e-10)
+    srv = cb.Server(slots=2)
+    rid = srv.submit(op, [src], stop_rsd=1e-10, precision=cb.F64)
+    op._zb[:] = 0.0
+    op._zc[:] = 0.0
+    xs, res, _ = srv.wait(rid)
+    srv.close()
+    assert res[0].status == 0 and res[0].iters == r_ref.iters
+    np.testing.assert_array_equal(xs[0], x_ref)
