@@ -12,6 +12,12 @@
 //
 //   dag 0:  out = scale * mix(M5^-1 in)                 (precedes D_W in MatPc)
 //   dag 1:  out = [x +] scale * M5^-dag(mix^dag(in))    (follows D_W^dag in MatPcDag)
+//
+// 16-bit storage: a chunk is one (chirality pair, colour) of both spins, half
+// of a stored uint4 -- the same values as an FP32 chunk -- so the column
+// arithmetic is shared.  The site's quantum is the maximum over its six
+// chunks, so a site's chunks sit in one 8-lane group of a warp (two lanes
+// idle) and the group agrees on the maximum by shuffles before encoding.
 #include "blas.h"
 
 namespace cpsb {
@@ -19,6 +25,7 @@ namespace cpsb {
 template <int P> struct ChunkT;
 template <> struct ChunkT<P64> { static const int NCH = 12, NC = 1; typedef double T; };
 template <> struct ChunkT<P32> { static const int NCH = 6, NC = 2; typedef float T; };
+template <> struct ChunkT<P16> { static const int NCH = 6, NC = 2; typedef float T; };
 
 template <int P>
 __device__ __forceinline__ void ld_chunk(const SpinorPtr &f, long i, int k, cplx<typename ChunkT<P>::T> *v);
@@ -33,6 +40,14 @@ __device__ __forceinline__ void ld_chunk<P32>(const SpinorPtr &f, long i, int k,
   v[0] = mk(a.x, a.z);
   v[1] = mk(a.y, a.w);
 }
+// chunk j = 3p + c: words 2j (Re) and 2j+1 (Im) of the site, both spins each
+template <>
+__device__ __forceinline__ void ld_chunk<P16>(const SpinorPtr &f, long i, int j, cplx<float> *v) {
+  const uint2 w = __ldg((const uint2 *)((const uint4 *)f.data + (long)(j >> 1) * f.stride + i) + (j & 1));
+  const float q = __ldg(f.norm + i);
+  v[0] = mk(dec16(w.x, 0) * q, dec16(w.y, 0) * q);
+  v[1] = mk(dec16(w.x, 1) * q, dec16(w.y, 1) * q);
+}
 template <int P>
 __device__ __forceinline__ void st_chunk(const SpinorPtr &f, long i, int k, const cplx<typename ChunkT<P>::T> *v);
 template <>
@@ -42,6 +57,29 @@ __device__ __forceinline__ void st_chunk<P64>(const SpinorPtr &f, long i, int k,
 template <>
 __device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k, const cplx<float> *v) {
   ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[1].re, v[0].im, v[1].im);
+}
+// 16-bit store of chunk j of site i from lane j of the site's 8-lane group
+// (every lane of the warp calls it; lanes with active = false only take part
+// in the maximum).  Returns |stored values|^2 of this lane (the rounded
+// values a later load returns), encoded as store_spinor<P16> encodes them.
+__device__ __forceinline__ float st_chunk16(const SpinorPtr &f, long i, int j, const cplx<float> *v, bool active) {
+  float m = active ? fmaxf(fmaxf(fabsf(v[0].re), fabsf(v[0].im)), fmaxf(fabsf(v[1].re), fabsf(v[1].im))) : 0.f;
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
+  if (!active) return 0.f;
+  const float scale = m > 0.f ? 32767.0f / m : 0.f;
+  const float nq = m * (1.0f / 32767.0f);
+  const unsigned wx = enc16x2(v[0].re, v[1].re, scale), wy = enc16x2(v[0].im, v[1].im, scale);
+  ((uint2 *)((uint4 *)f.data + (long)(j >> 1) * f.stride + i))[j & 1] = make_uint2(wx, wy);
+  if (j == 0) f.norm[i] = nq;
+  float n = 0.f;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const float a = dec16(wx, h) * nq, b = dec16(wy, h) * nq;
+    n += a * a + b * b;
+  }
+  return n;
 }
 
 // v[s] += f * w[s] on one chunk
@@ -56,6 +94,80 @@ __device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k,
     (dst)[q].im *= (f);                                      \
   }
 
+// y = mix(M5^-1 v) (DAG 0) or M5^-dag(mix^dag(v)) (DAG 1) on one column, real
+// coefficients; the output scale is applied by the caller.
+template <int LS, int DAG, int NC, typename T>
+__device__ __forceinline__ void m5_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS][NC], bool upper, const M5Coef &cf) {
+  const T K = (T)cf.K, b = (T)cf.b, c = (T)cf.c, mwall = (T)(-cf.mass * cf.c), invd = (T)cf.invd;
+  if (DAG == 1) {
+    // mix^dag: upper from s+1, lower from s-1
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
+      if (upper) {
+        if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
+      } else {
+        if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < LS; s++)
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
+  }
+  // M5^-1 (DAG 0) or M5^-dag (DAG 1) sweeps.  The structure of the
+  // dag-0 lower sweep equals the dag-1 upper sweep and vice versa.
+  const bool walls_first = (DAG == 0) ? !upper : upper;
+  if (walls_first) {
+    SCALC(v[LS - 1], invd);
+#pragma unroll
+    for (int s = 0; s <= LS - 2; s++) { const T f = (T)cf.f1[s]; AXPYC(v[LS - 1], f, v[s]); }
+#pragma unroll
+    for (int s = LS - 2; s >= 0; s--) { AXPYC(v[s], -K, v[s + 1]); }
+  } else {
+#pragma unroll
+    for (int s = 0; s <= LS - 2; s++) { AXPYC(v[s + 1], -K, v[s]); }
+#pragma unroll
+    for (int s = LS - 2; s >= 0; s--) { const T f = (T)cf.f2[s]; AXPYC(v[s], f, v[LS - 1]); }
+    SCALC(v[LS - 1], invd);
+  }
+  if (DAG == 0) {
+    // mix: upper from s-1, lower from s+1
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
+      if (upper) {
+        if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
+      } else {
+        if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < LS; s++)
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
+  }
+}
+
+// Per-RHS |out|^2 of the block into red (deterministic: partials summed in
+// block order by the last block).
+template <int NT>
+__device__ __forceinline__ void m5_norm_epilogue(double acc, const Geom &g, Reduce red, const int *skip, double *sh) {
+  const int rhs = blockIdx.y;
+  double bs = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bs;
+  if (last_block(red.ticket, gridDim.x * gridDim.y)) {
+    for (int q = 0; q < g.nrhs; q++) {
+      double t = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
+      if (threadIdx.x == 0 && !(skip && skip[q])) red.result[q] = t;
+      __syncthreads();
+    }
+  }
+}
+
 template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
 __global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
                                                 Reduce red, const int *skip) {
@@ -66,67 +178,16 @@ __global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr
   const long per = (long)g.n4cb * LS;
   const long work = (long)g.n4cb * NCH;
   double acc = 0;
-  const T K = (T)cf.K, b = (T)cf.b, c = (T)cf.c, mwall = (T)(-cf.mass * cf.c), sc = (T)cf.scale, invd = (T)cf.invd;
+  const T sc = (T)cf.scale;
   const bool sk = skip && skip[rhs];
   for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
     const int x = (int)(w % g.n4cb);
     const int k = (int)(w / g.n4cb);
-    const bool upper = (k < NCH / 2);
     const long base = rhs * per + x;
     cplx<T> v[LS][NC], y[LS][NC];
 #pragma unroll
     for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    if (DAG == 1) {
-      // mix^dag: upper from s+1, lower from s-1
-#pragma unroll
-      for (int s = 0; s < LS; s++) {
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
-        if (upper) {
-          if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
-        } else {
-          if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
-        }
-      }
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
-    }
-    // M5^-1 (DAG 0) or M5^-dag (DAG 1) sweeps.  The structure of the
-    // dag-0 lower sweep equals the dag-1 upper sweep and vice versa.
-    const bool walls_first = (DAG == 0) ? !upper : upper;
-    if (walls_first) {
-      SCALC(v[LS - 1], invd);
-#pragma unroll
-      for (int s = 0; s <= LS - 2; s++) { const T f = (T)cf.f1[s]; AXPYC(v[LS - 1], f, v[s]); }
-#pragma unroll
-      for (int s = LS - 2; s >= 0; s--) { AXPYC(v[s], -K, v[s + 1]); }
-    } else {
-#pragma unroll
-      for (int s = 0; s <= LS - 2; s++) { AXPYC(v[s + 1], -K, v[s]); }
-#pragma unroll
-      for (int s = LS - 2; s >= 0; s--) { const T f = (T)cf.f2[s]; AXPYC(v[s], f, v[LS - 1]); }
-      SCALC(v[LS - 1], invd);
-    }
-    if (DAG == 0) {
-      // mix: upper from s-1, lower from s+1
-#pragma unroll
-      for (int s = 0; s < LS; s++) {
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
-        if (upper) {
-          if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
-        } else {
-          if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
-        }
-      }
-    } else {
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
-    }
+    m5_column<LS, DAG, NC, T>(v, y, k < NCH / 2, cf);
 #pragma unroll
     for (int s = 0; s < LS; s++) {
       cplx<T> o[NC];
@@ -140,33 +201,74 @@ __global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr
       st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
     }
   }
-  if (NORM) {
-    double bs = block_sum<NT>(acc, sh);
-    if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bs;
-    if (last_block(red.ticket, gridDim.x * gridDim.y)) {
-      for (int q = 0; q < g.nrhs; q++) {
-        double t = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
-        if (threadIdx.x == 0 && !(skip && skip[q])) red.result[q] = t;
-        __syncthreads();
-      }
+  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
+}
+
+// 16-bit storage: four sites per warp, 8 lanes per site (chunks 0..5, lanes
+// 6 and 7 idle); the loop is warp-uniform so every shuffle has the full warp.
+template <int LS, int DAG, bool XPAY, bool NORM, int NT>
+__global__ void __launch_bounds__(NT) m5h_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
+                                                 Reduce red, const int *skip) {
+  __shared__ double sh[NT / 32];
+  const int rhs = blockIdx.y;
+  const long per = (long)g.n4cb * LS;
+  const int lane = threadIdx.x & 31, j = lane & 7;
+  const long nw = (long)gridDim.x * (NT / 32);
+  double acc = 0;
+  const float sc = (float)cf.scale;
+  const bool sk = skip && skip[rhs];
+  for (long x0 = ((long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5)) * 4; !sk && x0 < g.n4cb; x0 += nw * 4) {
+    const long x = x0 + (lane >> 3);
+    const bool active = j < 6 && x < g.n4cb;
+    const int jj = active ? j : 0;
+    const long base = rhs * per + (active ? x : 0);
+    cplx<float> v[LS][2], y[LS][2];
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      if (active) ld_chunk<P16>(in, base + (long)s * g.n4cb, jj, v[s]);
+      else v[s][0] = v[s][1] = mk(0.f, 0.f);
+    }
+    m5_column<LS, DAG, 2, float>(v, y, jj < 3, cf);
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      cplx<float> o[2];
+      if (XPAY && active) ld_chunk<P16>(xv, base + (long)s * g.n4cb, jj, o);
+#pragma unroll
+      for (int q = 0; q < 2; q++) o[q] = (XPAY && active) ? o[q] + cscale(sc, y[s][q]) : cscale(sc, y[s][q]);
+      const float n = st_chunk16(out, base + (long)s * g.n4cb, jj, o, active);
+      if (NORM) acc += (double)n;
     }
   }
+  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
 }
 
 template <int P, int LS>
 static cudaError_t m5_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
                                 int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
   const int NT = 128;
+  if constexpr (P == P16) {
+    dim3 grid(grid_blocks((long)g.n4cb * 8, NT), g.nrhs);
+#define M5H(D, XP, NR)                                                                              \
+    if (dag == D && !!xpay == XP && !!norm == NR) {                                                 \
+      m5h_kernel<LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
+      return launched();                                                                            \
+    }
+    M5H(0, false, false) M5H(0, true, false) M5H(0, true, true) M5H(0, false, true)
+    M5H(1, false, false) M5H(1, true, false) M5H(1, true, true) M5H(1, false, true)
+#undef M5H
+    return cudaErrorInvalidValue;
+  } else {
   dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
 #define M5L(D, XP, NR)                                                                              \
   if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
     m5_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
-    return launched();                                                                      \
+    return launched();                                                                              \
   }
   M5L(0, false, false) M5L(0, true, false) M5L(0, true, true) M5L(0, false, true)
   M5L(1, false, false) M5L(1, true, false) M5L(1, true, true) M5L(1, false, true)
 #undef M5L
   return cudaErrorInvalidValue;
+  }
 }
 
 template <int P>
@@ -188,7 +290,8 @@ cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr
                       int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
   if (prec == P64) return m5_launch_p<P64>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
   if (prec == P32) return m5_launch_p<P32>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-  return cudaErrorInvalidValue;  // FP16 Mobius storage is not supported by this kernel
+  if (prec == P16) return m5_launch_p<P16>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
+  return cudaErrorInvalidValue;
 }
 
 // ----------------------------------------------------------------- zMobius
@@ -201,6 +304,65 @@ template <typename T> __device__ __forceinline__ cplx<T> ldz(const double2 *p) {
 #define ZSCALC(dst, f)                                       \
   _Pragma("unroll") for (int q = 0; q < NC; q++) (dst)[q] = cmul((f), (dst)[q]);
 
+// y = post . mix(M5^-1(pre . v)) (DAG 0) or post . M5^-dag(mix^dag(pre . v))
+// (DAG 1) on one column of chirality half h, the stages the table enables.
+template <int LS, int DAG, int NC, typename T>
+__device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS][NC], int h, const ZM5Tab *tab) {
+  const int sweep = tab->sweep, mix = tab->mix, pre_on = tab->pre_on, post_on = tab->post_on;
+  if (pre_on) {
+#pragma unroll
+    for (int s = 0; s < LS; s++) { ZSCALC(v[s], ldz<T>(&tab->pre[s])); }
+  }
+  // upper half at dag 0 and lower half at dag 1 take slice s-1, the others s+1
+  const bool from_below = (DAG == 0) == (h == 0);
+  if (DAG == 1 && mix) {
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
+      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
+    }
+#pragma unroll
+    for (int s = 0; s < LS; s++)
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
+  }
+  if (sweep) {
+    if (tab->walls_first[h]) {
+      ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
+#pragma unroll
+      for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[LS - 1], ldz<T>(&tab->w[h][s]), v[s]); }
+#pragma unroll
+      for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->a[h][s]), v[s + 1]); }
+    } else {
+#pragma unroll
+      for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[s + 1], ldz<T>(&tab->a[h][s]), v[s]); }
+#pragma unroll
+      for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->w[h][s]), v[LS - 1]); }
+      ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
+    }
+  }
+  if (DAG == 0 && mix) {
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
+      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < LS; s++)
+#pragma unroll
+      for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
+  }
+  if (post_on) {
+#pragma unroll
+    for (int s = 0; s < LS; s++) { ZSCALC(y[s], ldz<T>(&tab->post[s])); }
+  }
+}
+
 template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
 __global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv,
                                                  const ZM5Tab *tab, Reduce red, const int *skip) {
@@ -212,66 +374,16 @@ __global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPt
   const long work = (long)g.n4cb * NCH;
   double acc = 0;
   const bool sk = skip && skip[rhs];
-  const int sweep = tab->sweep, mix = tab->mix, pre_on = tab->pre_on, post_on = tab->post_on;
   for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
     const int x = (int)(w % g.n4cb);
     const int k = (int)(w / g.n4cb);
-    const int h = (k < NCH / 2) ? 0 : 1;
     const long base = rhs * per + x;
     cplx<T> v[LS][NC], y[LS][NC];
 #pragma unroll
     for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    if (pre_on) {
-#pragma unroll
-      for (int s = 0; s < LS; s++) { ZSCALC(v[s], ldz<T>(&tab->pre[s])); }
-    }
-    // upper half at dag 0 and lower half at dag 1 take slice s-1, the others s+1
-    const bool from_below = (DAG == 0) == (h == 0);
-    if (DAG == 1 && mix) {
-#pragma unroll
-      for (int s = 0; s < LS; s++) {
-        const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
-        const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
-      }
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
-    }
-    if (sweep) {
-      if (tab->walls_first[h]) {
-        ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
-#pragma unroll
-        for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[LS - 1], ldz<T>(&tab->w[h][s]), v[s]); }
-#pragma unroll
-        for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->a[h][s]), v[s + 1]); }
-      } else {
-#pragma unroll
-        for (int s = 0; s <= LS - 2; s++) { ZAXPYC(v[s + 1], ldz<T>(&tab->a[h][s]), v[s]); }
-#pragma unroll
-        for (int s = LS - 2; s >= 0; s--) { ZAXPYC(v[s], ldz<T>(&tab->w[h][s]), v[LS - 1]); }
-        ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
-      }
-    }
-    if (DAG == 0 && mix) {
-#pragma unroll
-      for (int s = 0; s < LS; s++) {
-        const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
-        const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
-      }
-    } else {
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
-    }
+    m5z_column<LS, DAG, NC, T>(v, y, k < NCH / 2 ? 0 : 1, tab);
 #pragma unroll
     for (int s = 0; s < LS; s++) {
-      if (post_on) { ZSCALC(y[s], ldz<T>(&tab->post[s])); }
       cplx<T> o[NC];
       if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
 #pragma unroll
@@ -282,17 +394,43 @@ __global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPt
       st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
     }
   }
-  if (NORM) {
-    double bs = block_sum<NT>(acc, sh);
-    if (threadIdx.x == 0) red.partial[rhs * gridDim.x + blockIdx.x] = bs;
-    if (last_block(red.ticket, gridDim.x * gridDim.y)) {
-      for (int q = 0; q < g.nrhs; q++) {
-        double t = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
-        if (threadIdx.x == 0 && !(skip && skip[q])) red.result[q] = t;
-        __syncthreads();
-      }
+  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
+}
+
+// 16-bit zMobius: the lane layout of m5h_kernel.
+template <int LS, int DAG, bool XPAY, bool NORM, int NT>
+__global__ void __launch_bounds__(NT) m5zh_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv,
+                                                  const ZM5Tab *tab, Reduce red, const int *skip) {
+  __shared__ double sh[NT / 32];
+  const int rhs = blockIdx.y;
+  const long per = (long)g.n4cb * LS;
+  const int lane = threadIdx.x & 31, j = lane & 7;
+  const long nw = (long)gridDim.x * (NT / 32);
+  double acc = 0;
+  const bool sk = skip && skip[rhs];
+  for (long x0 = ((long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5)) * 4; !sk && x0 < g.n4cb; x0 += nw * 4) {
+    const long x = x0 + (lane >> 3);
+    const bool active = j < 6 && x < g.n4cb;
+    const int jj = active ? j : 0;
+    const long base = rhs * per + (active ? x : 0);
+    cplx<float> v[LS][2], y[LS][2];
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      if (active) ld_chunk<P16>(in, base + (long)s * g.n4cb, jj, v[s]);
+      else v[s][0] = v[s][1] = mk(0.f, 0.f);
+    }
+    m5z_column<LS, DAG, 2, float>(v, y, jj < 3 ? 0 : 1, tab);
+#pragma unroll
+    for (int s = 0; s < LS; s++) {
+      cplx<float> o[2];
+      if (XPAY && active) ld_chunk<P16>(xv, base + (long)s * g.n4cb, jj, o);
+#pragma unroll
+      for (int q = 0; q < 2; q++) o[q] = (XPAY && active) ? o[q] + y[s][q] : y[s][q];
+      const float n = st_chunk16(out, base + (long)s * g.n4cb, jj, o, active);
+      if (NORM) acc += (double)n;
     }
   }
+  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
 }
 
 template <int P, int LS>
@@ -300,6 +438,18 @@ static cudaError_t m5z_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPt
                                  const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip,
                                  cudaStream_t st) {
   const int NT = 128;
+  if constexpr (P == P16) {
+    dim3 grid(grid_blocks((long)g.n4cb * 8, NT), g.nrhs);
+#define M5ZH(D, XP, NR)                                                                             \
+    if (dag == D && !!xpay == XP && !!norm == NR) {                                                 \
+      m5zh_kernel<LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, tab, red, skip);           \
+      return launched();                                                                            \
+    }
+    M5ZH(0, false, false) M5ZH(0, true, false) M5ZH(0, true, true)
+    M5ZH(1, false, false) M5ZH(1, true, false) M5ZH(1, true, true)
+#undef M5ZH
+    return cudaErrorInvalidValue;
+  } else {
   dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
 #define M5ZL(D, XP, NR)                                                                             \
   if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
@@ -310,6 +460,7 @@ static cudaError_t m5z_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPt
   M5ZL(1, false, false) M5ZL(1, true, false) M5ZL(1, true, true)
 #undef M5ZL
   return cudaErrorInvalidValue;
+  }
 }
 
 template <int P>
@@ -332,6 +483,7 @@ cudaError_t launch_m5z(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPt
                        const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
   if (prec == P64) return m5z_launch_p<P64>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
   if (prec == P32) return m5z_launch_p<P32>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+  if (prec == P16) return m5z_launch_p<P16>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
   return cudaErrorInvalidValue;
 }
 

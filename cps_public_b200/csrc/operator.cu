@@ -300,7 +300,6 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
   if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
   if (mobius_like()) {
-    if (prec == P16) throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     const int ok[] = {4, 8, 12, 16, 20, 24, 32};
     bool found = false;
     for (int v : ok) found |= (v == ls);

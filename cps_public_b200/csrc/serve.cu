@@ -291,8 +291,6 @@ int cpsb_serve_submit(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p,
     if (!srv || !id || !x || !b || nrhs < 1 || nrhs > 4096) throw Error{CPSB_ERR_ARG, "bad submit arguments"};
     for (int i = 0; i < nrhs; i++)
       if (!x[i] || !b[i]) throw Error{CPSB_ERR_ARG, "null vector"};
-    if (p->action >= CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
-      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     Server &S = srv->s;
     const long n = cb_sites(h, p);
     int g = std::min(nrhs, MAX_RHS);
@@ -346,8 +344,6 @@ int cpsb_serve_submit_minvcg(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_par
       throw Error{CPSB_ERR_ARG, "bad multishift submit arguments"};
     if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE"};
     if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
-    if (p->action >= CPSB_MOBIUS && a->precision == CPSB_PREC_F16)
-      throw Error{CPSB_ERR_UNSUPPORTED, "FP16 storage is not implemented for Mobius / zMobius"};
     const int nvec = type == CPSB_SINGLE ? 1 : nshift;
     for (int i = 0; i < nvec; i++)
       if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};

@@ -44,8 +44,6 @@ def test_minvcg_fp64_vs_reference(name, action):
 @pytest.mark.parametrize("name,action", CASES)
 def test_minvcg_reduced_precision_refined(name, action, prec):
     import cps_public_b200 as cb
-    if action == "mobius" and prec == "F16":
-        pytest.skip("16-bit storage is not implemented for Mobius")
     rec, u, src = load(name)
     op = device_op(rec, u, action)
     shifts = list(rec["minvcg_shifts"])

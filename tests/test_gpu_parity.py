@@ -70,8 +70,6 @@ def test_fp64_cg_vs_reference(name, action):
 @pytest.mark.parametrize("name,action", CASES + PC_CASES)
 def test_mixed_cg_reaches_fp64_true_residual(name, action, prec):
     import cps_public_b200 as cb
-    if action == "mobius" and prec == "F16":
-        pytest.skip("FP16 storage is not implemented for Mobius")
     rec, u, src = load(name)
     op = device_op(rec, u, action)
     x, r = op.InvCg(src, stop_rsd=1e-10, max_num_iter=5000, precision=getattr(cb, prec))
@@ -151,8 +149,6 @@ def test_reduced_precision_operators(action, ls, prec):
     import cps_public_b200 as cb
     from cps_public_b200 import fields
     from oracle import oracle
-    if action == "mobius" and prec == "F16":
-        pytest.skip("16-bit storage is not implemented for Mobius")
     tol = {"F32": 2e-6, "F16": 5e-4}[prec]
     P = getattr(cb, prec)
     dims = (4, 6, 4, 8)
@@ -267,10 +263,11 @@ def test_zmobius_operators_vs_reference(name):
 
 
 @pytest.mark.parametrize("name", ZMOBIUS_CASES)
-@pytest.mark.parametrize("prec", ["F64", "F32"])
+@pytest.mark.parametrize("prec", ["F64", "F32", "F16"])
 def test_zmobius_cg_vs_reference(name, prec):
     """zMobius CG: FP64 follows CPS's InvCg (iterations within 1, solution within
-    1e-9); mixed FP32 reaches the FP64 true residual 1e-10 (solution within 1e-8)."""
+    1e-9); mixed FP32 / 16-bit reach the FP64 true residual 1e-10 (solution
+    within 1e-8)."""
     import cps_public_b200 as cb
     rec, u, src = load(name)
     op = zmobius_op(rec, u)

@@ -4,7 +4,7 @@ The autotuner picks one launch shape per operator shape, so the parity tests
 exercise only the winners; here each shape is pinned in a fresh process
 (CPSB_TUNE_FORCE) and Dslash / MatPcDagMatPc are compared with the oracle for
 Wilson, DWF and Mobius at FP64 (tolerance 1e-13), FP32 (2e-6 per hop) and
-16-bit storage (5e-4 per hop; Mobius has no 16-bit storage), on two non-cubic
+16-bit storage (5e-4 per hop), on two non-cubic
 antiperiodic lattices: 4x6x4x8 (tiles of consecutive sites) and 8x8x4x6 (32
 sites per (z, t) plane, so the multi-plane tiles are used).
 """
@@ -40,8 +40,6 @@ def _child():
         rdd = ref.dslash(src, 0, 1)
         rm, rdot = ref.mdagm(src)
         for prec in (0, 1, 2):
-            if action == "mobius" and prec == 2:
-                continue
             d0 = op.DslashPrec(src, 1, 0, prec)
             d1 = op.DslashPrec(src, 0, 1, prec)
             m, dot = op.MatPcDagMatPcPrec(src, prec)
