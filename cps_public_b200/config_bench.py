@@ -5,8 +5,8 @@
       M5 = 1.8, m_f = 0.005, links reunitarise(exp(i 0.15 H)) seeded: the 12
       spin-colour point sources at one seeded odd site (4-D source embedded on
       s = 0 / Ls-1 by chirality) solved in one batched mixed-precision CG
-      (FP32 inner, FP64 reliable updates) to FP64 true residual 1e-10, against
-      the plain FP64 CG on one of the sources.
+      (16-bit and FP32 storage inner, FP64 reliable updates) to FP64 true
+      residual 1e-10, against the plain FP64 CG on one of the sources.
 
   python -m cps_public_b200.config_bench multishift
       Shamir DWF on 24^3x64, Ls = 12, m_f = 0.01, links as above: MInvCG with 12
@@ -30,7 +30,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import F32, F64, MULTI, CgArg, DiracOp, Gauge, SolveResult, _lib, fields, init
+from . import F16, F32, F64, MULTI, CgArg, DiracOp, Gauge, SolveResult, _lib, fields, init
 
 DIMS = (24, 24, 24, 64)
 
@@ -66,8 +66,10 @@ def mobius12(a):
         return dt, [res[i].as_dict() for i in range(nrhs)]
 
     # warm-up: tunes every launch shape and captures the iteration graphs
+    solve_dev(nr, F16, 40)
     solve_dev(nr, F32, 40)
     solve_dev(1, F64, 40)
+    t_f16, r_f16 = solve_dev(nr, F16, 100000)
     t_mixed, r_mixed = solve_dev(nr, F32, 100000)
     x_mixed0 = x_d[0].cpu().numpy()
     t_f64, r_f64 = solve_dev(1, F64, 100000)
@@ -79,6 +81,11 @@ def mobius12(a):
     xs, rs = op.InvCgMulti(srcs, stop_rsd=a.stop, max_num_iter=100000, precision=F32)
     t_e2e = time.perf_counter() - t0
     out = {"workload": "mobius_multi_rhs_24x24x24x64_ls16", "rhs": nr, "site": site,
+           "mixed_f16_x12": {"solves_per_s": nr / t_f16, "seconds": t_f16,
+                             "iters": max(r["iters"] for r in r_f16),
+                             "max_true_rsd": max(r["true_rsd"] for r in r_f16),
+                             "reliable_updates": max(r["reliable_updates"] for r in r_f16)},
+           "mixed_f16_vs_fp64": (nr / t_f16) * t_f64,
            "mixed_f32_x12": {"solves_per_s": nr / t_mixed, "seconds": t_mixed,
                              "iters": max(r["iters"] for r in r_mixed),
                              "max_true_rsd": max(r["true_rsd"] for r in r_mixed),
