@@ -48,6 +48,24 @@ __device__ __forceinline__ void ld_chunk<P16>(const SpinorPtr &f, long i, int j,
   v[0] = mk(dec16(w.x, 0) * q, dec16(w.y, 0) * q);
   v[1] = mk(dec16(w.x, 1) * q, dec16(w.y, 1) * q);
 }
+// A 16-bit column of Ls slices: all raw loads issued first, then decoded, so
+// the Ls loads are in flight together.
+template <int LS>
+__device__ __forceinline__ void ld_column16(const SpinorPtr &f, long base, long step, int j, cplx<float> (&v)[LS][2]) {
+  uint2 w[LS];
+  float q[LS];
+#pragma unroll
+  for (int s = 0; s < LS; s++) {
+    const long i = base + (long)s * step;
+    w[s] = __ldg((const uint2 *)((const uint4 *)f.data + (long)(j >> 1) * f.stride + i) + (j & 1));
+    q[s] = __ldg(f.norm + i);
+  }
+#pragma unroll
+  for (int s = 0; s < LS; s++) {
+    v[s][0] = mk(dec16(w[s].x, 0) * q[s], dec16(w[s].y, 0) * q[s]);
+    v[s][1] = mk(dec16(w[s].x, 1) * q[s], dec16(w[s].y, 1) * q[s]);
+  }
+}
 template <int P>
 __device__ __forceinline__ void st_chunk(const SpinorPtr &f, long i, int k, const cplx<typename ChunkT<P>::T> *v);
 template <>
@@ -58,28 +76,40 @@ template <>
 __device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k, const cplx<float> *v) {
   ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[1].re, v[0].im, v[1].im);
 }
-// 16-bit store of chunk j of site i from lane j of the site's 8-lane group
-// (every lane of the warp calls it; lanes with active = false only take part
-// in the maximum).  Returns |stored values|^2 of this lane (the rounded
-// values a later load returns), encoded as store_spinor<P16> encodes them.
-__device__ __forceinline__ float st_chunk16(const SpinorPtr &f, long i, int j, const cplx<float> *v, bool active) {
-  float m = active ? fmaxf(fmaxf(fabsf(v[0].re), fabsf(v[0].im)), fmaxf(fabsf(v[1].re), fabsf(v[1].im))) : 0.f;
-  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
-  if (!active) return 0.f;
-  const float scale = m > 0.f ? 32767.0f / m : 0.f;
-  const float nq = m * (1.0f / 32767.0f);
-  const unsigned wx = enc16x2(v[0].re, v[1].re, scale), wy = enc16x2(v[0].im, v[1].im, scale);
-  ((uint2 *)((uint4 *)f.data + (long)(j >> 1) * f.stride + i))[j & 1] = make_uint2(wx, wy);
-  if (j == 0) f.norm[i] = nq;
-  float n = 0.f;
+// Stores the column y[0..LS) of chunk j (16-bit), slice s at base + s*step:
+// the site maxima of all slices first, combined across the 8-lane group by
+// independent shuffles (pipelined over s rather than one dependent round trip
+// per slice), then encode and store.  Every lane of the warp calls it.
+// Returns the sum of |stored values|^2 of this lane.
+template <int LS>
+__device__ __forceinline__ double st_column16(const SpinorPtr &f, long base, long step, int j,
+                                              const cplx<float> (&y)[LS][2], bool active) {
+  float m[LS];
 #pragma unroll
-  for (int h = 0; h < 2; h++) {
-    const float a = dec16(wx, h) * nq, b = dec16(wy, h) * nq;
-    n += a * a + b * b;
+  for (int s = 0; s < LS; s++)
+    m[s] = active ? fmaxf(fmaxf(fabsf(y[s][0].re), fabsf(y[s][0].im)), fmaxf(fabsf(y[s][1].re), fabsf(y[s][1].im)))
+                  : 0.f;
+#pragma unroll
+  for (int d = 1; d < 8; d <<= 1)
+#pragma unroll
+    for (int s = 0; s < LS; s++) m[s] = fmaxf(m[s], __shfl_xor_sync(0xffffffffu, m[s], d));
+  double acc = 0;
+  if (!active) return acc;
+#pragma unroll
+  for (int s = 0; s < LS; s++) {
+    const float scale = m[s] > 0.f ? 32767.0f / m[s] : 0.f;
+    const float nq = m[s] * (1.0f / 32767.0f);
+    const long i = base + (long)s * step;
+    const unsigned wx = enc16x2(y[s][0].re, y[s][1].re, scale), wy = enc16x2(y[s][0].im, y[s][1].im, scale);
+    ((uint2 *)((uint4 *)f.data + (long)(j >> 1) * f.stride + i))[j & 1] = make_uint2(wx, wy);
+    if (j == 0) f.norm[i] = nq;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const float a = dec16(wx, h) * nq, b = dec16(wy, h) * nq;
+      acc += (double)(a * a + b * b);
+    }
   }
-  return n;
+  return acc;
 }
 
 // v[s] += f * w[s] on one chunk
@@ -94,28 +124,42 @@ __device__ __forceinline__ float st_chunk16(const SpinorPtr &f, long i, int j, c
     (dst)[q].im *= (f);                                      \
   }
 
-// y = mix(M5^-1 v) (DAG 0) or M5^-dag(mix^dag(v)) (DAG 1) on one column, real
-// coefficients; the output scale is applied by the caller.
-template <int LS, int DAG, int NC, typename T>
-__device__ __forceinline__ void m5_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS][NC], bool upper, const M5Coef &cf) {
-  const T K = (T)cf.K, b = (T)cf.b, c = (T)cf.c, mwall = (T)(-cf.mass * cf.c), invd = (T)cf.invd;
-  if (DAG == 1) {
-    // mix^dag: upper from s+1, lower from s-1
+// v[s] <- b v[s] + c v[s -+ 1] in place (from_below: slice s-1, the wall term
+// mwall v[Ls-1] at s = 0; otherwise slice s+1, the wall mwall v[0] at Ls-1):
+// sweeping away from the slice each step reads keeps that slice unmodified,
+// so no second column of registers is needed.
+template <int LS, int NC, typename T>
+__device__ __forceinline__ void mix_inplace(cplx<T> (&v)[LS][NC], bool from_below, T b, T c, T mwall) {
+  if (from_below) {
+    cplx<T> wall[NC];
 #pragma unroll
-    for (int s = 0; s < LS; s++) {
+    for (int q = 0; q < NC; q++) wall[q] = v[LS - 1][q];
 #pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
-      if (upper) {
-        if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
-      } else {
-        if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
-      }
-    }
+    for (int s = LS - 1; s >= 1; s--)
 #pragma unroll
-    for (int s = 0; s < LS; s++)
+      for (int q = 0; q < NC; q++) v[s][q] = cscale(b, v[s][q]) + cscale(c, v[s - 1][q]);
 #pragma unroll
-      for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
+    for (int q = 0; q < NC; q++) v[0][q] = cscale(b, v[0][q]) + cscale(mwall, wall[q]);
+  } else {
+    cplx<T> wall[NC];
+#pragma unroll
+    for (int q = 0; q < NC; q++) wall[q] = v[0][q];
+#pragma unroll
+    for (int s = 0; s <= LS - 2; s++)
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[s][q] = cscale(b, v[s][q]) + cscale(c, v[s + 1][q]);
+#pragma unroll
+    for (int q = 0; q < NC; q++) v[LS - 1][q] = cscale(b, v[LS - 1][q]) + cscale(mwall, wall[q]);
   }
+}
+
+// v <- mix(M5^-1 v) (DAG 0) or M5^-dag(mix^dag(v)) (DAG 1) on one column, in
+// place, real coefficients; the output scale is applied by the caller.
+template <int LS, int DAG, int NC, typename T>
+__device__ __forceinline__ void m5_column(cplx<T> (&v)[LS][NC], bool upper, const M5Coef &cf) {
+  const T K = (T)cf.K, b = (T)cf.b, c = (T)cf.c, mwall = (T)(-cf.mass * cf.c), invd = (T)cf.invd;
+  // mix^dag (DAG 1): upper from s+1, lower from s-1
+  if (DAG == 1) mix_inplace<LS, NC, T>(v, !upper, b, c, mwall);
   // M5^-1 (DAG 0) or M5^-dag (DAG 1) sweeps.  The structure of the
   // dag-0 lower sweep equals the dag-1 upper sweep and vice versa.
   const bool walls_first = (DAG == 0) ? !upper : upper;
@@ -132,24 +176,8 @@ __device__ __forceinline__ void m5_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS]
     for (int s = LS - 2; s >= 0; s--) { const T f = (T)cf.f2[s]; AXPYC(v[s], f, v[LS - 1]); }
     SCALC(v[LS - 1], invd);
   }
-  if (DAG == 0) {
-    // mix: upper from s-1, lower from s+1
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-#pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = cscale(b, v[s][q]);
-      if (upper) {
-        if (s > 0) { AXPYC(y[s], c, v[s - 1]); } else { AXPYC(y[s], mwall, v[LS - 1]); }
-      } else {
-        if (s < LS - 1) { AXPYC(y[s], c, v[s + 1]); } else { AXPYC(y[s], mwall, v[0]); }
-      }
-    }
-  } else {
-#pragma unroll
-    for (int s = 0; s < LS; s++)
-#pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
-  }
+  // mix (DAG 0): upper from s-1, lower from s+1
+  if (DAG == 0) mix_inplace<LS, NC, T>(v, upper, b, c, mwall);
 }
 
 // Per-RHS |out|^2 of the block into red (deterministic: partials summed in
@@ -184,18 +212,18 @@ __global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr
     const int x = (int)(w % g.n4cb);
     const int k = (int)(w / g.n4cb);
     const long base = rhs * per + x;
-    cplx<T> v[LS][NC], y[LS][NC];
+    cplx<T> v[LS][NC];
 #pragma unroll
     for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    m5_column<LS, DAG, NC, T>(v, y, k < NCH / 2, cf);
+    m5_column<LS, DAG, NC, T>(v, k < NCH / 2, cf);
 #pragma unroll
     for (int s = 0; s < LS; s++) {
       cplx<T> o[NC];
       if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
 #pragma unroll
       for (int q = 0; q < NC; q++) {
-        if (XPAY) o[q] = o[q] + cscale(sc, y[s][q]);
-        else o[q] = cscale(sc, y[s][q]);
+        if (XPAY) o[q] = o[q] + cscale(sc, v[s][q]);
+        else o[q] = cscale(sc, v[s][q]);
         if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
       }
       st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
@@ -222,22 +250,25 @@ __global__ void __launch_bounds__(NT) m5h_kernel(Geom g, SpinorPtr out, SpinorPt
     const bool active = j < 6 && x < g.n4cb;
     const int jj = active ? j : 0;
     const long base = rhs * per + (active ? x : 0);
-    cplx<float> v[LS][2], y[LS][2];
+    cplx<float> v[LS][2];
+    // inactive lanes read a valid chunk of site 0 and store nothing
+    ld_column16<LS>(in, base, g.n4cb, jj, v);
+    m5_column<LS, DAG, 2, float>(v, jj < 3, cf);
+    if (XPAY) {
+      cplx<float> o[LS][2];
+      ld_column16<LS>(xv, base, g.n4cb, jj, o);
 #pragma unroll
-    for (int s = 0; s < LS; s++) {
-      if (active) ld_chunk<P16>(in, base + (long)s * g.n4cb, jj, v[s]);
-      else v[s][0] = v[s][1] = mk(0.f, 0.f);
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) v[s][q] = o[s][q] + cscale(sc, v[s][q]);
+    } else {
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) v[s][q] = cscale(sc, v[s][q]);
     }
-    m5_column<LS, DAG, 2, float>(v, y, jj < 3, cf);
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      cplx<float> o[2];
-      if (XPAY && active) ld_chunk<P16>(xv, base + (long)s * g.n4cb, jj, o);
-#pragma unroll
-      for (int q = 0; q < 2; q++) o[q] = (XPAY && active) ? o[q] + cscale(sc, y[s][q]) : cscale(sc, y[s][q]);
-      const float n = st_chunk16(out, base + (long)s * g.n4cb, jj, o, active);
-      if (NORM) acc += (double)n;
-    }
+    const double n = st_column16<LS>(out, base, g.n4cb, jj, v, active);
+    if (NORM) acc += n;
   }
   if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
 }
@@ -304,10 +335,43 @@ template <typename T> __device__ __forceinline__ cplx<T> ldz(const double2 *p) {
 #define ZSCALC(dst, f)                                       \
   _Pragma("unroll") for (int q = 0; q < NC; q++) (dst)[q] = cmul((f), (dst)[q]);
 
-// y = post . mix(M5^-1(pre . v)) (DAG 0) or post . M5^-dag(mix^dag(pre . v))
-// (DAG 1) on one column of chirality half h, the stages the table enables.
+// v[s] <- bb_s v[s] + cc[h]_s v[s -+ 1] in place (cyclic: the wall terms
+// are in cc), in the sweep order of mix_inplace.
+template <int LS, int NC, typename T>
+__device__ __forceinline__ void zmix_inplace(cplx<T> (&v)[LS][NC], bool from_below, int h, const ZM5Tab *tab) {
+  cplx<T> wall[NC];
+  if (from_below) {
+#pragma unroll
+    for (int q = 0; q < NC; q++) wall[q] = v[LS - 1][q];
+#pragma unroll
+    for (int s = LS - 1; s >= 1; s--) {
+      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[s][q] = cmul(b, v[s][q]) + cmul(c, v[s - 1][q]);
+    }
+    const cplx<T> b = ldz<T>(&tab->bb[0]), c = ldz<T>(&tab->cc[h][0]);
+#pragma unroll
+    for (int q = 0; q < NC; q++) v[0][q] = cmul(b, v[0][q]) + cmul(c, wall[q]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < NC; q++) wall[q] = v[0][q];
+#pragma unroll
+    for (int s = 0; s <= LS - 2; s++) {
+      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[s][q] = cmul(b, v[s][q]) + cmul(c, v[s + 1][q]);
+    }
+    const cplx<T> b = ldz<T>(&tab->bb[LS - 1]), c = ldz<T>(&tab->cc[h][LS - 1]);
+#pragma unroll
+    for (int q = 0; q < NC; q++) v[LS - 1][q] = cmul(b, v[LS - 1][q]) + cmul(c, wall[q]);
+  }
+}
+
+// v <- post . mix(M5^-1(pre . v)) (DAG 0) or post . M5^-dag(mix^dag(pre . v))
+// (DAG 1) on one column of chirality half h, in place, the stages the table
+// enables.
 template <int LS, int DAG, int NC, typename T>
-__device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS][NC], int h, const ZM5Tab *tab) {
+__device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], int h, const ZM5Tab *tab) {
   const int sweep = tab->sweep, mix = tab->mix, pre_on = tab->pre_on, post_on = tab->post_on;
   if (pre_on) {
 #pragma unroll
@@ -315,19 +379,7 @@ __device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS
   }
   // upper half at dag 0 and lower half at dag 1 take slice s-1, the others s+1
   const bool from_below = (DAG == 0) == (h == 0);
-  if (DAG == 1 && mix) {
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
-      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
-#pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
-    }
-#pragma unroll
-    for (int s = 0; s < LS; s++)
-#pragma unroll
-      for (int q = 0; q < NC; q++) v[s][q] = y[s][q];
-  }
+  if (DAG == 1 && mix) zmix_inplace<LS, NC, T>(v, from_below, h, tab);
   if (sweep) {
     if (tab->walls_first[h]) {
       ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
@@ -343,23 +395,10 @@ __device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], cplx<T> (&y)[LS
       ZSCALC(v[LS - 1], ldz<T>(&tab->invd[h]));
     }
   }
-  if (DAG == 0 && mix) {
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      const int nb = from_below ? (s == 0 ? LS - 1 : s - 1) : (s == LS - 1 ? 0 : s + 1);
-      const cplx<T> b = ldz<T>(&tab->bb[s]), c = ldz<T>(&tab->cc[h][s]);
-#pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = cmul(b, v[s][q]) + cmul(c, v[nb][q]);
-    }
-  } else {
-#pragma unroll
-    for (int s = 0; s < LS; s++)
-#pragma unroll
-      for (int q = 0; q < NC; q++) y[s][q] = v[s][q];
-  }
+  if (DAG == 0 && mix) zmix_inplace<LS, NC, T>(v, from_below, h, tab);
   if (post_on) {
 #pragma unroll
-    for (int s = 0; s < LS; s++) { ZSCALC(y[s], ldz<T>(&tab->post[s])); }
+    for (int s = 0; s < LS; s++) { ZSCALC(v[s], ldz<T>(&tab->post[s])); }
   }
 }
 
@@ -378,17 +417,17 @@ __global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPt
     const int x = (int)(w % g.n4cb);
     const int k = (int)(w / g.n4cb);
     const long base = rhs * per + x;
-    cplx<T> v[LS][NC], y[LS][NC];
+    cplx<T> v[LS][NC];
 #pragma unroll
     for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    m5z_column<LS, DAG, NC, T>(v, y, k < NCH / 2 ? 0 : 1, tab);
+    m5z_column<LS, DAG, NC, T>(v, k < NCH / 2 ? 0 : 1, tab);
 #pragma unroll
     for (int s = 0; s < LS; s++) {
       cplx<T> o[NC];
       if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
 #pragma unroll
       for (int q = 0; q < NC; q++) {
-        o[q] = XPAY ? o[q] + y[s][q] : y[s][q];
+        o[q] = XPAY ? o[q] + v[s][q] : v[s][q];
         if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
       }
       st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
@@ -413,22 +452,20 @@ __global__ void __launch_bounds__(NT) m5zh_kernel(Geom g, SpinorPtr out, SpinorP
     const bool active = j < 6 && x < g.n4cb;
     const int jj = active ? j : 0;
     const long base = rhs * per + (active ? x : 0);
-    cplx<float> v[LS][2], y[LS][2];
+    cplx<float> v[LS][2];
+    // inactive lanes read a valid chunk of site 0 and store nothing
+    ld_column16<LS>(in, base, g.n4cb, jj, v);
+    m5z_column<LS, DAG, 2, float>(v, jj < 3 ? 0 : 1, tab);
+    if (XPAY) {
+      cplx<float> o[LS][2];
+      ld_column16<LS>(xv, base, g.n4cb, jj, o);
 #pragma unroll
-    for (int s = 0; s < LS; s++) {
-      if (active) ld_chunk<P16>(in, base + (long)s * g.n4cb, jj, v[s]);
-      else v[s][0] = v[s][1] = mk(0.f, 0.f);
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) v[s][q] = o[s][q] + v[s][q];
     }
-    m5z_column<LS, DAG, 2, float>(v, y, jj < 3 ? 0 : 1, tab);
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      cplx<float> o[2];
-      if (XPAY && active) ld_chunk<P16>(xv, base + (long)s * g.n4cb, jj, o);
-#pragma unroll
-      for (int q = 0; q < 2; q++) o[q] = (XPAY && active) ? o[q] + y[s][q] : y[s][q];
-      const float n = st_chunk16(out, base + (long)s * g.n4cb, jj, o, active);
-      if (NORM) acc += (double)n;
-    }
+    const double n = st_column16<LS>(out, base, g.n4cb, jj, v, active);
+    if (NORM) acc += n;
   }
   if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
 }
