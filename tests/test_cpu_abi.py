@@ -44,3 +44,27 @@ def test_error_strings_and_no_device_status():
     h = C.c_void_p()
     assert lib.cpsb_serve_create(C.byref(h), 2, 0.5, 0) == -6
     assert not h.value
+
+
+@pytest.mark.parametrize("cname,pyname", [("cpsb_dirac_params", "DiracParams"), ("cpsb_cg_arg", "CgArg"),
+                                          ("cpsb_solve_result", "SolveResult"),
+                                          ("cpsb_serve_stats_t", "ServeStats")])
+def test_struct_layout_matches_header(cname, pyname, tmp_path):
+    """The ctypes mirrors in _lib.py have the size and field offsets of the C
+    structs as a C compiler lays them out from include/cpsb200.h."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    py = getattr(_lib, pyname)
+    fields = [f for f, _ in py._fields_]
+    lines = [f'printf("%zu\\n", sizeof({cname}));'] + [f'printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "cpsb200.h"\nint main(void) {\n'
+                   + "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == C.sizeof(py), (cname, got[0], C.sizeof(py))
+    assert got[1:] == [getattr(py, f).offset for f in fields], (cname, got[1:])
