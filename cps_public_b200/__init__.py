@@ -185,7 +185,8 @@ class DiracOp:
         return out, r
 
     def Dminus(self, x_full):
-        """DiracOpMobius::Dminus on a full vector (4-D-even half first)."""
+        """DiracOpMobius::Dminus on a full vector (4-D-even half first), or for
+        zMobius DiracOpZMobius::Dminus (odd half first, complex c_s)."""
         x = np.ascontiguousarray(x_full, np.float64)
         if x.size != 2 * self.n:
             raise ValueError(f"full vector has {x.size} reals, expected {2 * self.n}")

@@ -611,18 +611,37 @@ int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const dou
   return guarded([&] {
     need_init();
     check_params(h, p);
-    if (p->action != CPSB_MOBIUS) throw Error{CPSB_ERR_ARG, "Dminus is a Mobius operator"};
+    if (p->action != CPSB_MOBIUS && p->action != CPSB_ZMOBIUS)
+      throw Error{CPSB_ERR_ARG, "Dminus is a Mobius / zMobius operator"};
     if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     const long n = op.nsites();
     if (out < in + 48 * n && in < out + 48 * n) throw Error{CPSB_ERR_ARG, "out and in overlap"};
-    const double *in_e = in, *in_o = in + 24 * n;
-    double *out_e = out, *out_o = out + 24 * n;
+    // DiracOpMobius keeps the even half first, DiracOpZMobius the odd half
+    const bool zm = p->action == CPSB_ZMOBIUS;
+    const double *in_e = in + (zm ? 24 * n : 0), *in_o = in + (zm ? 0 : 24 * n);
+    double *out_e = out + (zm ? 24 * n : 0), *out_o = out + (zm ? 0 : 24 * n);
     Field fe(P64, n), fo(P64, n), ge(P64, n), go(P64, n);
     upload(fe, &in_e, 1, n, st);
     upload(fo, &in_o, 1, n, st);
-    mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
+    if (!zm) {
+      mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
+    } else {
+      // DiracOpZMobius::Dminus (d_op_zmobius.C:1213-1272, zmobius_dminus.C:44-116):
+      // out_x = (c_s/2) D_W in_y - (c_s(4 - M5) - a5_inv) in_x, per slice s
+      Reduce none;
+      memset(&none, 0, sizeof(none));
+      const ZM5Tab *t = (const ZM5Tab *)op.ztab.p;
+      Field th(P64, n);
+      for (int half = 0; half < 2; half++) {
+        const Field &src_other = half ? fo : fe, &src_same = half ? fe : fo;
+        const Field &dst = half ? ge : go;
+        op.hop(th.ptr(), src_other.ptr(), half ? 1 : 0, 0, 1.0, nullptr, nullptr, nullptr, st);
+        CK(launch_m5z(P64, 0, op.geom, dst.ptr(), src_same.ptr(), SpinorPtr{}, t + 11, 0, 0, none, nullptr, st));
+        CK(launch_m5z(P64, 0, op.geom, dst.ptr(), th.ptr(), dst.ptr(), t + 12, 1, 0, none, nullptr, st));
+      }
+    }
     download(&out_e, 1, n, ge, st);
     download(&out_o, 1, n, go, st);
     return CPSB_OK;

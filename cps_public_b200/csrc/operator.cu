@@ -258,17 +258,24 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   //   2 dag1 conj(kb) . M5^-dag(mix^dag(-conj(kb) .))              3 dag1 M5^-dag(mix^dag(.))
   //   7 dag1 mix^dag alone            8 dag1 K-weighted H5^dag       9 dag1 -conj(kb) . M5^-dag(.)
   //  10 dag1 conj(kb) . M5^-dag(mix^dag(.))
-  const int NT = 11;
+  //  11 dag0 -(c_s (4 - M5) - a5_inv) .    12 dag0 (c_s / 2) .   (DiracOpZMobius::Dminus)
+  const int NT = 13;
   std::vector<ZM5Tab> t(NT);
   memset(t.data(), 0, sizeof(ZM5Tab) * NT);
   const std::vector<zc_t> zero(ls, zc_t(0.0, 0.0));
-  auto dag_of = [](int k) { return (k == 0 || k == 1 || k == 4 || k == 5 || k == 6) ? 0 : 1; };
+  auto dag_of = [](int k) { return (k == 0 || k == 1 || k == 4 || k == 5 || k == 6 || k >= 11) ? 0 : 1; };
   for (int k = 0; k < NT; k++) {
     const int dag = dag_of(k);
+    if (k >= 11) continue;  // scale-only tables
     if (k != 4 && k != 5 && k != 7 && k != 8) zmobius_sweeps(t[k], dag, ls, pp.mass, K.data());
     if (k == 5 || k == 8) zmobius_mix(t[k], dag, ls, pp.mass, zero.data(), K.data());
     else if (k != 6 && k != 9) zmobius_mix(t[k], dag, ls, pp.mass, op.zb.data(), op.zc.data());
   }
+  for (int s = 0; s < ls; s++) {
+    t[11].post[s] = d2(-(op.zc[s] * (4 - pp.m5) - pp.a5_inv));
+    t[12].post[s] = d2(0.5 * op.zc[s]);
+  }
+  t[11].post_on = t[12].post_on = 1;
   for (int s = 0; s < ls; s++) {
     t[0].post[s] = t[4].post[s] = d2(kb[s]);
     t[1].post[s] = d2(-kb[s]);

@@ -174,7 +174,9 @@ int cpsb_fmatinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a,
 /* DiracOpMobius::Dminus(out, in) (d_op_mobius.C:745-777, mobius_dminus.C:29-86) on
  * full Mobius vectors (4-D-even half first): out = -(c(4 - M5) - a5_inv) in
  * + (c/2) D_W in, D_W the 4-D hop of every s slice into the other checkerboard.
- * Mobius only (CPSB_ERR_ARG otherwise); out and in must not overlap. */
+ * zMobius: DiracOpZMobius::Dminus (d_op_zmobius.C:1213-1272) with the complex c_s
+ * of each slice, on its full vectors (odd half first).  Mobius and zMobius only
+ * (CPSB_ERR_ARG otherwise); out and in must not overlap. */
 int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in);
 
 /* DiracOp::MinResExt(psi, phi, v, vm, degree) (include/util/dirac_op.h;

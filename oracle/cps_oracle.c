@@ -967,6 +967,44 @@ int orc_mobius_dminus(const orc_op *op, double *out, const double *in) {
   return 0;
 }
 
+/* DiracOpZMobius::Dminus, d_op_zmobius.C:1213-1272, with zmobius_dminus
+ * (d_op_zmobius/noarch/zmobius_dminus.C:44-116), on a full zMobius vector
+ * (solve checkerboard -- odd -- half first): per slice s
+ *   out_o = D_W(even -> odd)(-c_s/2 in_e),  out_e = D_W(odd -> even)(-c_s/2 in_o),
+ * then out = -(k_s in + out), k_s = c_s (4 - M5) - a5_inv, all complex. */
+int orc_zmobius_dminus(const orc_op *op, double *out, const double *in) {
+  if (op->action != 2) return -1;
+  const long n = orc_op_size(op);
+  const int ls = op->mob.ls;
+  const long n4 = n / ls;
+  double *t = scratch(n);
+  for (int half = 0; half < 2; half++) {
+    const double *src = in + (half ? 0 : n);   /* out_o from in_e, out_e from in_o */
+    double *dst = out + (half ? n : 0);
+    const int cb = half ? 1 : 0;               /* checkerboard of the input */
+    for (int s = 0; s < ls; s++) {
+      const cplx c = {op->mob.c[s][0], op->mob.c[s][1]};
+      zscale_copy(t + s * n4, src + s * n4, cscal(-0.5, c), n4);
+    }
+    for (int s = 0; s < ls; s++) orc_wilson_dslash(dst + s * n4, op->u, t + s * n4, cb, 0, op->dims);
+  }
+  for (int half = 0; half < 2; half++)
+    for (int s = 0; s < ls; s++) {
+      const cplx k = {op->mob.c[s][0] * (4 - op->m5) - op->a5_inv, op->mob.c[s][1] * (4 - op->m5)};
+      double *o = out + half * n + s * n4;
+      const double *x = in + half * n + s * n4;
+      for (long i = 0; i < n4 / 2; i++) {      /* zTimesV1PlusV2: o = k x + o */
+        const cplx xv = {x[2 * i], x[2 * i + 1]};
+        const cplx r = cmul(k, xv);
+        o[2 * i] = r.re + o[2 * i];
+        o[2 * i + 1] = r.im + o[2 * i + 1];
+      }
+    }
+  for (long i = 0; i < 2 * n; i++) out[i] = -out[i];
+  free(t);
+  return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* DiracOp::MinResExt, d_op_base/comsrc/minresext.C:32-156             */
 /* ------------------------------------------------------------------ */

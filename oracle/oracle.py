@@ -170,6 +170,15 @@ class Op:
         assert rc == 0
         return out
 
+    def zdminus(self, x_full):
+        """DiracOpZMobius::Dminus on a full vector (odd half first), complex c_s."""
+        x = np.ascontiguousarray(x_full, np.float64)
+        assert self.action == 2 and x.size == 2 * self.n
+        out = np.zeros(2 * self.n)
+        rc = lib().orc_zmobius_dminus(C.byref(self.s), _p(out), _p(x))
+        assert rc == 0
+        return out
+
     def fmatinv(self, src_full, guess_full=None, dminus=0, stop_rsd=1e-10, max_iter=5000):
         """Lattice::FmatInv(..., dminus): Fmobius applies Dminus to the source
         before MatInv (f_mobius.C:45-117); the other actions ignore the flag."""
@@ -199,6 +208,7 @@ def _setup():
     L.orc_matinv.restype = C.c_int
     L.orc_minresext.restype = C.c_double
     L.orc_mobius_dminus.restype = C.c_int
+    L.orc_zmobius_dminus.restype = C.c_int
     L.orc_mdagm.restype = C.c_int
     L.orc_invcg.restype = C.c_int
     L.orc_invcg.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_double), _dp]

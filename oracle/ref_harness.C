@@ -314,13 +314,16 @@ int main(int argc, char **argv) {
     sfree(fout);
   } else if (op == OP_DMINUS) {
     // Mobius only: one full vector (4-D-even half first) in, Dminus of it out.
-    if (action != 2) die("Dminus is a Mobius operator");
+    if (action < 2) die("Dminus is a Mobius / zMobius operator");
     Vector *fin = (Vector *)smalloc(2 * fsz * sizeof(double));
     Vector *fout = (Vector *)smalloc(2 * fsz * sizeof(double));
     read_all(fi, fin, 2 * fsz * sizeof(double));
     memset(fout, 0, 2 * fsz * sizeof(double));
-    {
+    if (action == 2) {
       DiracOpMobius d(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+      d.Dminus(fout, fin);
+    } else {  // DiracOpZMobius::Dminus, d_op_zmobius.C:1213-1272
+      DiracOpZMobius d(lat, fout, fin, &cg_arg, CNV_FRM_NO);
       d.Dminus(fout, fin);
     }
     out_payload.assign((double *)fout, (double *)fout + 2 * fsz);

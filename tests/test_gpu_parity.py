@@ -293,6 +293,16 @@ def test_zmobius_minvcg_vs_reference(name):
         assert rel(xs[i], rec["minvcg_sol"][i]) < 1e-9
 
 
+def test_zmobius_dminus_vs_reference():
+    """DiracOpZMobius::Dminus (complex c_s, odd half first) on the device against
+    the compiled CPS, FP64, within 1e-13."""
+    from tests.golden.make_golden import matinv_inputs
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    full, _ = matinv_inputs(rec)
+    assert rel(op.Dminus(full), rec["dminus_out"]) < OP_TOL
+
+
 def test_zmobius_constant_coefficients_equal_mobius():
     """zMobius with b_s = b, c_s = c is Mobius: both device paths agree."""
     import cps_public_b200 as cb

@@ -176,3 +176,9 @@ def test_zmobius_bitexact(name):
     assert it == int(rec["minvcg_iters"])
     for i in range(len(shifts)):
         np.testing.assert_array_equal(sols[i], rec["minvcg_sol"][i])
+    if "dminus_out" in rec:  # DiracOpZMobius::Dminus
+        from tests.golden.make_golden import matinv_inputs
+        from tests.golden_util import sha
+        full, _ = matinv_inputs(rec)
+        assert sha(full) == str(rec["dminus_src_sha"])
+        np.testing.assert_array_equal(op.zdminus(full), rec["dminus_out"])
