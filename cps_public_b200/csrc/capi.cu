@@ -518,15 +518,37 @@ static void mobius_dminus_dev(Operator &op, const cpsb_dirac_params &p, const Fi
   lin64(op.geom, out_o, 0.5 * c, out_o, -k, &in_o, st);
 }
 
+// DiracOpZMobius::Dminus (d_op_zmobius.C:1213-1272, zmobius_dminus.C:44-116):
+// out_x = (c_s/2) D_W in_y - (c_s(4 - M5) - a5_inv) in_x per slice s (complex c_s),
+// x, y the two checkerboards (o: the solve checkerboard).
+static void zmobius_dminus_dev(Operator &op, const Field &out_o, const Field &out_e, const Field &in_o,
+                               const Field &in_e, cudaStream_t st) {
+  Reduce none;
+  memset(&none, 0, sizeof(none));
+  const ZM5Tab *t = (const ZM5Tab *)op.ztab.p;
+  Field th(P64, op.nsites());
+  for (int half = 0; half < 2; half++) {
+    const Field &src_other = half ? in_o : in_e, &src_same = half ? in_e : in_o;
+    const Field &dst = half ? out_e : out_o;
+    op.hop(th.ptr(), src_other.ptr(), half ? 1 : 0, 0, 1.0, nullptr, nullptr, nullptr, st);
+    CK(launch_m5z(P64, 0, op.geom, dst.ptr(), src_same.ptr(), SpinorPtr{}, t + 11, 0, 0, none, nullptr, st));
+    CK(launch_m5z(P64, 0, op.geom, dst.ptr(), th.ptr(), dst.ptr(), t + 12, 1, 0, none, nullptr, st));
+  }
+}
+
+// fmat: the Lattice::FmatInv form (Mobius: Dminus of the source when dminus;
+// zMobius: f_zmobius.C:70-130, Dminus for dminus == 1, then 2 kappa_b(s) per
+// slice); otherwise DiracOp*::MatInv.
 static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out,
-                       const double *in, int dminus, cpsb_solve_result *res) {
+                       const double *in, int dminus, bool fmat, cpsb_solve_result *res) {
   return guarded([&] {
     need_init();
     check_params(h, p);
     check_cg(a);
     if (!out || !in || !res) throw Error{CPSB_ERR_ARG, "null vector or result"};
-    if (p->action == CPSB_ZMOBIUS)
-      throw Error{CPSB_ERR_UNSUPPORTED, "zMobius MatInv (DiracOpZMobius::MatInv) is not implemented"};
+    const bool zm = p->action == CPSB_ZMOBIUS;
+    if (zm && p->pc_type == 1)  // d_op_zmobius.C:929-960: ERR.NotImplemented for the other types
+      throw Error{CPSB_ERR_UNSUPPORTED, "zMobius MatInv: only ZMOB_PC_SYM2 and ZMOB_PC_ORIG"};
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     const long n = op.nsites();
@@ -539,17 +561,41 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     upload(fin_c, &in_c, 1, n, st);
     upload(fin_e, &in_e, 1, n, st);
     upload(fout_c, (const double *const *)&out_c, 1, n, st);
-    if (mob && dminus) {
+    Reduce none;
+    memset(&none, 0, sizeof(none));
+    const ZM5Tab *zt = zm ? (const ZM5Tab *)op.ztab.p : nullptr;
+    if (fmat && mob && dminus) {
       // f_mobius.C:45-117: the source becomes Dminus(source) before MatInv
       mobius_dminus_dev(op, *p, t, t2, fin_e, fin_c, st);
       CK(cudaMemcpyAsync(fin_e.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
       CK(cudaMemcpyAsync(fin_c.data.p, t2.data.p, t2.data.bytes, cudaMemcpyDeviceToDevice, st));
     }
+    if (fmat && zm) {
+      // f_zmobius.C:70-130: Dminus (dminus == 1), then 2 kappa_b(s) on both halves
+      if (dminus == 1) {
+        zmobius_dminus_dev(op, t, t2, fin_c, fin_e, st);
+        CK(cudaMemcpyAsync(fin_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(fin_e.data.p, t2.data.p, t2.data.bytes, cudaMemcpyDeviceToDevice, st));
+      }
+      CK(launch_m5z(P64, 0, g, fin_c.ptr(), fin_c.ptr(), SpinorPtr{}, zt + 13, 0, 0, none, nullptr, st));
+      CK(launch_m5z(P64, 0, g, fin_e.ptr(), fin_e.ptr(), SpinorPtr{}, zt + 13, 0, 0, none, nullptr, st));
+    }
     auto lin = [&](const Field &o, double fa, const Field &x, double fb, const Field *y) {
       lin64(g, o, fa, x, fb, y, st);
     };
     double kb = 0;
-    if (!mob) {
+    if (zm) {
+      // d_op_zmobius.C:829-1080: t = kb . D4(M5^-1 in_e, CHKB_EVEN) + in_o (kb per
+      // slice, commuting with the slice-local hop); SYM2: guess = M5 guess
+      const SpinorPtr xc = fin_c.ptr();
+      CK(launch_m5z(P64, 0, g, t.ptr(), fin_e.ptr(), SpinorPtr{}, zt + 6, 0, 0, none, nullptr, st));
+      CK(launch_m5z(P64, 0, g, t2.ptr(), t.ptr(), SpinorPtr{}, zt + 4, 0, 0, none, nullptr, st));
+      op.hop(t.ptr(), t2.ptr(), 0, 0, 1.0, &xc, nullptr, nullptr, st);
+      if (p->pc_type == 2) {
+        CK(cudaMemcpyAsync(t2.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
+        CK(launch_m5z(P64, 0, g, fout_c.ptr(), t2.ptr(), t2.ptr(), zt + 5, 1, 0, none, nullptr, st));
+      }
+    } else if (!mob) {
       // d_op_wilson.C:257-334, d_op_dwf.C:316-507
       op.dslash(t, fin_e, 0, 0, st);
       lin(t, op.kappa, t, 1.0, &fin_c);        // t = kappa D in_e + in_o
@@ -575,7 +621,17 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     CK(cudaMemcpyAsync(s->x64.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
     const int rc = s->solve(*a, res, st);
     CK(cudaMemcpyAsync(fout_c.data.p, s->x64.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
-    if (!mob) {
+    if (zm) {
+      // SYM2: out_o = M5^-1 out_o; out_e = M5^-1(kb . D4(out_o, CHKB_ODD)) + M5^-1 in_e
+      if (p->pc_type == 2) {
+        CK(launch_m5z(P64, 0, g, t.ptr(), fout_c.ptr(), SpinorPtr{}, zt + 6, 0, 0, none, nullptr, st));
+        CK(cudaMemcpyAsync(fout_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
+      }
+      CK(launch_m5z(P64, 0, g, t2.ptr(), fout_c.ptr(), SpinorPtr{}, zt + 4, 0, 0, none, nullptr, st));
+      op.hop(t.ptr(), t2.ptr(), 1, 0, 1.0, nullptr, nullptr, nullptr, st);
+      CK(launch_m5z(P64, 0, g, t2.ptr(), fin_e.ptr(), SpinorPtr{}, zt + 6, 0, 0, none, nullptr, st));
+      CK(launch_m5z(P64, 0, g, fout_e.ptr(), t.ptr(), t2.ptr(), zt + 6, 1, 0, none, nullptr, st));
+    } else if (!mob) {
       op.dslash(t, fout_c, 1, 0, st);
       lin(fout_e, op.kappa, t, 1.0, &fin_e);   // out_e = kappa D out_o + in_e
     } else {
@@ -599,12 +655,16 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
 
 int cpsb_matinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
                 cpsb_solve_result *res) {
-  return matinv_impl(h, p, a, out, in, 0, res);
+  return matinv_impl(h, p, a, out, in, 0, false, res);
 }
 
 int cpsb_fmatinv(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *out, const double *in,
                  int dminus, cpsb_solve_result *res) {
-  return matinv_impl(h, p, a, out, in, dminus, res);
+  if (p && p->action == CPSB_ZMOBIUS && dminus == -1) {  // f_zmobius.C:98: out = Dminus(in), no solve
+    if (res) memset(res, 0, sizeof(*res));
+    return cpsb_dminus(h, p, out, in);
+  }
+  return matinv_impl(h, p, a, out, in, dminus, true, res);
 }
 
 int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in) {
@@ -625,23 +685,8 @@ int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const dou
     Field fe(P64, n), fo(P64, n), ge(P64, n), go(P64, n);
     upload(fe, &in_e, 1, n, st);
     upload(fo, &in_o, 1, n, st);
-    if (!zm) {
-      mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
-    } else {
-      // DiracOpZMobius::Dminus (d_op_zmobius.C:1213-1272, zmobius_dminus.C:44-116):
-      // out_x = (c_s/2) D_W in_y - (c_s(4 - M5) - a5_inv) in_x, per slice s
-      Reduce none;
-      memset(&none, 0, sizeof(none));
-      const ZM5Tab *t = (const ZM5Tab *)op.ztab.p;
-      Field th(P64, n);
-      for (int half = 0; half < 2; half++) {
-        const Field &src_other = half ? fo : fe, &src_same = half ? fe : fo;
-        const Field &dst = half ? ge : go;
-        op.hop(th.ptr(), src_other.ptr(), half ? 1 : 0, 0, 1.0, nullptr, nullptr, nullptr, st);
-        CK(launch_m5z(P64, 0, op.geom, dst.ptr(), src_same.ptr(), SpinorPtr{}, t + 11, 0, 0, none, nullptr, st));
-        CK(launch_m5z(P64, 0, op.geom, dst.ptr(), th.ptr(), dst.ptr(), t + 12, 1, 0, none, nullptr, st));
-      }
-    }
+    if (!zm) mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
+    else zmobius_dminus_dev(op, go, ge, fo, fe, st);
     download(&out_e, 1, n, ge, st);
     download(&out_o, 1, n, go, st);
     return CPSB_OK;

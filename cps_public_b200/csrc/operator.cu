@@ -259,7 +259,8 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   //   7 dag1 mix^dag alone            8 dag1 K-weighted H5^dag       9 dag1 -conj(kb) . M5^-dag(.)
   //  10 dag1 conj(kb) . M5^-dag(mix^dag(.))
   //  11 dag0 -(c_s (4 - M5) - a5_inv) .    12 dag0 (c_s / 2) .   (DiracOpZMobius::Dminus)
-  const int NT = 13;
+  //  13 dag0 2 kb .                          (the source scale of Fzmobius::FmatInv)
+  const int NT = 14;
   std::vector<ZM5Tab> t(NT);
   memset(t.data(), 0, sizeof(ZM5Tab) * NT);
   const std::vector<zc_t> zero(ls, zc_t(0.0, 0.0));
@@ -274,8 +275,9 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   for (int s = 0; s < ls; s++) {
     t[11].post[s] = d2(-(op.zc[s] * (4 - pp.m5) - pp.a5_inv));
     t[12].post[s] = d2(0.5 * op.zc[s]);
+    t[13].post[s] = d2(2.0 * kb[s]);
   }
-  t[11].post_on = t[12].post_on = 1;
+  t[11].post_on = t[12].post_on = t[13].post_on = 1;
   for (int s = 0; s < ls; s++) {
     t[0].post[s] = t[4].post[s] = d2(kb[s]);
     t[1].post[s] = d2(-kb[s]);

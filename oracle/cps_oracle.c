@@ -1005,6 +1005,71 @@ int orc_zmobius_dminus(const orc_op *op, double *out, const double *in) {
   return 0;
 }
 
+/* DiracOpZMobius::MatInv(out, in, true_res, PRESERVE_YES), d_op_zmobius.C:829-1080
+ * (ZMOB_PC_SYM2 and ORIG), on full vectors with the solve checkerboard first:
+ *   t = kb . D4(M5^-1 in_2, CHKB_EVEN) + in_1;  SYM2: out_1 = M5 out_1 (guess);
+ *   src = MatPcDag t;  CG;  SYM2: out_1 = M5^-1 out_1;
+ *   out_2 = M5^-1(kb . D4(out_1, CHKB_ODD)) + M5^-1 in_2   (no overall scale).
+ * Returns the CG iteration count; *true_res as InvCg reports it. */
+int orc_zmobius_matinv(const orc_op *op, double *out, const double *in, double stop_rsd, int max_num_iter,
+                       double *true_res) {
+  if (op->action != 2 || (op->mob.pc_type != 2 && op->mob.pc_type != 0)) return -1;
+  const long n = orc_op_size(op);
+  orc_mobius_params p = op->mob;
+  p.mass = op->mass;
+  const int ls = p.ls;
+  const long n4 = n / ls;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(&p, kb, kc, kr);
+  const double *in_1 = in, *in_2 = in + n;
+  double *out_1 = out, *out_2 = out + n;
+  double *t = scratch(n), *t2 = scratch(n), *src = scratch(n);
+  memcpy(t, in_2, n * sizeof(double));
+  orc_mobius_m5inv(t, 0, op->dims, &p);
+  orc_mobius_dslash_4(t2, op->u, t, 0, 0, op->dims, &p);
+  for (int s = 0; s < ls; s++)                                    /* zmobius_zvectTimesV1PlusV2 */
+    for (long i = 0; i < n4 / 2; i++) {
+      const cplx x = {t2[s * n4 + 2 * i], t2[s * n4 + 2 * i + 1]};
+      const cplx r = cmul(kb[s], x);
+      t[s * n4 + 2 * i] = r.re + in_1[s * n4 + 2 * i];
+      t[s * n4 + 2 * i + 1] = r.im + in_1[s * n4 + 2 * i + 1];
+    }
+  if (p.pc_type == 2) {                                           /* SYM2: guess transform */
+    memcpy(t2, out_1, n * sizeof(double));
+    orc_zmobius_dslash_5_plus(out_1, t2, p.mass, 0, op->dims, ls, kr);
+  }
+  orc_matpc(op, src, t, 1);
+  const int it = orc_invcg(op, out_1, src, stop_rsd, max_num_iter, true_res, NULL);
+  if (p.pc_type == 2) orc_mobius_m5inv(out_1, 0, op->dims, &p);
+  orc_mobius_dslash_4(t, op->u, out_1, 1, 0, op->dims, &p);
+  for (int s = 0; s < ls; s++) zscale(t + s * n4, kb[s], n4);    /* zmobius_zvectTimesEquComplex */
+  memcpy(out_2, t, n * sizeof(double));
+  orc_mobius_m5inv(out_2, 0, op->dims, &p);
+  memcpy(t, in_2, n * sizeof(double));
+  orc_mobius_m5inv(t, 0, op->dims, &p);
+  for (long i = 0; i < n; i++) out_2[i] += t[i];                 /* VecAddEquVec */
+  free(t);
+  free(t2);
+  free(src);
+  return it;
+}
+
+/* Fzmobius::FmatInv's source scale (f_zmobius.C:70-130): both halves of a full
+ * vector times 2 kappa_b(s) per slice (vecTimesEquComplex). */
+int orc_zmobius_scale_2kb(const orc_op *op, double *v) {
+  if (op->action != 2) return -1;
+  const long n = orc_op_size(op);
+  orc_mobius_params p = op->mob;
+  p.mass = op->mass;
+  const int ls = p.ls;
+  const long n4 = n / ls;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(&p, kb, kc, kr);
+  for (int h = 0; h < 2; h++)
+    for (int s = 0; s < ls; s++) zscale(v + h * n + s * n4, cscal(2.0, kb[s]), n4);
+  return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* DiracOp::MinResExt, d_op_base/comsrc/minresext.C:32-156             */
 /* ------------------------------------------------------------------ */

@@ -179,6 +179,28 @@ class Op:
         assert rc == 0
         return out
 
+    def zmatinv(self, src_full, guess_full=None, stop_rsd=1e-10, max_iter=5000):
+        """DiracOpZMobius::MatInv on a full vector (solve checkerboard first);
+        returns (solution, iterations, true_res)."""
+        src = np.ascontiguousarray(src_full, np.float64)
+        assert self.action == 2 and src.size == 2 * self.n
+        out = np.zeros(2 * self.n) if guess_full is None else np.array(guess_full, np.float64)
+        tr = C.c_double(0)
+        it = lib().orc_zmobius_matinv(C.byref(self.s), _p(out), _p(src), C.c_double(stop_rsd), max_iter,
+                                      C.byref(tr))
+        assert it >= 0
+        return out, it, tr.value
+
+    def zfmatinv(self, src_full, guess_full=None, dminus=0, stop_rsd=1e-10, max_iter=5000):
+        """Fzmobius::FmatInv (f_zmobius.C:70-130): the source (Dminus of it for
+        dminus = 1) times 2 kappa_b(s), then DiracOpZMobius::MatInv; dminus = -1
+        returns Dminus(source) without a solve (iterations 0)."""
+        if dminus == -1:
+            return self.zdminus(src_full), 0, 0.0
+        src = self.zdminus(src_full) if dminus == 1 else np.array(src_full, np.float64)
+        assert lib().orc_zmobius_scale_2kb(C.byref(self.s), _p(src)) == 0
+        return self.zmatinv(src, guess_full, stop_rsd, max_iter)
+
     def fmatinv(self, src_full, guess_full=None, dminus=0, stop_rsd=1e-10, max_iter=5000):
         """Lattice::FmatInv(..., dminus): Fmobius applies Dminus to the source
         before MatInv (f_mobius.C:45-117); the other actions ignore the flag."""
@@ -209,6 +231,8 @@ def _setup():
     L.orc_minresext.restype = C.c_double
     L.orc_mobius_dminus.restype = C.c_int
     L.orc_zmobius_dminus.restype = C.c_int
+    L.orc_zmobius_matinv.restype = C.c_int
+    L.orc_zmobius_scale_2kb.restype = C.c_int
     L.orc_mdagm.restype = C.c_int
     L.orc_invcg.restype = C.c_int
     L.orc_invcg.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_double), _dp]

@@ -302,10 +302,11 @@ int main(int argc, char **argv) {
     DiracOp *d = 0;
     if (action == 0) d = new DiracOpWilson(lat, fout, fin, &cg_arg, CNV_FRM_NO);
     else if (action == 1) d = new DiracOpDwf(lat, fout, fin, &cg_arg, CNV_FRM_NO);
-    else d = new DiracOpMobius(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+    else if (action == 2) d = new DiracOpMobius(lat, fout, fin, &cg_arg, CNV_FRM_NO);
+    else d = new DiracOpZMobius(lat, fout, fin, &cg_arg, CNV_FRM_NO);  // d_op_zmobius.C:829-1080
     Float true_res = 0;
     double t0 = now_s();
-    d->MatInv(fout, fin, &true_res, PRESERVE_YES);
+    rhdr[0] = d->MatInv(fout, fin, &true_res, PRESERVE_YES);
     rpar[10] = now_s() - t0;
     delete d;
     rpar[0] = true_res;

@@ -247,10 +247,18 @@ def gen_zmobius(name, dims, ls, eps, seed, mass, b, c, pc_type=2):
     for cb, dag in ([(1, 0), (0, 1)] if pc_type == 2 else []):
         _, _, rec[f"d4_cb{cb}_dag{dag}"] = refrun.run(refrun.OP_MOBIUS_D4, "zmobius", dims, u, [src], cb=cb,
                                                       dag=dag, **kw)
+    full, guess = matinv_inputs({"dims": np.array(dims), "ls": ls, "seed": seed})
     if pc_type == 2:  # DiracOpZMobius::Dminus of the full MatInv-fixture source (odd half first)
-        full, _ = matinv_inputs({"dims": np.array(dims), "ls": ls, "seed": seed})
         rec["dminus_src_sha"] = sha(full)
         _, _, rec["dminus_out"] = refrun.run(refrun.OP_DMINUS, "zmobius", dims, u, [full], **kw)
+    if pc_type in (0, 2):  # DiracOpZMobius::MatInv and Fzmobius::FmatInv(dminus = 1) from a nonzero guess
+        rec["matinv_src_sha"], rec["matinv_guess_sha"] = sha(full), sha(guess)
+        it, rp, rec["zmatinv_sol"] = refrun.run(refrun.OP_MATINV, "zmobius", dims, u, [full, guess],
+                                                stop_rsd=1e-10, max_iter=5000, **kw)
+        rec["zmatinv_iters"], rec["zmatinv_true_res"] = it, rp[0]
+        it, rp, rec["zfmatinv_sol"] = refrun.run(refrun.OP_FMATINV, "zmobius", dims, u, [full, guess],
+                                                 stop_rsd=1e-10, max_iter=5000, dminus=1, **kw)
+        rec["zfmatinv_iters"], rec["zfmatinv_true_res"] = it, rp[0]
     _, rp, rec["mdagm"] = refrun.run(refrun.OP_MDAGM, "zmobius", dims, u, [src], **kw)
     rec["mdagm_dot"] = rp[0]
     it, rp, rec["cg_sol"] = refrun.run(refrun.OP_INVCG, "zmobius", dims, u, [src, np.zeros_like(src)],

@@ -317,11 +317,40 @@ def test_zmobius_constant_coefficients_equal_mobius():
 
 
 def test_zmobius_unsupported_forms_refused():
-    """DiracOpZMobius::Dslash (unpreconditioned, full vectors) and MatInv are not
-    built on the device: the ABI says so instead of computing something else."""
+    """DiracOpZMobius::Dslash (unpreconditioned, full vectors) and the SYM1 MatInv
+    (not implemented by CPS either) are not built on the device: the ABI says so
+    instead of computing something else."""
     rec, u, src = load("zmobius_4x4x4x4_ls4")
     op = zmobius_op(rec, u)
     with pytest.raises(Exception, match="unsupported"):
         op.Dslash(src, 0, 0)
+    rec1, u1, src1 = load("zmobius_sym1_4x4x4x4_ls4")
     with pytest.raises(Exception, match="unsupported"):
-        op.MatInv(np.concatenate([src, src]))
+        zmobius_op(rec1, u1).MatInv(np.concatenate([src1, src1]))
+
+
+@pytest.mark.parametrize("name", ["zmobius_4x4x4x4_ls4", "zmobius_orig_4x4x4x4_ls4"])
+@pytest.mark.parametrize("prec", ["F64", "F32"])
+def test_zmobius_matinv_vs_reference(name, prec):
+    """DiracOpZMobius::MatInv and Fzmobius::FmatInv(dminus = 1) on the device
+    against the compiled CPS from a nonzero guess: FP64 within 1e-9 relative
+    (iterations within 1), mixed FP32 within 1e-8, true residual 1e-10; the
+    dminus = -1 form returns Dminus of the source."""
+    import cps_public_b200 as cb
+    from tests.golden.make_golden import matinv_inputs
+    rec, u, src = load(name)
+    op = zmobius_op(rec, u)
+    full, guess = matinv_inputs(rec)
+    P = getattr(cb, prec)
+    tol = 1e-9 if prec == "F64" else 1e-8
+    out, r = op.MatInv(full, guess, stop_rsd=1e-10, precision=P)
+    assert r.status == 0 and r.true_rsd <= 1e-10
+    assert rel(out, rec["zmatinv_sol"]) < tol
+    if prec == "F64":
+        assert abs(r.iters - int(rec["zmatinv_iters"])) <= 1
+    out, r = op.FmatInv(full, guess, dminus=1, stop_rsd=1e-10, precision=P)
+    assert r.status == 0 and r.true_rsd <= 1e-10
+    assert rel(out, rec["zfmatinv_sol"]) < tol
+    if "dminus_out" in rec:
+        out, r = op.FmatInv(full, guess, dminus=-1)
+        assert r.iters == 0 and rel(out, rec["dminus_out"]) < OP_TOL

@@ -176,9 +176,17 @@ def test_zmobius_bitexact(name):
     assert it == int(rec["minvcg_iters"])
     for i in range(len(shifts)):
         np.testing.assert_array_equal(sols[i], rec["minvcg_sol"][i])
+    from tests.golden.make_golden import matinv_inputs
+    from tests.golden_util import sha
+    full, guess = matinv_inputs(rec)
     if "dminus_out" in rec:  # DiracOpZMobius::Dminus
-        from tests.golden.make_golden import matinv_inputs
-        from tests.golden_util import sha
-        full, _ = matinv_inputs(rec)
         assert sha(full) == str(rec["dminus_src_sha"])
         np.testing.assert_array_equal(op.zdminus(full), rec["dminus_out"])
+    if "zmatinv_sol" in rec:  # DiracOpZMobius::MatInv and Fzmobius::FmatInv(dminus = 1)
+        assert sha(full) == str(rec["matinv_src_sha"]) and sha(guess) == str(rec["matinv_guess_sha"])
+        out, it, tr = op.zmatinv(full, guess)
+        np.testing.assert_array_equal(out, rec["zmatinv_sol"])
+        assert it == int(rec["zmatinv_iters"]) and tr == float(rec["zmatinv_true_res"])
+        out, it, tr = op.zfmatinv(full, guess, dminus=1)
+        np.testing.assert_array_equal(out, rec["zfmatinv_sol"])
+        assert it == int(rec["zfmatinv_iters"]) and tr == float(rec["zfmatinv_true_res"])
