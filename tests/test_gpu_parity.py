@@ -293,6 +293,23 @@ def test_zmobius_minvcg_vs_reference(name):
         assert rel(xs[i], rec["minvcg_sol"][i]) < 1e-9
 
 
+@pytest.mark.parametrize("prec", ["F32", "F16"])
+def test_zmobius_minvcg_reduced_precision_refined(prec):
+    """zMobius multishift with FP32 / 16-bit Krylov vectors and per-shift
+    refinement: every shift reaches FP64 true residual 1e-10 and agrees with
+    the FP64 reference solutions within 1e-7."""
+    import cps_public_b200 as cb
+    rec, u, src = load("zmobius_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    shifts = list(rec["minvcg_shifts"])
+    xs, r, rsd = op.MInvCG(src, shifts, [1e-10] * len(shifts), precision=getattr(cb, prec))
+    assert r.status == 0, r.as_dict()
+    for i, sh in enumerate(shifts):
+        ax, _ = op.MatPcDagMatPc(xs[i])
+        assert np.linalg.norm(src - ax - sh * xs[i]) / np.linalg.norm(src) <= 1.5e-10
+        assert rel(xs[i], rec["minvcg_sol"][i]) < 1e-7
+
+
 def test_zmobius_dminus_vs_reference():
     """DiracOpZMobius::Dminus (complex c_s, odd half first) on the device against
     the compiled CPS, FP64, within 1e-13."""
