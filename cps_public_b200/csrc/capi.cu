@@ -547,8 +547,8 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     check_cg(a);
     if (!out || !in || !res) throw Error{CPSB_ERR_ARG, "null vector or result"};
     const bool zm = p->action == CPSB_ZMOBIUS;
-    if (zm && p->pc_type == 1)  // d_op_zmobius.C:929-960: ERR.NotImplemented for the other types
-      throw Error{CPSB_ERR_UNSUPPORTED, "zMobius MatInv: only ZMOB_PC_SYM2 and ZMOB_PC_ORIG"};
+    if (zm && p->pc_type != 0 && p->pc_type != 2 && p->pc_type != 5)  // d_op_zmobius.C:929-1080
+      throw Error{CPSB_ERR_UNSUPPORTED, "zMobius MatInv: ZMOB_PC_SYM2, ORIG and SYM3 only (as the reference)"};
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     const long n = op.nsites();
@@ -591,7 +591,7 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
       CK(launch_m5z(P64, 0, g, t.ptr(), fin_e.ptr(), SpinorPtr{}, zt + 6, 0, 0, none, nullptr, st));
       CK(launch_m5z(P64, 0, g, t2.ptr(), t.ptr(), SpinorPtr{}, zt + 4, 0, 0, none, nullptr, st));
       op.hop(t.ptr(), t2.ptr(), 0, 0, 1.0, &xc, nullptr, nullptr, st);
-      if (p->pc_type == 2) {
+      if (p->pc_type == 2 || p->pc_type == 5) {
         CK(cudaMemcpyAsync(t2.data.p, fout_c.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
         CK(launch_m5z(P64, 0, g, fout_c.ptr(), t2.ptr(), t2.ptr(), zt + 5, 1, 0, none, nullptr, st));
       }
@@ -622,8 +622,8 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     const int rc = s->solve(*a, res, st);
     CK(cudaMemcpyAsync(fout_c.data.p, s->x64.data.p, fout_c.data.bytes, cudaMemcpyDeviceToDevice, st));
     if (zm) {
-      // SYM2: out_o = M5^-1 out_o; out_e = M5^-1(kb . D4(out_o, CHKB_ODD)) + M5^-1 in_e
-      if (p->pc_type == 2) {
+      // SYM2 / SYM3: out_o = M5^-1 out_o; out_e = M5^-1(kb . D4(out_o, CHKB_ODD)) + M5^-1 in_e
+      if (p->pc_type == 2 || p->pc_type == 5) {
         CK(launch_m5z(P64, 0, g, t.ptr(), fout_c.ptr(), SpinorPtr{}, zt + 6, 0, 0, none, nullptr, st));
         CK(cudaMemcpyAsync(fout_c.data.p, t.data.p, t.data.bytes, cudaMemcpyDeviceToDevice, st));
       }

@@ -239,8 +239,8 @@ static void zmobius_mix(ZM5Tab &t, int dag, int ls, double m, const zc_t *b, con
 
 static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   const int ls = op.geom.ls;
-  if (pp.pc_type < 0 || pp.pc_type > 2)
-    throw Error{CPSB_ERR_UNSUPPORTED, "zMobius preconditioners: ZMOB_PC_ORIG (0), ZMOB_PC_SYM1 (1), ZMOB_PC_SYM2 (2)"};
+  if (pp.pc_type < 0 || pp.pc_type > 5)
+    throw Error{CPSB_ERR_UNSUPPORTED, "zMobius preconditioners: ZMOB_PC_ORIG .. ZMOB_PC_SYM3 (0 .. 5)"};
   if (!pp.zmobius_b || !pp.zmobius_c) throw Error{CPSB_ERR_ARG, "zMobius needs zmobius_b and zmobius_c"};
   op.zb.resize(ls);
   op.zc.resize(ls);
@@ -260,14 +260,31 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
   //  10 dag1 conj(kb) . M5^-dag(mix^dag(.))
   //  11 dag0 -(c_s (4 - M5) - a5_inv) .    12 dag0 (c_s / 2) .   (DiracOpZMobius::Dminus)
   //  13 dag0 2 kb .                          (the source scale of Fzmobius::FmatInv)
-  const int NT = 14;
+  //  MIT preconditioners (zmobius_B_MIT / zmobius_Binv_MIT, d_op_zmobius.C:132-238, f = c/b):
+  //  14 dag0 B = b . (1 + f H5)   15 dag1 B^dag = (1 + f H5)^dag conj(b) .
+  //  16 dag0 B^-1 = M5^-1[K = f] (1/b .)   17 dag1 B^-dag = 1/conj(b) . M5^-dag[K = f]
+  //  18 dag0 mix(M5^-1 .) without a scale (SYM3)
+  const int NT = 19;
   std::vector<ZM5Tab> t(NT);
   memset(t.data(), 0, sizeof(ZM5Tab) * NT);
   const std::vector<zc_t> zero(ls, zc_t(0.0, 0.0));
-  auto dag_of = [](int k) { return (k == 0 || k == 1 || k == 4 || k == 5 || k == 6 || k >= 11) ? 0 : 1; };
+  auto dag_of = [](int k) {
+    return (k == 0 || k == 1 || k == 4 || k == 5 || k == 6 || k == 11 || k == 12 || k == 13 || k == 14 || k == 16 ||
+            k == 18) ? 0 : 1;
+  };
+  std::vector<zc_t> fact(ls), one(ls, zc_t(1.0, 0.0));
+  for (int s = 0; s < ls; s++) fact[s] = op.zc[s] / op.zb[s];
   for (int k = 0; k < NT; k++) {
     const int dag = dag_of(k);
-    if (k >= 11) continue;  // scale-only tables
+    if (k >= 11 && k <= 13) continue;  // scale-only tables
+    if (k == 14 || k == 15) {  // B, B^dag: mixing 1 + f H5
+      zmobius_mix(t[k], dag, ls, pp.mass, one.data(), fact.data());
+      continue;
+    }
+    if (k == 16 || k == 17) {  // B^-1, B^-dag: sweeps with K = f
+      zmobius_sweeps(t[k], dag, ls, pp.mass, fact.data());
+      continue;
+    }
     if (k != 4 && k != 5 && k != 7 && k != 8) zmobius_sweeps(t[k], dag, ls, pp.mass, K.data());
     if (k == 5 || k == 8) zmobius_mix(t[k], dag, ls, pp.mass, zero.data(), K.data());
     else if (k != 6 && k != 9) zmobius_mix(t[k], dag, ls, pp.mass, op.zb.data(), op.zc.data());
@@ -276,8 +293,13 @@ static void zmobius_setup(Operator &op, const cpsb_dirac_params &pp) {
     t[11].post[s] = d2(-(op.zc[s] * (4 - pp.m5) - pp.a5_inv));
     t[12].post[s] = d2(0.5 * op.zc[s]);
     t[13].post[s] = d2(2.0 * kb[s]);
+    t[14].post[s] = d2(op.zb[s]);
+    t[15].pre[s] = d2(std::conj(op.zb[s]));
+    t[16].pre[s] = d2(1.0 / op.zb[s]);
+    t[17].post[s] = d2(1.0 / std::conj(op.zb[s]));
   }
   t[11].post_on = t[12].post_on = t[13].post_on = 1;
+  t[14].post_on = t[15].pre_on = t[16].pre_on = t[17].post_on = 1;
   for (int s = 0; s < ls; s++) {
     t[0].post[s] = t[4].post[s] = d2(kb[s]);
     t[1].post[s] = d2(-kb[s]);
@@ -504,6 +526,55 @@ void Operator::matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag,
   const Reduce rd = red ? *red : none;
   const int nr = red != nullptr;
   const int pc = p.pc_type;
+  if (pc >= 3) {
+    // SYM1_MIT (zmobius_m-sym1-MIT.h):  in + B M5^-1 (-kb) D4(0) M5^-1 kb D4(1) B^-1 in
+    // SYM2_MIT (zmobius_m-sym2-MIT.h):  in + B (-kb) D4(0) M5^-1 kb D4(1) M5^-1 B^-1 in
+    // SYM3 (zmobius_m-sym3.h):          in + D4(0) M5^-1 D4(1) M5^-1 in
+    // and their adjoints (the mdag files), D4 = hop . mix, D4^dag = mix^dag . hop^dag.
+    if (!dag) {
+      if (pc == 5) {
+        CK(launch_m5z(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, t + 18, 0, 0, none, skip, st));
+        hop(t3.ptr(), t1.ptr(), 1, 0, 1.0, nullptr, nullptr, skip, st);
+        CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 18, 0, 0, none, skip, st));
+        hop(out, t1.ptr(), 0, 0, 1.0, &in, red, skip, st);
+        return;
+      }
+      CK(launch_m5z(prec, 0, geom, t3.ptr(), in, SpinorPtr{}, t + 16, 0, 0, none, skip, st));
+      CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + (pc == 3 ? 4 : 0), 0, 0, none, skip, st));
+      hop(t3.ptr(), t1.ptr(), 1, 0, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 1, 0, 0, none, skip, st));
+      hop(t3.ptr(), t1.ptr(), 0, 0, 1.0, nullptr, nullptr, skip, st);
+      if (pc == 3) {
+        CK(launch_m5z(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 6, 0, 0, none, skip, st));
+        CK(launch_m5z(prec, 0, geom, out, t1.ptr(), in, t + 14, 1, nr, rd, skip, st));
+      } else {
+        CK(launch_m5z(prec, 0, geom, out, t3.ptr(), in, t + 14, 1, nr, rd, skip, st));
+      }
+      return;
+    }
+    if (pc == 5) {
+      hop(t1.ptr(), in, 1, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 3, 0, 0, none, skip, st));
+      hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, out, t1.ptr(), in, t + 3, 1, nr, rd, skip, st));
+      return;
+    }
+    CK(launch_m5z(prec, 1, geom, t3.ptr(), in, SpinorPtr{}, t + 15, 0, 0, none, skip, st));
+    if (pc == 3) {
+      CK(launch_m5z(prec, 1, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 9, 0, 0, none, skip, st));
+      hop(t3.ptr(), t1.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 10, 0, 0, none, skip, st));
+      hop(t3.ptr(), t1.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, t + 7, 0, 0, none, skip, st));
+    } else {
+      hop(t1.ptr(), t3.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 2, 0, 0, none, skip, st));
+      hop(t1.ptr(), t3.ptr(), 0, 1, 1.0, nullptr, nullptr, skip, st);
+      CK(launch_m5z(prec, 1, geom, t3.ptr(), t1.ptr(), SpinorPtr{}, t + 3, 0, 0, none, skip, st));
+    }
+    CK(launch_m5z(prec, 1, geom, out, pc == 3 ? t1.ptr() : t3.ptr(), in, t + 17, 1, nr, rd, skip, st));
+    return;
+  }
   if (!dag) {
     // SYM2 (zmobius_m-sym2.h): in - kb D4(0) M5^-1 kb D4(1) M5^-1 in
     // ORIG (zmobius_m-orig.h): in - kb D4(0) M5^-1 kb D4(1) in + K H5 in

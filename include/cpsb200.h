@@ -49,8 +49,10 @@ typedef struct cpsb_gauge_s *cpsb_gauge;
  *   mobius_b, mobius_c   GJP.Mobius_b/c() (gjp.h:594-601)
  *   pc_type GJP.ZMobius_PC_Type() (include/util/dwf.h:42-48): ZMOB_PC_ORIG (0),
  *           ZMOB_PC_SYM1 (1) and ZMOB_PC_SYM2 (2, the CPS default, src/util/gjp/
- *           gjp.C:129) are implemented for Mobius, SYM2 for zMobius; the MIT and
- *           SYM3 forms return CPSB_ERR_UNSUPPORTED.
+ *           gjp.C:129) for Mobius; for zMobius also ZMOB_PC_SYM1_MIT (3),
+ *           ZMOB_PC_SYM2_MIT (4) and ZMOB_PC_SYM3 (5).  Other values (and the MIT
+ *           and SYM3 forms for real Mobius, where the reference reads empty
+ *           zMobius coefficient arrays) return CPSB_ERR_UNSUPPORTED.
  *   zmobius_b, zmobius_c   zMobius (CPSB_ZMOBIUS) only: the complex per-slice
  *           coefficients b_s, c_s as ls (re, im) pairs each, the layout of
  *           DoArgExt::zmobius_b_coeff / zmobius_c_coeff (GJP.ZMobius_b/c(),

@@ -412,12 +412,19 @@ void orc_mobius_dslash_4(double *out, const double *u, const double *in, int cb,
 
 /* zmobius_m5inv.C:247-400 (dag 0) and :534-686 (dag 1): in-place exact M5^-1
  * by a forward and a backward sweep along s with the wall correction. */
+static void m5inv_k(double *io, int dag, const int *dims, const orc_mobius_params *p, const cplx *K);
 void orc_mobius_m5inv(double *io, int dag, const int *dims, const orc_mobius_params *p) {
+  cplx kb[64], kc[64], K[64];
+  mobius_kappas(p, kb, kc, K);
+  m5inv_k(io, dag, dims, p, K);
+}
+
+/* zmobius_m5inv with the hopping ratios K[s] given (kappa_ratio, or c_s/b_s for
+ * the MIT preconditioners' B^-1). */
+static void m5inv_k(double *io, int dag, const int *dims, const orc_mobius_params *p, const cplx *K) {
   const int ls = p->ls;
   const long v = (long)dims[0] * dims[1] * dims[2] * dims[3] / 2;
   const double mass = p->mass;
-  cplx kb[64], kc[64], K[64];
-  mobius_kappas(p, kb, kc, K);
 #define F(x, s) (io + 24 * ((x) + v * (long)(s)))
   if (!dag) {
     cplx prod = {1.0, 0.0};
@@ -592,13 +599,174 @@ static void mobius_mdag_sym1(double *out, const double *u, const double *in, con
   free(t2);
 }
 
+/* zmobius_B_MIT / zmobius_Binv_MIT (d_op_zmobius.C:132-238), fact_s = c_s / b_s:
+ *   B   dag 0: v = b_s (v + fact-H5 v);        dag 1: v = conj(b_s) v + fact-H5^dag(conj(b) v)
+ *   B^-1 dag 0: v = M5^-1[K = fact](v / b_s);  dag 1: v = M5^-dag[K = fact](v) / conj(b_s) */
+static void b_mit(double *v, int dag, const int *dims, const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx b[64], c[64], fact[64];
+  for (int s = 0; s < ls; s++) {
+    b[s].re = p->b[s][0]; b[s].im = p->b[s][1];
+    c[s].re = p->c[s][0]; c[s].im = p->c[s][1];
+    fact[s] = cdiv(c[s], b[s]);
+  }
+  double *t = scratch(n * ls);
+  if (!dag) {
+    memcpy(t, v, sizeof(double) * n * ls);
+    orc_zmobius_dslash_5_plus(v, t, p->mass, 0, dims, ls, fact);
+    for (int s = 0; s < ls; s++) zscale(v + s * n, b[s], n);
+  } else {
+    memcpy(t, v, sizeof(double) * n * ls);
+    for (int s = 0; s < ls; s++) zscale(t + s * n, cconj(b[s]), n);
+    memcpy(v, t, sizeof(double) * n * ls);
+    orc_zmobius_dslash_5_plus(v, t, p->mass, 1, dims, ls, fact);
+  }
+  free(t);
+}
+static void binv_mit(double *v, int dag, const int *dims, const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx b[64], fact[64];
+  const cplx one = {1.0, 0.0};
+  for (int s = 0; s < ls; s++) {
+    cplx c = {p->c[s][0], p->c[s][1]};
+    b[s].re = p->b[s][0]; b[s].im = p->b[s][1];
+    fact[s] = cdiv(c, b[s]);
+  }
+  if (!dag) {
+    for (int s = 0; s < ls; s++) zscale(v + s * n, cdiv(one, b[s]), n);
+    m5inv_k(v, 0, dims, p, fact);
+  } else {
+    m5inv_k(v, 1, dims, p, fact);
+    for (int s = 0; s < ls; s++) zscale(v + s * n, cdiv(one, cconj(b[s])), n);
+  }
+}
+
+/* zmobius_m-sym1-MIT.h / zmobius_mdag-sym1-MIT.h */
+static void mobius_m_sym1_mit(double *out, const double *u, const double *in, const int *dims,
+                              const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(t2, in, sizeof(double) * n * ls);
+  binv_mit(t2, 0, dims, p);
+  orc_mobius_dslash_4(out, u, t2, 1, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, kb[s], n);
+  orc_mobius_m5inv(out, 0, dims, p);
+  orc_mobius_dslash_4(t2, u, out, 0, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cneg(kb[s]), n);
+  orc_mobius_m5inv(t2, 0, dims, p);
+  b_mit(t2, 0, dims, p);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (long i = 0; i < n * ls; i++) out[i] += t2[i];
+  free(t2);
+}
+static void mobius_mdag_sym1_mit(double *out, const double *u, const double *in, const int *dims,
+                                 const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(out, in, sizeof(double) * n * ls);
+  b_mit(out, 1, dims, p);
+  orc_mobius_m5inv(out, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, cneg(cconj(kb[s])), n);
+  orc_mobius_dslash_4(t2, u, out, 1, 1, dims, p);
+  orc_mobius_m5inv(t2, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cconj(kb[s]), n);
+  orc_mobius_dslash_4(out, u, t2, 0, 1, dims, p);
+  binv_mit(out, 1, dims, p);
+  for (long i = 0; i < n * ls; i++) out[i] += in[i];
+  free(t2);
+}
+
+/* zmobius_m-sym2-MIT.h / zmobius_mdag-sym2-MIT.h */
+static void mobius_m_sym2_mit(double *out, const double *u, const double *in, const int *dims,
+                              const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(t2, in, sizeof(double) * n * ls);
+  binv_mit(t2, 0, dims, p);
+  orc_mobius_m5inv(t2, 0, dims, p);
+  orc_mobius_dslash_4(out, u, t2, 1, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, kb[s], n);
+  orc_mobius_m5inv(out, 0, dims, p);
+  orc_mobius_dslash_4(t2, u, out, 0, 0, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cneg(kb[s]), n);
+  b_mit(t2, 0, dims, p);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (long i = 0; i < n * ls; i++) out[i] += t2[i];
+  free(t2);
+}
+static void mobius_mdag_sym2_mit(double *out, const double *u, const double *in, const int *dims,
+                                 const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  cplx kb[64], kc[64], kr[64];
+  mobius_kappas(p, kb, kc, kr);
+  double *t2 = scratch(n * ls);
+  memcpy(out, in, sizeof(double) * n * ls);
+  b_mit(out, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(out + s * n, cneg(cconj(kb[s])), n);
+  orc_mobius_dslash_4(t2, u, out, 1, 1, dims, p);
+  orc_mobius_m5inv(t2, 1, dims, p);
+  for (int s = 0; s < ls; s++) zscale(t2 + s * n, cconj(kb[s]), n);
+  orc_mobius_dslash_4(out, u, t2, 0, 1, dims, p);
+  orc_mobius_m5inv(out, 1, dims, p);
+  binv_mit(out, 1, dims, p);
+  for (long i = 0; i < n * ls; i++) out[i] += in[i];
+  free(t2);
+}
+
+/* zmobius_m-sym3.h / zmobius_mdag-sym3.h.  The reference scales GJP's b, c by
+ * kappa_b i around its D4 calls, but zmobius_dslash_4 reads the DiracOp's own
+ * copies (zmobius_dslash_4.C:61-62), so the operator it applies is
+ *   M = 1 + D4(0) M5^-1 D4(1) M5^-1,  M^dag = 1 + M5^-dag D4^dag(0) M5^-dag D4^dag(1). */
+static void mobius_m_sym3(double *out, const double *u, const double *in, const int *dims,
+                          const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  double *t2 = scratch(n * ls);
+  memcpy(t2, in, sizeof(double) * n * ls);
+  orc_mobius_m5inv(t2, 0, dims, p);
+  orc_mobius_dslash_4(out, u, t2, 1, 0, dims, p);
+  orc_mobius_m5inv(out, 0, dims, p);
+  orc_mobius_dslash_4(t2, u, out, 0, 0, dims, p);
+  memcpy(out, in, sizeof(double) * n * ls);
+  for (long i = 0; i < n * ls; i++) out[i] += t2[i];
+  free(t2);
+}
+static void mobius_mdag_sym3(double *out, const double *u, const double *in, const int *dims,
+                             const orc_mobius_params *p) {
+  const int ls = p->ls;
+  const long n = 24L * dims[0] * dims[1] * dims[2] * dims[3] / 2;
+  double *t2 = scratch(n * ls);
+  memcpy(out, in, sizeof(double) * n * ls);
+  orc_mobius_dslash_4(t2, u, out, 1, 1, dims, p);
+  orc_mobius_m5inv(t2, 1, dims, p);
+  orc_mobius_dslash_4(out, u, t2, 0, 1, dims, p);
+  orc_mobius_m5inv(out, 1, dims, p);
+  for (long i = 0; i < n * ls; i++) out[i] += in[i];
+  free(t2);
+}
+
 /* mobius_m.C:28-42 -> zmobius_m.C:40-74 (pc dispatch); mobius_mdag.C:35-55. */
 int orc_mobius_m(double *out, const double *u, const double *in, int dag, const int *dims,
                  const orc_mobius_params *p) {
-  switch (p->pc_type) {  /* ZMOB_PC_ORIG, ZMOB_PC_SYM1, ZMOB_PC_SYM2 (util/dwf.h:42-48) */
+  switch (p->pc_type) {  /* ZMOB_PC_ORIG, SYM1, SYM2, SYM1_MIT, SYM2_MIT, SYM3 (util/dwf.h:42-48) */
     case 0: if (dag) mobius_mdag_orig(out, u, in, dims, p); else mobius_m_orig(out, u, in, dims, p); return 0;
     case 1: if (dag) mobius_mdag_sym1(out, u, in, dims, p); else mobius_m_sym1(out, u, in, dims, p); return 0;
     case 2: if (dag) mobius_mdag_sym2(out, u, in, dims, p); else mobius_m_sym2(out, u, in, dims, p); return 0;
+    case 3: if (dag) mobius_mdag_sym1_mit(out, u, in, dims, p); else mobius_m_sym1_mit(out, u, in, dims, p); return 0;
+    case 4: if (dag) mobius_mdag_sym2_mit(out, u, in, dims, p); else mobius_m_sym2_mit(out, u, in, dims, p); return 0;
+    case 5: if (dag) mobius_mdag_sym3(out, u, in, dims, p); else mobius_m_sym3(out, u, in, dims, p); return 0;
     default: return -1;
   }
 }
@@ -1013,7 +1181,7 @@ int orc_zmobius_dminus(const orc_op *op, double *out, const double *in) {
  * Returns the CG iteration count; *true_res as InvCg reports it. */
 int orc_zmobius_matinv(const orc_op *op, double *out, const double *in, double stop_rsd, int max_num_iter,
                        double *true_res) {
-  if (op->action != 2 || (op->mob.pc_type != 2 && op->mob.pc_type != 0)) return -1;
+  if (op->action != 2 || (op->mob.pc_type != 2 && op->mob.pc_type != 0 && op->mob.pc_type != 5)) return -1;
   const long n = orc_op_size(op);
   orc_mobius_params p = op->mob;
   p.mass = op->mass;
@@ -1034,13 +1202,14 @@ int orc_zmobius_matinv(const orc_op *op, double *out, const double *in, double s
       t[s * n4 + 2 * i] = r.re + in_1[s * n4 + 2 * i];
       t[s * n4 + 2 * i + 1] = r.im + in_1[s * n4 + 2 * i + 1];
     }
-  if (p.pc_type == 2) {                                           /* SYM2: guess transform */
+  const int sym23 = p.pc_type == 2 || p.pc_type == 5;
+  if (sym23) {                                                    /* SYM2 / SYM3: guess transform */
     memcpy(t2, out_1, n * sizeof(double));
     orc_zmobius_dslash_5_plus(out_1, t2, p.mass, 0, op->dims, ls, kr);
   }
   orc_matpc(op, src, t, 1);
   const int it = orc_invcg(op, out_1, src, stop_rsd, max_num_iter, true_res, NULL);
-  if (p.pc_type == 2) orc_mobius_m5inv(out_1, 0, op->dims, &p);
+  if (sym23) orc_mobius_m5inv(out_1, 0, op->dims, &p);
   orc_mobius_dslash_4(t, op->u, out_1, 1, 0, op->dims, &p);
   for (int s = 0; s < ls; s++) zscale(t + s * n4, kb[s], n4);    /* zmobius_zvectTimesEquComplex */
   memcpy(out_2, t, n * sizeof(double));

@@ -221,7 +221,11 @@ def main_pc():
 # complex Gaussian z, z' from the case seed), SYM2
 ZMOBIUS_CASES = [("zmobius_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 37, 0.04, 1.5, 0.5),
                  ("zmobius_orig_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 38, 0.04, 1.5, 0.5, 0),
-                 ("zmobius_sym1_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 39, 0.04, 1.5, 0.5, 1)]
+                 ("zmobius_sym1_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 39, 0.04, 1.5, 0.5, 1),
+                 # ZMOB_PC_SYM1_MIT (3), SYM2_MIT (4), SYM3 (5): operators and CG only
+                 ("zmobius_sym1mit_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 40, 0.04, 1.5, 0.5, 3),
+                 ("zmobius_sym2mit_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 41, 0.04, 1.5, 0.5, 4),
+                 ("zmobius_sym3_4x4x4x4_ls4", (4, 4, 4, 4), 4, 0.2, 42, 0.04, 1.5, 0.5, 5)]
 
 
 def zmobius_coefficients(ls, seed, b, c):
@@ -264,6 +268,8 @@ def gen_zmobius(name, dims, ls, eps, seed, mass, b, c, pc_type=2):
     it, rp, rec["cg_sol"] = refrun.run(refrun.OP_INVCG, "zmobius", dims, u, [src, np.zeros_like(src)],
                                        stop_rsd=1e-10, max_iter=5000, **kw)
     rec["cg_iters"], rec["cg_true_res"] = it, rp[0]
+    if pc_type >= 3:
+        return rec
     ns = 2
     it, rp, r = refrun.run(refrun.OP_MINVCG, "zmobius", dims, u, [src], shifts=SHIFTS[:ns],
                            extra=[np.full(ns, 1e-9), np.ones(ns)], max_iter=5000, **kw)

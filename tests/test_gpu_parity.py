@@ -238,6 +238,10 @@ def test_fmatinv_dminus_ignored_outside_mobius():
 
 
 ZMOBIUS_CASES = ["zmobius_4x4x4x4_ls4", "zmobius_orig_4x4x4x4_ls4", "zmobius_sym1_4x4x4x4_ls4"]
+# SYM1_MIT, SYM2_MIT, SYM3 (operators and CG only).  The reference's SYM3 CG drifts
+# at rounding level (its GJP coefficients are scaled and unscaled around every
+# call), so its iteration count is compared within 20.
+ZMOBIUS_MORE = ["zmobius_sym1mit_4x4x4x4_ls4", "zmobius_sym2mit_4x4x4x4_ls4", "zmobius_sym3_4x4x4x4_ls4"]
 
 
 def zmobius_op(rec, u):
@@ -248,7 +252,7 @@ def zmobius_op(rec, u):
                       bs=list(rec["zb"]), cs=list(rec["zc"]), pc_type=int(rec.get("pc_type", 2)))
 
 
-@pytest.mark.parametrize("name", ZMOBIUS_CASES)
+@pytest.mark.parametrize("name", ZMOBIUS_CASES + ZMOBIUS_MORE)
 def test_zmobius_operators_vs_reference(name):
     """zMobius (complex b_s, c_s; SYM2, ORIG, SYM1) MatPc, MatPcDag and
     MatPcDagMatPc on the device against the compiled CPS DiracOpZMobius, FP64,
@@ -371,3 +375,33 @@ def test_zmobius_matinv_vs_reference(name, prec):
     if "dminus_out" in rec:
         out, r = op.FmatInv(full, guess, dminus=-1)
         assert r.iters == 0 and rel(out, rec["dminus_out"]) < OP_TOL
+
+
+@pytest.mark.parametrize("name", ZMOBIUS_MORE)
+def test_zmobius_more_cg_vs_reference(name):
+    """FP64 CG with the SYM1_MIT, SYM2_MIT and SYM3 preconditioners against the
+    compiled CPS (solution within 1e-9; iterations within 1, SYM3 within 20)."""
+    import cps_public_b200 as cb
+    rec, u, src = load(name)
+    op = zmobius_op(rec, u)
+    x, r = op.InvCg(src, stop_rsd=1e-10, max_num_iter=10000, precision=cb.F64)
+    assert r.status == 0 and r.true_rsd <= 1e-10, r.as_dict()
+    tol_it = 20 if int(rec["pc_type"]) == 5 else 1
+    assert abs(r.iters - int(rec["cg_iters"])) <= tol_it, (r.iters, int(rec["cg_iters"]))
+    assert rel(x, rec["cg_sol"]) < 1e-9
+
+
+def test_zmobius_sym3_matinv_vs_oracle():
+    """DiracOpZMobius::MatInv with SYM3 (handled like SYM2 by the reference) on the
+    device against the oracle's restatement, FP64, within 1e-9."""
+    from oracle import oracle
+    from tests.golden.make_golden import matinv_inputs
+    rec, u, src = load("zmobius_sym3_4x4x4x4_ls4")
+    op = zmobius_op(rec, u)
+    full, guess = matinv_inputs(rec)
+    ref = oracle.Op("mobius", tuple(rec["dims"]), u, ls=int(rec["ls"]), mass=float(rec["mass"]),
+                    m5=float(rec["m5"]), bs=list(rec["zb"]), cs=list(rec["zc"]), pc_type=5)
+    want, it, tr = ref.zmatinv(full, guess, 1e-10, 10000)
+    out, r = op.MatInv(full, guess, stop_rsd=1e-10, max_num_iter=10000)
+    assert r.status == 0 and r.true_rsd <= 1e-10
+    assert rel(out, want) < 1e-9
