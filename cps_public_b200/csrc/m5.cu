@@ -40,16 +40,9 @@ __device__ __forceinline__ void ld_chunk<P32>(const SpinorPtr &f, long i, int k,
   v[0] = mk(a.x, a.z);
   v[1] = mk(a.y, a.w);
 }
-// chunk j = 3p + c: words 2j (Re) and 2j+1 (Im) of the site, both spins each
-template <>
-__device__ __forceinline__ void ld_chunk<P16>(const SpinorPtr &f, long i, int j, cplx<float> *v) {
-  const uint2 w = __ldg((const uint2 *)((const uint4 *)f.data + (long)(j >> 1) * f.stride + i) + (j & 1));
-  const float q = __ldg(f.norm + i);
-  v[0] = mk(dec16(w.x, 0) * q, dec16(w.y, 0) * q);
-  v[1] = mk(dec16(w.x, 1) * q, dec16(w.y, 1) * q);
-}
-// A 16-bit column of Ls slices: all raw loads issued first, then decoded, so
-// the Ls loads are in flight together.
+// A 16-bit column of Ls slices, chunk j = 3p + c (words 2j (Re) and 2j+1 (Im)
+// of each site, both spins in each word): all raw loads issued first, then
+// decoded, so the Ls loads are in flight together.
 template <int LS>
 __device__ __forceinline__ void ld_column16(const SpinorPtr &f, long base, long step, int j, cplx<float> (&v)[LS][2]) {
   uint2 w[LS];
