@@ -1,0 +1,75 @@
+"""Properties of the operators that hold independently of any golden vector,
+checked on the C oracle (CPU): MatPcDag is the adjoint of MatPc and
+MatPcDagMatPc is Hermitian and positive, for every action and every
+preconditioner; zMobius with constant coefficients is Mobius; Dminus is
+linear.  Tolerances are rounding level (1e-13 relative)."""
+import numpy as np
+import pytest
+
+from cps_public_b200 import fields
+from oracle import oracle
+
+DIMS = (4, 4, 4, 4)
+ZB = [1.5 + 0.3j, 1.4 - 0.2j, 1.6 + 0.1j, 1.5 - 0.05j]
+ZC = [0.5 - 0.1j, 0.45 + 0.2j, 0.55, 0.5 + 0.05j]
+
+
+def cdot(a, b):
+    """conj(a) . b over complex pairs."""
+    a = a.reshape(-1, 2)
+    b = b.reshape(-1, 2)
+    return complex(np.sum(a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1]), np.sum(a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]))
+
+
+def make(kind):
+    u = fields.random_gauge(DIMS, 0.2, 7)
+    action, pc = kind
+    if action == "wilson":
+        return oracle.Op("wilson", DIMS, u, mass=0.1)
+    if action == "dwf":
+        return oracle.Op("dwf", DIMS, u, ls=4, mass=0.05)
+    if action == "mobius":
+        return oracle.Op("mobius", DIMS, u, ls=4, mass=0.05, pc_type=pc)
+    return oracle.Op("mobius", DIMS, u, ls=4, mass=0.05, pc_type=pc, bs=ZB, cs=ZC)
+
+
+KINDS = [("wilson", 2), ("dwf", 2)] + [("mobius", pc) for pc in (0, 1, 2)] + [("zmobius", pc) for pc in range(6)]
+
+
+@pytest.mark.parametrize("kind", KINDS, ids=[f"{a}-pc{p}" for a, p in KINDS])
+def test_matpcdag_is_adjoint_and_mdagm_hermitian_positive(kind):
+    op = make(kind)
+    n = op.n // 24
+    x, y = fields.random_source(n, 1), fields.random_source(n, 2)
+    lhs, rhs = cdot(y, op.matpc(x, 0)), cdot(op.matpc(y, 1), x)
+    assert abs(lhs - rhs) <= 1e-13 * abs(lhs)
+    ax, dot = op.mdagm(x)
+    ay, _ = op.mdagm(y)
+    assert abs(cdot(x, ay) - cdot(ax, y)) <= 1e-13 * abs(cdot(x, ay))
+    xax = cdot(x, ax)
+    assert xax.real > 0 and abs(xax.imag) <= 1e-13 * xax.real
+    # the fused norm is |MatPc x|^2
+    mx = op.matpc(x, 0)
+    assert abs(dot - float(mx @ mx)) <= 1e-13 * dot
+
+
+@pytest.mark.parametrize("pc", [0, 1, 2])
+def test_zmobius_constant_coefficients_are_mobius(pc):
+    u = fields.random_gauge(DIMS, 0.2, 8)
+    m = oracle.Op("mobius", DIMS, u, ls=4, mass=0.05, b=1.5, c=0.5, pc_type=pc)
+    z = oracle.Op("mobius", DIMS, u, ls=4, mass=0.05, pc_type=pc, bs=[1.5] * 4, cs=[0.5] * 4)
+    x = fields.random_source(m.n // 24, 3)
+    a, da = m.mdagm(x)
+    b, db = z.mdagm(x)
+    assert np.linalg.norm(a - b) <= 1e-14 * np.linalg.norm(a) and abs(da - db) <= 1e-14 * da
+
+
+@pytest.mark.parametrize("action", ["mobius", "zmobius"])
+def test_dminus_is_linear(action):
+    op = make((action, 2))
+    n = 2 * (op.n // 24)
+    x, y = fields.random_source(n, 4), fields.random_source(n, 5)
+    f = op.dminus if action == "mobius" else op.zdminus
+    lhs = f(0.7 * x - 1.3 * y)
+    rhs = 0.7 * f(x) - 1.3 * f(y)
+    assert np.linalg.norm(lhs - rhs) <= 1e-13 * np.linalg.norm(rhs)
