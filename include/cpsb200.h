@@ -149,7 +149,14 @@ int cpsb_invcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg
  * x[0].  rsd[s]: stop_rsd per shift on entry; on return the residual reported
  * per shift.  With a->precision != F64 the Krylov vectors are kept in that
  * precision and every shift is then refined by mixed-precision CG to its
- * tolerance with an FP64 true residual (rsd[s] then holds that true residual). */
+ * tolerance with an FP64 true residual (rsd[s] then holds that true residual).
+ * CPS's third type, GENERAL (2, include/alg/enum_int.h:236: start from the
+ * guess in x[0], minvcg.C:125-129), has no caller in CPS and returns
+ * CPSB_ERR_UNSUPPORTED.  Its first solution update subtracts bs[s]*chi where
+ * the recurrence needs bs[s]*r (minvcg.C:174-184).  Replayed on a small SPD
+ * system with a nonzero guess, every shift ends at relative residual ~1, not the
+ * tolerance.  With bs[s]*r, shift 0 converges, but the other shifts still stop
+ * short: one guess breaks the collinearity of their residuals with r. */
 int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double **x, const double *b,
                 const double *shift, int nshift, double *rsd, int type, const double *alpha,
                 cpsb_solve_result *res);
