@@ -2,7 +2,10 @@
 checked on the C oracle (CPU): MatPcDag is the adjoint of MatPc and
 MatPcDagMatPc is Hermitian and positive, for every action and every
 preconditioner; zMobius with constant coefficients is Mobius; Dminus is
-linear.  Tolerances are rounding level (1e-13 relative)."""
+linear (tolerances at rounding level, 1e-13 relative).  The solvers solve:
+InvCg's solution meets its tolerance against an independently formed
+residual, MInvCG's MULTI solutions each solve their shifted system, and SINGLE
+returns the alpha-weighted sum of the MULTI solutions."""
 import numpy as np
 import pytest
 
@@ -73,3 +76,34 @@ def test_dminus_is_linear(action):
     lhs = f(0.7 * x - 1.3 * y)
     rhs = 0.7 * f(x) - 1.3 * f(y)
     assert np.linalg.norm(lhs - rhs) <= 1e-13 * np.linalg.norm(rhs)
+
+
+def shifted_residual(op, x, b, shift):
+    ax, _ = op.mdagm(x)
+    return np.linalg.norm(ax + shift * x - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("kind", [("wilson", 2), ("dwf", 2), ("mobius", 2), ("zmobius", 2)], ids=lambda k: k[0])
+def test_invcg_solves_the_system(kind):
+    op = make(kind)
+    b = fields.random_source(op.n // 24, 6)
+    x, it, true_res = op.invcg(b, stop_rsd=1e-10)
+    res = shifted_residual(op, x, b, 0.0)
+    assert 0 < it < 5000 and res < 2e-10
+    assert abs(true_res - res) <= 1e-3 * res
+
+
+@pytest.mark.parametrize("action", ["wilson", "dwf"])
+def test_minvcg_multi_solves_every_shift_and_single_is_their_sum(action):
+    op = make((action, 2))
+    b = fields.random_source(op.n // 24, 7)
+    shifts = [1e-3, 0.05, 0.4, 2.0]
+    alpha = [0.7, -0.2, 1.3, 0.45]
+    xs, _, rs = op.minvcg(b, shifts, [1e-10] * 4, ms_type=0)
+    for x, s, r in zip(xs, shifts, rs):
+        # the reported residual is the iterated absolute one; the true relative residual follows it
+        assert shifted_residual(op, x, b, s) < 3e-10
+        assert r < 1e-10 * np.linalg.norm(b)
+    (xsum,), _, _ = op.minvcg(b, shifts, [1e-10] * 4, ms_type=1, alpha=alpha)
+    ref = sum(a * x for a, x in zip(alpha, xs))
+    assert np.linalg.norm(xsum - ref) <= 1e-12 * np.linalg.norm(ref)
