@@ -81,7 +81,7 @@ def gen_case(name, action, dims, ls, eps, seed, mass, extra):
     return rec
 
 
-def gen_baseline_config0():
+def gen_wilson_8x8x8x8_cg():
     """The reference's own CPU-runnable benchmark case: Wilson 8^4, eps 0.3,
     mass 0.1, Gaussian source on the odd checkerboard, stop_rsd 1e-10."""
     dims = (8, 8, 8, 8)
@@ -191,7 +191,7 @@ def main():
         rec = gen_case(*case)
         np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **rec)
         print("wrote", case[0])
-    np.savez_compressed(os.path.join(OUT, "wilson_8x8x8x8_cg.npz"), **gen_baseline_config0())
+    np.savez_compressed(os.path.join(OUT, "wilson_8x8x8x8_cg.npz"), **gen_wilson_8x8x8x8_cg())
     print("wrote wilson_8x8x8x8_cg")
     main_matinv()
     main_fconvert()
