@@ -199,6 +199,7 @@ def main():
     main_pc()
     main_dminus()
     main_zmobius()
+    main_cg16()
 
 
 # Mobius with the non-default preconditioners ZMOB_PC_ORIG (0) and ZMOB_PC_SYM1 (1)
@@ -325,6 +326,39 @@ def main_fconvert():
     print("wrote fconvert_4x4x4x6")
 
 
+# CG at the 8^4 x Ls 16 volume, where a whole CPS solve still takes well under
+# a minute: the solution is pinned by the SHA-256 of its bytes (the oracle
+# restates CPS bit for bit), with its norm and inner products with four seeded
+# vectors kept as a readable digest.
+CG16_CASES = [("cg_dwf_8x8x8x8_ls16", "dwf", (8, 8, 8, 8), 16, 0.2, 60, 0.1, {"m5": 1.8}),
+              ("cg_mobius_8x8x8x8_ls16", "mobius", (8, 8, 8, 8), 16, 0.2, 61, 0.1, {"m5": 1.8, "b": 1.5, "c": 0.5})]
+DIGEST_SEEDS = (1000, 1001, 1002, 1003)
+
+
+def solution_digest(x, nsites):
+    return np.array([float(x @ x)] + [float(x @ fields.random_source(nsites, s)) for s in DIGEST_SEEDS])
+
+
+def gen_cg16(name, action, dims, ls, eps, seed, mass, extra):
+    u = fields.random_gauge(dims, eps, seed)
+    nsites = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(nsites, seed)
+    it, rp, r = refrun.run(refrun.OP_INVCG, action, dims, u, [src, np.zeros_like(src)], ls=ls, mass=mass,
+                           stop_rsd=1e-10, max_iter=5000, threads=1, **extra)
+    rec = {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
+           "mass": mass, "cg_iters": it, "cg_true_res": rp[0], "cg_sol_sha": sha(r),
+           "cg_sol_digest": solution_digest(r, nsites)}
+    for k, v in extra.items():
+        rec[k] = v
+    return rec
+
+
+def main_cg16():
+    for case in CG16_CASES:
+        np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **gen_cg16(*case))
+        print("wrote", case[0])
+
+
 if __name__ == "__main__":
     if "--matinv" in sys.argv:
         main_matinv()
@@ -338,5 +372,7 @@ if __name__ == "__main__":
         main_pc()
     elif "--zmobius" in sys.argv:
         main_zmobius()
+    elif "--cg16" in sys.argv:
+        main_cg16()
     else:
         main()

@@ -84,6 +84,21 @@ def test_wilson_8x8x8x8_cg_config():
     np.testing.assert_array_equal(sol, rec["cg_sol"])
 
 
+@pytest.mark.parametrize("name", ["cg_dwf_8x8x8x8_ls16", "cg_mobius_8x8x8x8_ls16"])
+def test_cg_8x8x8x8_ls16_bitexact(name):
+    """DWF and Mobius (SYM2) InvCg at 8^4 x Ls 16, m_f 0.1, to 1e-10 (175-200
+    iterations): iteration count, true residual and the solution's bytes."""
+    from tests.golden.make_golden import solution_digest
+    from tests.golden_util import sha
+    rec, u, src = load(name)
+    op = make_op(rec, u, name.split("_")[1])
+    sol, it, tr = op.invcg(src, 1e-10, 5000)
+    assert it == int(rec["cg_iters"])
+    assert tr == float(rec["cg_true_res"]) and tr <= 1e-10
+    np.testing.assert_array_equal(solution_digest(sol, op.n // 24), rec["cg_sol_digest"])
+    assert sha(sol) == str(rec["cg_sol_sha"])
+
+
 @pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_matinv_bitexact(name):
     """DiracOp*::MatInv (full-lattice solve with source preparation and
