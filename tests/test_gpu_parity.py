@@ -94,6 +94,33 @@ def test_wilson_8x8x8x8_config_cg():
         assert r.true_rsd <= 1e-10 and rel(x, rec["cg_sol"]) < 1e-8
 
 
+@pytest.mark.parametrize("name", ["cg_dwf_8x8x8x8_ls16", "cg_mobius_8x8x8x8_ls16"])
+def test_cg_8x8x8x8_ls16_vs_reference(name):
+    """DWF and Mobius CG at 8^4 x Ls 16 against CPS's solve (kept as a digest:
+    |x|^2 and x.v for four seeded v).  A solution within e relative of CPS's
+    moves x.v by at most e |x| |v|.  FP64 follows CPS's recurrence: e = 1e-9.
+    Mixed solves only share the 1e-10 true residual, and at that residual the
+    Mobius solve is still 6.5e-9 from the exact solution (measured against a
+    1e-14 solve), so two such solutions may differ by 1.3e-8: e = 3e-8."""
+    import cps_public_b200 as cb
+    from tests.golden.make_golden import DIGEST_SEEDS, solution_digest
+    from cps_public_b200 import fields
+    rec, u, src = load(name)
+    op = device_op(rec, u, name.split("_")[1])
+    n = src.size // 24
+    ref = rec["cg_sol_digest"]
+    xnorm = np.sqrt(ref[0])
+    vnorm = np.array([np.linalg.norm(fields.random_source(n, s)) for s in DIGEST_SEEDS])
+    for prec, tol in ((cb.F64, 1e-9), (cb.F32, 3e-8), (cb.F16, 3e-8)):
+        x, r = op.InvCg(src, stop_rsd=1e-10, max_num_iter=5000, precision=prec)
+        assert r.status == 0 and r.true_rsd <= 1e-10, (prec, r.as_dict())
+        if prec == cb.F64:
+            assert abs(r.iters - int(rec["cg_iters"])) <= 1, (r.iters, int(rec["cg_iters"]))
+        d = solution_digest(x, n)
+        assert abs(d[0] - ref[0]) <= 2 * tol * ref[0], (prec, d[0], ref[0])
+        assert np.all(np.abs(d[1:] - ref[1:]) <= tol * xnorm * vnorm), (prec, d[1:], ref[1:])
+
+
 @pytest.mark.parametrize("action,ls", [("wilson", 1), ("dwf", 8), ("mobius", 8)])
 def test_operators_vs_oracle_random(action, ls):
     """Fresh seeds and a non-cubic lattice against the C oracle."""
