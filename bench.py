@@ -152,7 +152,7 @@ def peak_hbm():
 def ncu_traffic():
     """DRAM bytes per launch of the FP16 Dslash from the committed ncu summary."""
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "dslash_dram_traffic.json")))
+        d = json.load(open(os.path.join(ROOT, "profiles", "dslash_dram_traffic_dwf_16x16x16x32_ls16.json")))
         return d
     except Exception:
         return None
