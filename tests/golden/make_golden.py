@@ -353,10 +353,34 @@ def gen_cg16(name, action, dims, ls, eps, seed, mass, extra):
     return rec
 
 
+# MInvCG (MULTI) at the same volume: four shifts, each solution pinned the same way
+MINVCG16_CASE = ("minvcg_dwf_8x8x8x8_ls16", "dwf", (8, 8, 8, 8), 16, 0.2, 62, 0.1, {"m5": 1.8})
+MINVCG16_SHIFTS = (1e-3, 0.05, 0.4, 2.0)
+
+
+def gen_minvcg16(name, action, dims, ls, eps, seed, mass, extra):
+    u = fields.random_gauge(dims, eps, seed)
+    nsites = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(nsites, seed)
+    ns = len(MINVCG16_SHIFTS)
+    it, rp, r = refrun.run(refrun.OP_MINVCG, action, dims, u, [src], ls=ls, mass=mass, shifts=MINVCG16_SHIFTS,
+                           extra=[np.full(ns, 1e-10), np.ones(ns)], max_iter=5000, threads=1, **extra)
+    sols = r.reshape(ns, -1)
+    rec = {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
+           "mass": mass, "minvcg_shifts": np.array(MINVCG16_SHIFTS), "minvcg_iters": it,
+           "minvcg_rsd": rp[:ns].copy(), "minvcg_sol_sha": np.array([sha(x) for x in sols]),
+           "minvcg_sol_digest": np.stack([solution_digest(x, nsites) for x in sols])}
+    for k, v in extra.items():
+        rec[k] = v
+    return rec
+
+
 def main_cg16():
     for case in CG16_CASES:
         np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **gen_cg16(*case))
         print("wrote", case[0])
+    np.savez_compressed(os.path.join(OUT, MINVCG16_CASE[0] + ".npz"), **gen_minvcg16(*MINVCG16_CASE))
+    print("wrote", MINVCG16_CASE[0])
 
 
 if __name__ == "__main__":

@@ -99,6 +99,22 @@ def test_cg_8x8x8x8_ls16_bitexact(name):
     assert sha(sol) == str(rec["cg_sol_sha"])
 
 
+def test_minvcg_8x8x8x8_ls16_bitexact():
+    """DWF MInvCG (MULTI, shifts 1e-3..2, 1e-10 each) at 8^4 x Ls 16: iteration
+    count, the reported residuals and every solution's bytes."""
+    from tests.golden.make_golden import solution_digest
+    from tests.golden_util import sha
+    rec, u, src = load("minvcg_dwf_8x8x8x8_ls16")
+    op = make_op(rec, u, "dwf")
+    shifts = list(rec["minvcg_shifts"])
+    sols, it, rsd = op.minvcg(src, shifts, [1e-10] * len(shifts))
+    assert it == int(rec["minvcg_iters"])
+    np.testing.assert_array_equal(rsd, rec["minvcg_rsd"])
+    for k, x in enumerate(sols):
+        np.testing.assert_array_equal(solution_digest(x, op.n // 24), rec["minvcg_sol_digest"][k])
+        assert sha(x) == str(rec["minvcg_sol_sha"][k])
+
+
 @pytest.mark.parametrize("name", CASES + PC_CASES)
 def test_matinv_bitexact(name):
     """DiracOp*::MatInv (full-lattice solve with source preparation and
