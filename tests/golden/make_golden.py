@@ -375,12 +375,30 @@ def gen_minvcg16(name, action, dims, ls, eps, seed, mass, extra):
     return rec
 
 
+# zMobius (SYM2, complex b_s, c_s from zmobius_coefficients) CG at the same volume
+ZCG16_CASE = ("cg_zmobius_8x8x8x8_ls16", (8, 8, 8, 8), 16, 0.2, 63, 0.1, 1.5, 0.5)
+
+
+def gen_zcg16(name, dims, ls, eps, seed, mass, b, c):
+    u = fields.random_gauge(dims, eps, seed)
+    nsites = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(nsites, seed)
+    zb, zc = zmobius_coefficients(ls, seed, b, c)
+    it, rp, r = refrun.run(refrun.OP_INVCG, "zmobius", dims, u, [src, np.zeros_like(src)], ls=ls, mass=mass, m5=1.8,
+                           b=b, c=c, zb=zb, zc=zc, pc_type=2, stop_rsd=1e-10, max_iter=5000, threads=1)
+    return {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
+            "mass": mass, "m5": 1.8, "zb": zb, "zc": zc, "pc_type": 2, "cg_iters": it, "cg_true_res": rp[0],
+            "cg_sol_sha": sha(r), "cg_sol_digest": solution_digest(r, nsites)}
+
+
 def main_cg16():
     for case in CG16_CASES:
         np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **gen_cg16(*case))
         print("wrote", case[0])
     np.savez_compressed(os.path.join(OUT, MINVCG16_CASE[0] + ".npz"), **gen_minvcg16(*MINVCG16_CASE))
     print("wrote", MINVCG16_CASE[0])
+    np.savez_compressed(os.path.join(OUT, ZCG16_CASE[0] + ".npz"), **gen_zcg16(*ZCG16_CASE))
+    print("wrote", ZCG16_CASE[0])
 
 
 if __name__ == "__main__":

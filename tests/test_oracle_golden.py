@@ -99,6 +99,21 @@ def test_cg_8x8x8x8_ls16_bitexact(name):
     assert sha(sol) == str(rec["cg_sol_sha"])
 
 
+def test_zmobius_cg_8x8x8x8_ls16_bitexact():
+    """zMobius (SYM2, complex b_s, c_s) InvCg at 8^4 x Ls 16, m_f 0.1, to 1e-10
+    (421 iterations): iteration count, true residual and the solution's bytes."""
+    from tests.golden.make_golden import solution_digest
+    from tests.golden_util import sha
+    rec, u, src = load("cg_zmobius_8x8x8x8_ls16")
+    op = oracle.Op("mobius", tuple(rec["dims"]), u, ls=int(rec["ls"]), mass=float(rec["mass"]),
+                   m5=float(rec["m5"]), bs=list(rec["zb"]), cs=list(rec["zc"]), pc_type=int(rec["pc_type"]))
+    sol, it, tr = op.invcg(src, 1e-10, 5000)
+    assert it == int(rec["cg_iters"])
+    assert tr == float(rec["cg_true_res"]) and tr <= 1e-10
+    np.testing.assert_array_equal(solution_digest(sol, op.n // 24), rec["cg_sol_digest"])
+    assert sha(sol) == str(rec["cg_sol_sha"])
+
+
 def test_minvcg_8x8x8x8_ls16_bitexact():
     """DWF MInvCG (MULTI, shifts 1e-3..2, 1e-10 each) at 8^4 x Ls 16: iteration
     count, the reported residuals and every solution's bytes."""
