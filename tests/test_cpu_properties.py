@@ -4,8 +4,9 @@ MatPcDagMatPc is Hermitian and positive, for every action and every
 preconditioner; zMobius with constant coefficients is Mobius; Dminus is
 linear (tolerances at rounding level, 1e-13 relative).  The solvers solve:
 InvCg's solution meets its tolerance against an independently formed
-residual, MInvCG's MULTI solutions each solve their shifted system, and SINGLE
-returns the alpha-weighted sum of the MULTI solutions."""
+residual, MInvCG's MULTI solutions each solve their shifted system, SINGLE
+returns the alpha-weighted sum of the MULTI solutions, and the Wilson and DWF
+full-lattice MatInv solves M x = b on both checkerboards."""
 import numpy as np
 import pytest
 
@@ -107,3 +108,23 @@ def test_minvcg_multi_solves_every_shift_and_single_is_their_sum(action):
     (xsum,), _, _ = op.minvcg(b, shifts, [1e-10] * 4, ms_type=1, alpha=alpha)
     ref = sum(a * x for a, x in zip(alpha, xs))
     assert np.linalg.norm(xsum - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("action", ["wilson", "dwf"])
+def test_matinv_solves_the_full_lattice_system(action):
+    """MatInv solves M x = b on both checkerboards with M = 1 - kappa D
+    (d_op_wilson.C:257-334, d_op_dwf.C:316-507); kappa = 1/(2(m + 4)) for Wilson
+    (d_op_wilson.C:134-137), 1/(2(4 + a5_inv - M5)) for DWF (dwf_init.C:97-98).
+    Full vectors are odd half first; Dslash(in, cb) reads checkerboard cb and
+    writes the other one.  The even half is rebuilt exactly, the odd half is
+    the CG solution."""
+    op = make((action, 2))
+    kappa = 1 / (2 * (0.1 + 4)) if action == "wilson" else 1 / (2 * (4 + 1.0 - 1.8))
+    n = op.n
+    b = np.concatenate([fields.random_source(n // 24, 8), fields.random_source(n // 24, 9)])
+    x, it, _ = op.matinv(b, stop_rsd=1e-12)
+    xo, xe = x[:n], x[n:]
+    ro = xo - kappa * op.dslash(xe, 0, 0)
+    re = xe - kappa * op.dslash(xo, 1, 0)
+    assert np.linalg.norm(ro - b[:n]) <= 1e-10 * np.linalg.norm(b[:n])
+    assert np.linalg.norm(re - b[n:]) <= 1e-13 * np.linalg.norm(b[n:])
