@@ -128,3 +128,26 @@ def test_matinv_solves_the_full_lattice_system(action):
     re = xe - kappa * op.dslash(xo, 1, 0)
     assert np.linalg.norm(ro - b[:n]) <= 1e-10 * np.linalg.norm(b[:n])
     assert np.linalg.norm(re - b[n:]) <= 1e-13 * np.linalg.norm(b[n:])
+
+
+def gamma5(v):
+    """gamma_5 = diag(1, 1, -1, -1) over spins in CPS's chiral basis (spin slowest in a site)."""
+    w = v.reshape(-1, 4, 3, 2).copy()
+    w[:, 2:] *= -1
+    return w.reshape(-1)
+
+
+@pytest.mark.parametrize("kind", [("wilson", 2), ("dwf", 2), ("mobius", 2)], ids=lambda k: k[0])
+def test_dslash_dag_is_the_adjoint(kind):
+    """<y, D(cb) x> = <D^dag(1 - cb) y, x> for the hop of every action; the
+    Wilson hop is also gamma_5-hermitian, D^dag = gamma_5 D gamma_5, bit for bit
+    (the 5-D operators are hermitian only together with the reflection
+    s -> Ls - 1 - s, which moves a field to the other 5-D checkerboard)."""
+    op = make(kind)
+    n = op.n // 24
+    x, y = fields.random_source(n, 1), fields.random_source(n, 2)
+    for cb in (0, 1):
+        lhs, rhs = cdot(y, op.dslash(x, cb, 0)), cdot(op.dslash(y, 1 - cb, 1), x)
+        assert abs(lhs - rhs) <= 1e-13 * abs(lhs)
+        if kind[0] == "wilson":
+            np.testing.assert_array_equal(op.dslash(x, cb, 1), gamma5(op.dslash(gamma5(x), cb, 0)))
