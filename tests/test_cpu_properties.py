@@ -1,5 +1,6 @@
 """Properties of the operators that hold independently of any golden vector,
-checked on the C oracle (CPU): MatPcDag is the adjoint of MatPc and
+checked on the C oracle (CPU): Dslash's dag form is its adjoint (and the
+Wilson hop gamma_5-hermitian), MatPcDag is the adjoint of MatPc and
 MatPcDagMatPc is Hermitian and positive, for every action and every
 preconditioner; zMobius with constant coefficients is Mobius; Dminus is
 linear (tolerances at rounding level, 1e-13 relative).  The solvers solve:
