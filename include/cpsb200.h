@@ -97,12 +97,15 @@ typedef struct {
   int status;
 } cpsb_solve_result;
 
-/* Selects the CUDA device and creates the library context (one per process). */
+/* Selects the CUDA device and creates the library context (one per process):
+ * the device half of CPS's Start(), which in QUDA builds calls
+ * initQuda(QudaParam.device) (src/util/gjp/qmp/start_end.C:54). */
 int cpsb_init(int device);
 const char *cpsb_error_string(int code);
 /* Detail message of the last error raised on the calling thread. */
 const char *cpsb_last_error(void);
-/* Free and total device memory in bytes (the serving loop admits work by it). */
+/* Free and total device memory in bytes (the serving loop admits work by it).
+ * No counterpart in the reference. */
 int cpsb_mem_info(unsigned long long *free_bytes, unsigned long long *total_bytes);
 
 /* Uploads a gauge field and keeps it resident (FP64 plus the reduced-precision
@@ -113,6 +116,9 @@ int cpsb_mem_info(unsigned long long *free_bytes, unsigned long long *total_byte
  * (lattice/lattice_base/lattice_base.C:5313-5370).  Replaces the gauge half of
  * the DiracOp constructor (d_op_dwf/d_op_dwf.C:67-123). */
 int cpsb_gauge_load(cpsb_gauge *h, const double *u, const int dims[4], int order, int bc_t);
+/* Releases a resident field and the solvers built on it: the device end of the
+ * DiracOp destructor's conversion back to CANONICAL (d_op_dwf/d_op_dwf.C:132-150)
+ * and of freeGaugeQuda in the QUDA bridge (d_op_dwf/quda/dwf_quda.C:173). */
 int cpsb_gauge_free(cpsb_gauge h);
 
 /* DiracOp*::Dslash(out, in, cb, dag) (include/util/dirac_op.h:275):
@@ -243,7 +249,8 @@ int cpsb_kernel_launches(unsigned long long *count);
 /* Times `reps` applications of the device Dslash of the given precision on
  * internally resident data (one checkerboard, dag 0); reports the mean kernel
  * time in ms measured with CUDA events on the launching stream, and the bytes
- * each application must move (spinors in + out + links). */
+ * each application must move (spinors in + out + links).  No counterpart in the
+ * reference. */
 int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
                       double *bytes);
 
