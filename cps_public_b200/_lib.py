@@ -25,7 +25,7 @@ SYMBOLS = [
     "cpsb_init", "cpsb_serve_submit_minvcg", "cpsb_error_string", "cpsb_last_error", "cpsb_mem_info", "cpsb_gauge_load", "cpsb_gauge_free", "cpsb_dslash",
     "cpsb_matpc", "cpsb_mdagm", "cpsb_invcg", "cpsb_invcg_multi", "cpsb_minvcg", "cpsb_matinv", "cpsb_fmatinv", "cpsb_dminus", "cpsb_invcg_dev",
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
-    "cpsb_kernel_launches",
+    "cpsb_kernel_launches", "cpsb_dslash_multi_dev", "cpsb_mdagm_multi_dev",
     "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
     "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert", "cpsb_minresext",
 ]
@@ -97,6 +97,9 @@ def load():
                                     _dp, R, C.c_void_p]
     lib.cpsb_dslash_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, C.c_int, C.c_int]
     lib.cpsb_mdagm_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, _dp]
+    lib.cpsb_dslash_multi_dev.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_void_p]
+    lib.cpsb_mdagm_multi_dev.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, _dp, C.c_void_p]
     lib.cpsb_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_ulonglong]
     lib.cpsb_serve_submit.argtypes = [C.c_void_p, C.c_void_p, P, A, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
                                       C.POINTER(C.c_ulonglong)]

@@ -212,6 +212,8 @@ int cpsb_gauge_free(cpsb_gauge h) {
   return guarded([&] {
     if (!h) return CPSB_OK;
     need_init();
+    if (h->g.inflight.load() > 0)
+      throw Error{CPSB_ERR_BUSY, "gauge field has queued or running requests of the request loop; wait for them"};
     CK(cudaStreamSynchronize(ctx().stream));
     drop_solvers(&h->g);
     delete h;
@@ -370,6 +372,48 @@ int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const 
     op.mdagm(fo, fi, &r, nullptr, st);
     CK(launch_unpack(P64, out, fo.ptr(), op.nsites(), st));
     if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return CPSB_OK;
+  });
+}
+
+int cpsb_dslash_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, double *out,
+                          const double *in, int cb, int dag, void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (precision < CPSB_PREC_F64 || precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+    if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
+    if (!out || !in || (cb != 0 && cb != 1) || (dag != 0 && dag != 1)) throw Error{CPSB_ERR_ARG, "bad argument"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    Operator op(&h->g, *p, precision, nrhs);
+    Field fi(precision, op.nsites()), fo(precision, op.nsites());
+    CK(launch_pack(precision, fi.ptr(), in, op.nsites(), st));
+    op.dslash(fo, fi, cb, dag, st);
+    CK(launch_unpack(precision, out, fo.ptr(), op.nsites(), st));
+    CK(cudaStreamSynchronize(st));
+    return CPSB_OK;
+  });
+}
+
+int cpsb_mdagm_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, double *out,
+                         const double *in, double *dot, void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    if (precision < CPSB_PREC_F64 || precision > CPSB_PREC_F16) throw Error{CPSB_ERR_ARG, "bad precision"};
+    if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
+    if (!out || !in) throw Error{CPSB_ERR_ARG, "null vector"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    Operator op(&h->g, *p, precision, nrhs);
+    Field fi(precision, op.nsites()), fo(precision, op.nsites());
+    RedSlot rs;
+    DevBuf d(sizeof(double) * MAX_RHS);
+    Reduce r = rs.r((double *)d.p);
+    CK(launch_pack(precision, fi.ptr(), in, op.nsites(), st));
+    op.mdagm(fo, fi, &r, nullptr, st);
+    CK(launch_unpack(precision, out, fo.ptr(), op.nsites(), st));
+    if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return CPSB_OK;
   });

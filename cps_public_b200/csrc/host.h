@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <complex>
 
 #include <map>
@@ -56,6 +57,9 @@ struct Gauge {
   bool recon_ok = false;
   double recon_err = 0;
   std::mutex mu;
+  // Work items of the request loop (serve.cu) queued or running on this field;
+  // cpsb_gauge_free refuses (CPSB_ERR_BUSY) while it is nonzero.
+  std::atomic<int> inflight{0};
   GaugePtr ptr(int prec);
 };
 

@@ -1,11 +1,10 @@
 // noalloc.cu -- global dot products that allocate no memory.
 //
 // cpsb_redot_noalloc is the deterministic reduction of redot_kernel (blas.cu)
-// for callers that must not allocate device memory: code that records its work
-// into a CUDA graph (cudaMalloc/cudaFree may not be called on a capturing
-// stream), HMC and serving loops that reserve their whole HBM budget up front
-// and run every solve out of that arena, and codes that keep the device free
-// of implicit synchronisation (cudaFree synchronises the device).  Its
+// for callers that must not allocate device memory: HMC and serving loops that
+// reserve their whole HBM budget up front and run every solve out of that
+// arena, and codes that keep the device free of implicit synchronisation
+// (cudaFree synchronises the device).  Its
 // reduction scratch -- one partial sum per block and vector, plus the
 // last-block ticket -- lives in a file-scope __device__ array of
 // NOALLOC_SCRATCH_BYTES (80 KiB) that every GPU loading the library holds

@@ -222,6 +222,7 @@ void Server::worker_main() {
       reserved -= it.bytes;
       running--;
       ServeRequest &r = *it.req;
+      r.h->g.inflight -= 1;  // the item no longer touches the gauge field
       if (rc != CPSB_OK && (r.status == CPSB_OK || (r.status > 0 && rc < 0))) {
         r.status = rc;
         r.err = msg;
@@ -325,6 +326,7 @@ int cpsb_serve_submit(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_params *p,
         S.queue.push_back(ServeItem{r.get(), r0, m, solve_footprint(*p, n, a->precision, m)});
         r0 += m;
       }
+      h->g.inflight += nitems;
       *id = r->id;
       S.reqs[r->id] = std::move(r);
     }
@@ -378,6 +380,7 @@ int cpsb_serve_submit_minvcg(cpsb_server srv, cpsb_gauge h, const cpsb_dirac_par
       r->t_submit = now_ms();
       if (S.t_first_submit < 0) S.t_first_submit = r->t_submit;
       S.queue.push_back(ServeItem{r.get(), 0, 1, bytes});
+      h->g.inflight += 1;
       *id = r->id;
       S.reqs[r->id] = std::move(r);
     }

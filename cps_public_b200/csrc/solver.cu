@@ -359,12 +359,26 @@ CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs)
   return s;
 }
 
+// Removes the cached solvers of G (cpsb_gauge_free).  Each one is destroyed only
+// after its busy lock could be taken, so a solve still running on another host
+// thread finishes first; no lock is held while waiting.  The cache keeps one
+// solver per distinct (parameters, precision, nrhs) until its gauge is freed.
 void drop_solvers(Gauge *G) {
-  std::lock_guard<std::mutex> lk(solvers_mu);
-  auto &m = solvers();
-  for (auto it = m.begin(); it != m.end();) {
-    if (it->first.G == G) it = m.erase(it);
-    else ++it;
+  std::vector<std::unique_ptr<CgSolver>> gone;
+  {
+    std::lock_guard<std::mutex> lk(solvers_mu);
+    auto &m = solvers();
+    for (auto it = m.begin(); it != m.end();) {
+      if (it->first.G == G) {
+        gone.push_back(std::move(it->second));
+        it = m.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  for (auto &s : gone) {
+    std::lock_guard<std::mutex> wait_for_solve(s->busy);
   }
 }
 

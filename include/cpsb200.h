@@ -118,7 +118,11 @@ int cpsb_mem_info(unsigned long long *free_bytes, unsigned long long *total_byte
 int cpsb_gauge_load(cpsb_gauge *h, const double *u, const int dims[4], int order, int bc_t);
 /* Releases a resident field and the solvers built on it: the device end of the
  * DiracOp destructor's conversion back to CANONICAL (d_op_dwf/d_op_dwf.C:132-150)
- * and of freeGaugeQuda in the QUDA bridge (d_op_dwf/quda/dwf_quda.C:173). */
+ * and of freeGaugeQuda in the QUDA bridge (d_op_dwf/quda/dwf_quda.C:173).
+ * Returns CPSB_ERR_BUSY (and frees nothing) while requests of the request loop
+ * (cpsb_serve_submit*) on this field are queued or running: wait for them
+ * first.  A solve running on another host thread is waited for.  The handle
+ * must not be used by any call that starts after this one. */
 int cpsb_gauge_free(cpsb_gauge h);
 
 /* DiracOp*::Dslash(out, in, cb, dag) (include/util/dirac_op.h:275):
@@ -223,6 +227,18 @@ int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg
                          const double *b, cpsb_solve_result *res, void *stream);
 int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const double *in, double *dot,
                    void *stream);
+/* The multi-right-hand-side Dslash and MatPcDagMatPc: the operator applied to
+ * nrhs vectors in one launch sequence, every link read once for all of them,
+ * with fields stored in the given precision (as cpsb_dslash_ex).  in, out:
+ * device pointers to nrhs consecutive CPS-order vectors; dot (host, nrhs
+ * entries, may be NULL) receives |MatPc in_q|^2.  Interfaces of DiracOp::Dslash
+ * (dirac_op.h:275) and DiracOp::MatPcDagMatPc (dirac_op.h:262), which CPS
+ * applies one vector at a time (its multi-source DiracOpMobius::MatInv,
+ * dirac_op.h:1886, loops over the sources). */
+int cpsb_dslash_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, double *out,
+                          const double *in, int cb, int dag, void *stream);
+int cpsb_mdagm_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, double *out,
+                         const double *in, double *dot, void *stream);
 /* cpsb_minvcg with b and the solutions x[s] in device memory (x: host array of
  * device pointers). */
 int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *const *x,
@@ -257,17 +273,16 @@ int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, i
 /* Real parts of nvec dot products <x_v, y_v> of device vectors of n doubles
  * each (vector v starts at x + v*n), written to result[0..nvec) in device
  * memory, in a fixed (reproducible) summation order.  It allocates nothing:
- * for callers that cannot call cudaMalloc -- code recording a CUDA graph
- * (allocation is not allowed on a capturing stream), loops that run inside a
- * pre-reserved HBM arena, codes that must avoid cudaFree's device-wide sync.
- * Its reduction scratch is an 80 KiB file-scope __device__ array that every
- * GPU using the library keeps until exit; the first call on a device looks up
- * that array's address (make it before any stream capture).  Calls whose work
- * overlaps on the GPU share the array and race: serialise them on one stream.
- * Limits: 1 <= nvec <= 16, n >= 1; larger nvec is rejected with CPSB_ERR_ARG.
- * Uses the current CUDA device; needs no cpsb_init.  No counterpart in the
- * reference: it is the device analogue of Vector::ReDotProductGlbSum
- * (include/util/vector.h:955) with no allocation of its own. */
+ * for callers that cannot call cudaMalloc -- solvers and HMC loops that run
+ * inside an HBM arena they reserved up front and may not grow, and codes that
+ * must avoid the device-wide synchronisation of cudaFree.  Its reduction
+ * scratch is an 80 KiB file-scope __device__ array that every GPU using the
+ * library keeps until exit; the first call on a device looks up that array's
+ * device address (make this first call before any stream capture).  Calls
+ * whose work overlaps on the GPU share the array and race: serialise them on
+ * one stream.  Limits: 1 <= nvec <= 16, n >= 1; larger nvec is rejected with
+ * CPSB_ERR_ARG.  Uses the current CUDA device; needs no cpsb_init.  It has no
+ * counterpart in the reference. */
 int cpsb_redot_noalloc(const double *x, const double *y, long n, int nvec, double *result, void *stream);
 
 /* Request loop for concurrent solves.  CPS runs one DiracOp at a time

@@ -6,7 +6,7 @@
 # links them with oracle/ref_harness.C into oracle/_ref/cpsref, the executable
 # that runs the reference's own Dslash / MatPcDagMatPc / InvCg / MInvCG.
 #
-# Usage: oracle/build_ref.sh [path-to-cps_pp]   (default /root/reference/cps_pp)
+# Usage: oracle/build_ref.sh [path-to-cps_pp]   (default $CPS_REFERENCE, else /root/reference/cps_pp)
 # Output goes only to oracle/_ref/ (git-ignored).  Nothing is written into the
 # reference tree and no reference source is copied into this repository.
 #
@@ -23,7 +23,7 @@
 #    the link keeps those first definitions (--allow-multiple-definition).
 #    OP_INVCG in the harness calls InvCgShift directly.
 set -euo pipefail
-REF=${1:-/root/reference/cps_pp}
+REF=${1:-${CPS_REFERENCE:-/root/reference/cps_pp}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 OBJ=$OUT/obj

@@ -41,7 +41,9 @@
 //        17 OP_MINRESEXT degree (number of previous solutions),
 //        18 OP_FMATINV dminus flag
 //   rpar[10] = wall seconds spent inside the timed CPS call(s) (MINVCG: rpar[42],
-//   since rpar[0..nshift) holds the per-shift residuals)
+//   since rpar[0..nshift) holds the per-shift residuals); OP_BENCH also
+//   returns the start and end of that window (steady clock, seconds) in
+//   rpar[11], rpar[12], so that concurrent processes can be checked for overlap
 //   par: 0 mass, 1 M5 (dwf_height), 2 a5_inv, 3 mobius b, 4 mobius c, 5 stop_rsd,
 //        8.. shifts[nshift], 24.. unused
 //   zMobius (action 3) only: 4*ls doubles right after par, before the gauge:
@@ -238,6 +240,7 @@ int main(int argc, char **argv) {
       t0 = now_s(); for (int i = 0; i < reps; i++) d.MatPcDagMatPc(out, in, &dot); t1 = now_s();
     }
     rpar[0] = dot; rpar[10] = t1 - t0; rhdr[0] = reps;
+    rpar[11] = t0; rpar[12] = t1;  // the timed window on the system-wide monotonic clock
     out_payload.assign((double *)out, (double *)out + fsz);
   } else if (op == OP_INVCG) {
     read_all(fi, in, fsz * sizeof(double));          // source

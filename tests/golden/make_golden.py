@@ -391,6 +391,31 @@ def gen_zcg16(name, dims, ls, eps, seed, mass, b, c):
             "cg_sol_sha": sha(r), "cg_sol_digest": solution_digest(r, nsites)}
 
 
+# The benchmark lattice itself (bench.py's fields: DWF 16^3x32, Ls 16, m_f 0.01,
+# M5 1.8, links eps 0.2 seed 2024, Gaussian source seed 2025): one Dslash
+# (cb 1, dag 0) and one MatPcDagMatPc of the compiled reference, each output
+# pinned by its SHA-256 and digest, and the fused dot.
+BENCH16_CASE = ("bench_dwf_16x16x16x32_ls16", "dwf", (16, 16, 16, 32), 16, 0.2, 2024, 2025, 0.01)
+
+
+def gen_bench16(name, action, dims, ls, eps, seed, src_seed, mass):
+    u = fields.random_gauge(dims, eps, seed)
+    nsites = int(np.prod(dims)) // 2 * ls
+    src = fields.random_source(nsites, src_seed)
+    _, _, d = refrun.run(refrun.OP_DSLASH, action, dims, u, [src], ls=ls, mass=mass, m5=1.8, cb=1, dag=0,
+                         threads=1)
+    _, rp, m = refrun.run(refrun.OP_MDAGM, action, dims, u, [src], ls=ls, mass=mass, m5=1.8, threads=1)
+    return {"gauge_sha": sha(u), "src_sha": sha(src), "dims": np.array(dims), "ls": ls, "eps": eps, "seed": seed,
+            "src_seed": src_seed, "mass": mass, "m5": 1.8,
+            "dslash_sha": sha(d), "dslash_digest": solution_digest(d, nsites),
+            "mdagm_sha": sha(m), "mdagm_digest": solution_digest(m, nsites), "mdagm_dot": rp[0]}
+
+
+def main_bench16():
+    np.savez_compressed(os.path.join(OUT, BENCH16_CASE[0] + ".npz"), **gen_bench16(*BENCH16_CASE))
+    print("wrote", BENCH16_CASE[0])
+
+
 def main_cg16():
     for case in CG16_CASES:
         np.savez_compressed(os.path.join(OUT, case[0] + ".npz"), **gen_cg16(*case))
@@ -416,5 +441,7 @@ if __name__ == "__main__":
         main_zmobius()
     elif "--cg16" in sys.argv:
         main_cg16()
+    elif "--bench16" in sys.argv:
+        main_bench16()
     else:
         main()

@@ -142,3 +142,25 @@ def test_zmobius_request_owns_coefficients(setup):
     srv.close()
     assert res[0].status == 0 and res[0].iters == r_ref.iters
     np.testing.assert_array_equal(xs[0], x_ref)
+
+
+def test_gauge_free_refused_while_requests_are_in_flight():
+    """cpsb_gauge_free returns CPSB_ERR_BUSY while a request on the field is
+    queued or running (its kernels read the links), and frees it afterwards."""
+    import cps_public_b200 as cb
+    from cps_public_b200 import _lib, fields
+    cb.init(0)
+    lib = _lib.load()
+    dims, ls = (8, 8, 8, 16), 8
+    g = cb.Gauge(fields.random_gauge(dims, 0.2, 311), dims)
+    op = cb.DiracOp(g, "dwf", mass=0.01, ls=ls, m5=1.8)
+    srcs = [fields.random_source(op.n // 24, 312 + i) for i in range(2)]
+    srv = cb.Server(slots=1)
+    rid = srv.submit(op, srcs, stop_rsd=1e-12, precision=cb.F64)
+    assert lib.cpsb_gauge_free(g.h) == -7          # CPSB_ERR_BUSY: the request holds the field
+    assert b"request" in lib.cpsb_last_error()
+    xs, res, _ = srv.wait(rid)
+    srv.close()
+    assert all(r.status == 0 for r in res)
+    assert lib.cpsb_gauge_free(g.h) == 0
+    g.h = None

@@ -246,3 +246,23 @@ def test_zmobius_bitexact(name):
         out, it, tr = op.zfmatinv(full, guess, dminus=1)
         np.testing.assert_array_equal(out, rec["zfmatinv_sol"])
         assert it == int(rec["zfmatinv_iters"]) and tr == float(rec["zfmatinv_true_res"])
+
+
+def test_bench_lattice_bitexact():
+    """The benchmark lattice (DWF 16^3x32, Ls 16, bench.py's links and first
+    source): the oracle's Dslash and MatPcDagMatPc equal the compiled
+    reference's bit for bit (SHA-256 of the outputs) and so does the dot."""
+    import os
+
+    from cps_public_b200 import fields
+    from tests.golden_util import GOLDEN, sha
+    rec = dict(np.load(os.path.join(GOLDEN, "bench_dwf_16x16x16x32_ls16.npz")))
+    dims, ls = tuple(int(d) for d in rec["dims"]), int(rec["ls"])
+    u = fields.random_gauge(dims, float(rec["eps"]), int(rec["seed"]))
+    src = fields.random_source(int(np.prod(dims)) // 2 * ls, int(rec["src_seed"]))
+    assert sha(u) == str(rec["gauge_sha"]) and sha(src) == str(rec["src_sha"])
+    op = oracle.Op("dwf", dims, u, ls=ls, mass=float(rec["mass"]), m5=float(rec["m5"]))
+    assert sha(op.dslash(src, 1, 0)) == str(rec["dslash_sha"])
+    out, dot = op.mdagm(src)
+    assert sha(out) == str(rec["mdagm_sha"])
+    assert dot == float(rec["mdagm_dot"])
