@@ -36,5 +36,7 @@ void check_params(cpsb_gauge h, const cpsb_dirac_params *p);
 void check_cg(const cpsb_cg_arg *a);
 // Sites of one checkerboard vector (4-D half volume x Ls).
 long cb_sites(cpsb_gauge h, const cpsb_dirac_params *p);
+// Geometry (column layout) of the checkerboard fields of this operator.
+Geom geom_of(cpsb_gauge h, const cpsb_dirac_params *p, int nrhs);
 
 }  // namespace cpsb

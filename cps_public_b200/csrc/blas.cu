@@ -21,27 +21,43 @@ int grid_blocks(long sites_per_rhs, int nt) {
 }
 
 // ---------------------------------------------------------------- packing
+// CPS order (right-hand side, then slice s, then 4-D checkerboard site x; 24
+// doubles per site) <-> the column layout of cpsb_device.cuh.  Threads walk
+// the device entries in order, so device chunks are read or written in whole
+// 128-byte segments and each thread moves its site's 192 contiguous CPS bytes.
+__device__ __forceinline__ long cps_index(const Geom &g, unsigned e) {
+  const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
+  const unsigned rhs = e / per;
+  const unsigned j = e - rhs * per;
+  const int k = (g.ncls == 2 && j >= (unsigned)g.kb1) ? 1 : 0;
+  const unsigned jj = j - (k ? (unsigned)g.kb1 : 0u);
+  const unsigned c = (unsigned)g.cs[k];
+  const unsigned x = jj / c, sp = jj - x * c;
+  const unsigned s = g.ncls == 2 ? (unsigned)k + 2 * sp : sp;
+  return (long)rhs * per + (long)s * g.n4cb + x;
+}
+
 template <int P>
-__global__ void pack_kernel(SpinorPtr dst, const double *src, long n) {
+__global__ void pack_kernel(SpinorPtr dst, const double *src, Geom g) {
   typedef typename PrecTraits<P>::real T;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < g.nsites; e += (long)gridDim.x * blockDim.x) {
     Spinor<T> s;
-    const double2 *p = (const double2 *)(src + 24 * i);
+    const double2 *p = (const double2 *)(src + 24 * cps_index(g, (unsigned)e));
 #pragma unroll
     for (int k = 0; k < 12; k++) {
       double2 v = p[k];
       s.c[k / 3][k % 3] = mk((T)v.x, (T)v.y);
     }
-    store_spinor<P>(dst, i, s);
+    store_spinor<P>(dst, e, s);
   }
 }
 
 template <int P>
-__global__ void unpack_kernel(double *dst, SpinorPtr src, long n) {
+__global__ void unpack_kernel(double *dst, SpinorPtr src, Geom g) {
   typedef typename PrecTraits<P>::real T;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    Spinor<T> s = load_spinor<P>(src, i);
-    double2 *p = (double2 *)(dst + 24 * i);
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < g.nsites; e += (long)gridDim.x * blockDim.x) {
+    Spinor<T> s = load_spinor<P>(src, e);
+    double2 *p = (double2 *)(dst + 24 * cps_index(g, (unsigned)e));
 #pragma unroll
     for (int k = 0; k < 12; k++) p[k] = make_double2((double)s.c[k / 3][k % 3].re, (double)s.c[k / 3][k % 3].im);
   }
@@ -61,17 +77,19 @@ static int flat_grid(long n) {
   return (int)(nb < 1 ? 1 : nb);
 }
 
-cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, long n, cudaStream_t st) {
-  if (prec == P64) pack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  else if (prec == P32) pack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  else pack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
+cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, const Geom &g, cudaStream_t st) {
+  const long n = g.nsites;
+  if (prec == P64) pack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
+  else if (prec == P32) pack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
+  else pack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
   return launched();
 }
 
-cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, long n, cudaStream_t st) {
-  if (prec == P64) unpack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  else if (prec == P32) unpack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
-  else unpack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, n);
+cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, const Geom &g, cudaStream_t st) {
+  const long n = g.nsites;
+  if (prec == P64) unpack_kernel<P64><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
+  else if (prec == P32) unpack_kernel<P32><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
+  else unpack_kernel<P16><<<flat_grid(n), 256, 0, st>>>(dst, src, g);
   return launched();
 }
 

@@ -47,6 +47,10 @@ long cb_sites(cpsb_gauge h, const cpsb_dirac_params *p) {
   return h->g.n4cb * (p->action == CPSB_WILSON ? 1 : p->ls);
 }
 
+Geom geom_of(cpsb_gauge h, const cpsb_dirac_params *p, int nrhs) {
+  return make_geom(h->g.dims, p->action == CPSB_WILSON ? 1 : p->ls, nrhs, p->action == CPSB_DWF);
+}
+
 }  // namespace cpsb
 
 namespace {
@@ -228,7 +232,8 @@ namespace {
 // Copies nvec host vectors (each nsites_each*24 doubles, CPS order) into the
 // multi-RHS field f one right-hand side at a time through a pinned buffer and
 // a device buffer of one vector, packing each into its slice of f.
-void upload(Field &f, const double *const *host, int nvec, long nsites_each, cudaStream_t st) {
+void upload(Field &f, const double *const *host, int nvec, const Geom &g1, cudaStream_t st) {
+  const long nsites_each = g1.nsites;
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
   Staging &sg = staging();
   std::lock_guard<std::mutex> lk(sg.mu);
@@ -238,13 +243,14 @@ void upload(Field &f, const double *const *host, int nvec, long nsites_each, cud
     CK(cudaEventSynchronize(sg.done[k]));  // the device is done with pin[k] / dev[k]
     par_copy(sg.pin[k], host[i], each);
     CK(cudaMemcpyAsync(sg.dev[k].p, sg.pin[k], each, cudaMemcpyHostToDevice, st));
-    CK(launch_pack(f.prec, f.view((long)i * nsites_each), (const double *)sg.dev[k].p, nsites_each, st));
+    CK(launch_pack(f.prec, f.view((long)i * nsites_each), (const double *)sg.dev[k].p, g1, st));
     CK(cudaEventRecord(sg.done[k], st));
   }
   CK(cudaStreamSynchronize(st));
 }
 
-void download(double *const *host, int nvec, long nsites_each, const Field &f, cudaStream_t st) {
+void download(double *const *host, int nvec, const Geom &g1, const Field &f, cudaStream_t st) {
+  const long nsites_each = g1.nsites;
   const size_t each = (size_t)nsites_each * 24 * sizeof(double);
   Staging &sg = staging();
   std::lock_guard<std::mutex> lk(sg.mu);
@@ -253,7 +259,7 @@ void download(double *const *host, int nvec, long nsites_each, const Field &f, c
   for (int i = 0; i <= nvec; i++) {
     if (i < nvec) {
       const int k = i & 1;
-      CK(launch_unpack(f.prec, (double *)sg.dev[k].p, f.view((long)i * nsites_each), nsites_each, st));
+      CK(launch_unpack(f.prec, (double *)sg.dev[k].p, f.view((long)i * nsites_each), g1, st));
       CK(cudaMemcpyAsync(sg.pin[k], sg.dev[k].p, each, cudaMemcpyDeviceToHost, st));
       CK(cudaEventRecord(sg.done[k], st));
     }
@@ -277,9 +283,9 @@ int cpsb_dslash(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const dou
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     Field fi(P64, op.nsites()), fo(P64, op.nsites());
-    upload(fi, &in, 1, op.nsites(), st);
+    upload(fi, &in, 1, op.geom, st);
     op.dslash(fo, fi, cb, dag, st);
-    download(&out, 1, op.nsites(), fo, st);
+    download(&out, 1, op.geom, fo, st);
     return CPSB_OK;
   });
 }
@@ -292,9 +298,9 @@ int cpsb_matpc(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const doub
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, P64, 1);
     Field fi(P64, op.nsites()), fo(P64, op.nsites());
-    upload(fi, &in, 1, op.nsites(), st);
+    upload(fi, &in, 1, op.geom, st);
     op.matpc(fo, fi, dag, nullptr, nullptr, st);
-    download(&out, 1, op.nsites(), fo, st);
+    download(&out, 1, op.geom, fo, st);
     return CPSB_OK;
   });
 }
@@ -310,10 +316,10 @@ int cpsb_mdagm(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const doub
     RedSlot rs;
     DevBuf d(sizeof(double) * MAX_RHS);
     Reduce r = rs.r((double *)d.p);
-    upload(fi, &in, 1, op.nsites(), st);
+    upload(fi, &in, 1, op.geom, st);
     op.mdagm(fo, fi, &r, nullptr, st);
     if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-    download(&out, 1, op.nsites(), fo, st);
+    download(&out, 1, op.geom, fo, st);
     return CPSB_OK;
   });
 }
@@ -328,9 +334,9 @@ int cpsb_dslash_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, doub
     cudaStream_t st = ctx().stream;
     Operator op(&h->g, *p, precision, 1);
     Field fi(precision, op.nsites()), fo(precision, op.nsites());
-    upload(fi, &in, 1, op.nsites(), st);
+    upload(fi, &in, 1, op.geom, st);
     op.dslash(fo, fi, cb, dag, st);
-    download(&out, 1, op.nsites(), fo, st);
+    download(&out, 1, op.geom, fo, st);
     return CPSB_OK;
   });
 }
@@ -348,10 +354,10 @@ int cpsb_mdagm_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, doubl
     RedSlot rs;
     DevBuf d(sizeof(double) * MAX_RHS);
     Reduce r = rs.r((double *)d.p);
-    upload(fi, &in, 1, op.nsites(), st);
+    upload(fi, &in, 1, op.geom, st);
     op.mdagm(fo, fi, &r, nullptr, st);
     if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-    download(&out, 1, op.nsites(), fo, st);
+    download(&out, 1, op.geom, fo, st);
     return CPSB_OK;
   });
 }
@@ -368,9 +374,9 @@ int cpsb_mdagm_dev(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const 
     RedSlot rs;
     DevBuf d(sizeof(double) * MAX_RHS);
     Reduce r = rs.r((double *)d.p);
-    CK(launch_pack(P64, fi.ptr(), in, op.nsites(), st));
+    CK(launch_pack(P64, fi.ptr(), in, op.geom, st));
     op.mdagm(fo, fi, &r, nullptr, st);
-    CK(launch_unpack(P64, out, fo.ptr(), op.nsites(), st));
+    CK(launch_unpack(P64, out, fo.ptr(), op.geom, st));
     if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return CPSB_OK;
@@ -388,9 +394,9 @@ int cpsb_dslash_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precisio
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
     Operator op(&h->g, *p, precision, nrhs);
     Field fi(precision, op.nsites()), fo(precision, op.nsites());
-    CK(launch_pack(precision, fi.ptr(), in, op.nsites(), st));
+    CK(launch_pack(precision, fi.ptr(), in, op.geom, st));
     op.dslash(fo, fi, cb, dag, st);
-    CK(launch_unpack(precision, out, fo.ptr(), op.nsites(), st));
+    CK(launch_unpack(precision, out, fo.ptr(), op.geom, st));
     CK(cudaStreamSynchronize(st));
     return CPSB_OK;
   });
@@ -410,9 +416,9 @@ int cpsb_mdagm_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision
     RedSlot rs;
     DevBuf d(sizeof(double) * MAX_RHS);
     Reduce r = rs.r((double *)d.p);
-    CK(launch_pack(precision, fi.ptr(), in, op.nsites(), st));
+    CK(launch_pack(precision, fi.ptr(), in, op.geom, st));
     op.mdagm(fo, fi, &r, nullptr, st);
-    CK(launch_unpack(precision, out, fo.ptr(), op.nsites(), st));
+    CK(launch_unpack(precision, out, fo.ptr(), op.geom, st));
     if (dot) CK(cudaMemcpyAsync(dot, d.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return CPSB_OK;
@@ -432,11 +438,11 @@ int cpsb_invcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg
     cudaStream_t st = ctx().stream;
     CgSolver *s = get_solver(&h->g, *p, a->precision, nrhs);
     std::lock_guard<std::mutex> lk(s->busy);
-    const long n = cb_sites(h, p);
-    upload(s->x64, (const double *const *)x, nrhs, n, st);
-    upload(s->b64, b, nrhs, n, st);
+    const Geom g1 = geom_of(h, p, 1);
+    upload(s->x64, (const double *const *)x, nrhs, g1, st);
+    upload(s->b64, b, nrhs, g1, st);
     int rc = s->solve(*a, res, st);
-    download(x, nrhs, n, s->x64, st);
+    download(x, nrhs, g1, s->x64, st);
     return rc;
   });
 }
@@ -458,10 +464,10 @@ int cpsb_invcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
     CgSolver *s = get_solver(&h->g, *p, a->precision, nrhs);
     std::lock_guard<std::mutex> lk(s->busy);
-    CK(launch_pack(P64, s->x64.ptr(), x, s->x64.nsites, st));
-    CK(launch_pack(P64, s->b64.ptr(), b, s->b64.nsites, st));
+    CK(launch_pack(P64, s->x64.ptr(), x, s->geom, st));
+    CK(launch_pack(P64, s->b64.ptr(), b, s->geom, st));
     int rc = s->solve(*a, res, st);
-    CK(launch_unpack(P64, x, s->x64.ptr(), s->x64.nsites, st));
+    CK(launch_unpack(P64, x, s->x64.ptr(), s->geom, st));
     CK(cudaStreamSynchronize(st));
     return rc;
   });
@@ -487,8 +493,9 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
       if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
     cudaStream_t st = ctx().stream;
     const long n = cb_sites(h, p);
+    const Geom g1 = geom_of(h, p, 1);
     Field chi(P64, n);
-    upload(chi, &b, 1, n, st);
+    upload(chi, &b, 1, g1, st);
     std::vector<Field> xs(nvec);
     for (int i = 0; i < nvec; i++) {
       xs[i].create(P64, n);
@@ -497,7 +504,7 @@ int cpsb_minvcg(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, 
     cpsb_solve_result r;
     memset(&r, 0, sizeof(r));
     const int rc = multishift(&h->g, *p, *a, chi, xs, shift, nshift, rsd, type, alpha, &r, st);
-    for (int i = 0; i < nvec; i++) download(&x[i], 1, n, xs[i], st);
+    for (int i = 0; i < nvec; i++) download(&x[i], 1, g1, xs[i], st);
     if (res) *res = r;
     return rc;
   });
@@ -518,8 +525,9 @@ int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg 
       if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
     const long n = cb_sites(h, p);
+    const Geom g1 = geom_of(h, p, 1);
     Field chi(P64, n);
-    CK(launch_pack(P64, chi.ptr(), b, n, st));
+    CK(launch_pack(P64, chi.ptr(), b, g1, st));
     std::vector<Field> xs(nvec);
     for (int i = 0; i < nvec; i++) {
       xs[i].create(P64, n);
@@ -528,7 +536,7 @@ int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg 
     cpsb_solve_result r;
     memset(&r, 0, sizeof(r));
     const int rc = multishift(&h->g, *p, *a, chi, xs, shift, nshift, rsd, type, alpha, &r, st);
-    for (int i = 0; i < nvec; i++) CK(launch_unpack(P64, x[i], xs[i].ptr(), n, st));
+    for (int i = 0; i < nvec; i++) CK(launch_unpack(P64, x[i], xs[i].ptr(), g1, st));
     CK(cudaStreamSynchronize(st));
     if (res) *res = r;
     return rc;
@@ -602,9 +610,9 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
     const double *in_c = in + (mob ? 24 * n : 0), *in_e = in + (mob ? 0 : 24 * n);
     double *out_c = out + (mob ? 24 * n : 0), *out_e = out + (mob ? 0 : 24 * n);
     Field fin_c(P64, n), fin_e(P64, n), fout_c(P64, n), fout_e(P64, n), t(P64, n), t2(P64, n);
-    upload(fin_c, &in_c, 1, n, st);
-    upload(fin_e, &in_e, 1, n, st);
-    upload(fout_c, (const double *const *)&out_c, 1, n, st);
+    upload(fin_c, &in_c, 1, g, st);
+    upload(fin_e, &in_e, 1, g, st);
+    upload(fout_c, (const double *const *)&out_c, 1, g, st);
     Reduce none;
     memset(&none, 0, sizeof(none));
     const ZM5Tab *zt = zm ? (const ZM5Tab *)op.ztab.p : nullptr;
@@ -691,8 +699,8 @@ static int matinv_impl(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_a
       lin(fout_e, 2 * kb, fout_e, 0.0, nullptr);
       lin(fout_c, 2 * kb, fout_c, 0.0, nullptr);
     }
-    download(&out_c, 1, n, fout_c, st);
-    download(&out_e, 1, n, fout_e, st);
+    download(&out_c, 1, g, fout_c, st);
+    download(&out_e, 1, g, fout_e, st);
     return rc;
   });
 }
@@ -727,12 +735,12 @@ int cpsb_dminus(cpsb_gauge h, const cpsb_dirac_params *p, double *out, const dou
     const double *in_e = in + (zm ? 24 * n : 0), *in_o = in + (zm ? 0 : 24 * n);
     double *out_e = out + (zm ? 24 * n : 0), *out_o = out + (zm ? 0 : 24 * n);
     Field fe(P64, n), fo(P64, n), ge(P64, n), go(P64, n);
-    upload(fe, &in_e, 1, n, st);
-    upload(fo, &in_o, 1, n, st);
+    upload(fe, &in_e, 1, op.geom, st);
+    upload(fo, &in_o, 1, op.geom, st);
     if (!zm) mobius_dminus_dev(op, *p, ge, go, fe, fo, st);
     else zmobius_dminus_dev(op, go, ge, fo, fe, st);
-    download(&out_e, 1, n, ge, st);
-    download(&out_o, 1, n, go, st);
+    download(&out_e, 1, op.geom, ge, st);
+    download(&out_o, 1, op.geom, go, st);
     return CPSB_OK;
   });
 }
@@ -774,11 +782,11 @@ int cpsb_minresext(cpsb_gauge h, const cpsb_dirac_params *p, double *psi, const 
     }
     Field fphi(P64, n), fpsi(P64, n), fr(P64, n);
     std::vector<Field> fv(degree), fvm(degree);
-    upload(fphi, &phi, 1, n, st);
+    upload(fphi, &phi, 1, g, st);
     for (int i = 0; i < degree; i++) {
       fv[i].create(P64, n);
       fvm[i].create(P64, n);
-      upload(fv[i], (const double *const *)&v[i], 1, n, st);
+      upload(fv[i], (const double *const *)&v[i], 1, g, st);
     }
     RedSlot rs;
     DevBuf dres(sizeof(double) * 4);
@@ -857,10 +865,10 @@ int cpsb_minresext(cpsb_gauge h, const cpsb_dirac_params *p, double *psi, const 
       CK(launch_caxpy(fr.ptr(), -a[i].real(), -a[i].imag(), fvm[i].ptr(), fr.ptr(), n, st));
     }
     if (resid) *resid = sqrt(norm2(fr) / norm2(fphi));
-    download(&psi, 1, n, fpsi, st);
+    download(&psi, 1, g, fpsi, st);
     for (int i = 0; i < degree; i++) {
-      download(&v[i], 1, n, fv[i], st);
-      download(&vm[i], 1, n, fvm[i], st);
+      download(&v[i], 1, g, fv[i], st);
+      download(&vm[i], 1, g, fvm[i], st);
     }
     return CPSB_OK;
   });

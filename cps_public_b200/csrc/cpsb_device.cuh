@@ -1,11 +1,13 @@
 // cpsb_device.cuh -- device-side building blocks shared by the sm_100a kernels.
 //
-// Field layouts in HBM (all "chunked structure of arrays" so that a warp's
-// 32 consecutive sites read one 16-byte chunk each in a single 512-byte
-// transaction):
+// Field layouts in HBM:
 //
-//  * spinor field of N sites (a 4-D checkerboard, or Ls such slices, or
-//    Nrhs x Ls slices): chunk k of site i lives at base[k*N + i].
+//  * spinor field (a 4-D checkerboard, or Ls such slices, or Nrhs x Ls
+//    slices): entries ordered by right-hand side, then column (4-D site and
+//    slice class, site_entry below), then slice; stored in blocks of 8
+//    entries, chunk k of the block's 8 entries as one 128-byte segment
+//    (entry_ptr below), so a warp's 32 consecutive entries read four aligned
+//    128-byte segments per chunk.  A chunk is 16 bytes:
 //      FP64: 12 chunks of double2 = one complex component (spin k/3, colour k%3)
 //      FP32:  6 chunks of float4, spin-paired: chunk 3p+c holds colour c of the
 //             spins (2p, 2p+1) as (re_2p, re_2p+1, im_2p, im_2p+1), so the two
@@ -67,7 +69,34 @@ struct Geom {
   int ls;           // slices per right-hand side (1 for Wilson)
   int nrhs;         // right-hand sides stacked along the slowest index
   long nsites;      // n4cb * ls * nrhs = sites of one checkerboard field
+  // Column layout (see below): ncls slice classes (2 for the DWF 5-D
+  // checkerboard, where class k holds the slices s = k, k+2, ...; 1 otherwise),
+  // cs[k] slices per column of class k, kb1 = first entry of class 1.
+  int ncls;
+  int cs[2];
+  int kb1;
 };
+
+// Entry of slice s of 4-D checkerboard site x within one right-hand side.
+// A field is stored as columns: the entries of one (site x, slice class k)
+// pair are consecutive, ordered by slice, and the columns of class 0 precede
+// those of class 1:  entry = k*kb1 + x*cs[k] + s/ncls.  Right-hand side q
+// adds q * n4cb * ls.  Every slice of a class shares the 4-D parity of its
+// sites, so the 4-D neighbours of a column are whole columns of the input.
+__host__ __device__ __forceinline__ unsigned site_entry(const Geom &g, int s, int x) {
+  const int k = g.ncls == 2 ? (s & 1) : 0;
+  const int sp = g.ncls == 2 ? (s >> 1) : s;
+  return (k ? (unsigned)g.kb1 : 0u) + (unsigned)x * (unsigned)g.cs[k] + (unsigned)sp;
+}
+
+// Entries are stored in blocks of 8: block b holds chunk 0 of its 8 entries,
+// then chunk 1, ... (chunks are 16 bytes), so chunk k of entry i sits at
+// entry_ptr(i)[8*k] and 8 consecutive entries read one 128-byte segment per
+// chunk.  NCH chunks per entry: 12 (FP64), 6 (FP32), 3 (16-bit).
+template <int NCH, typename V>
+__device__ __forceinline__ V *entry_ptr(const void *base, unsigned i) {
+  return (V *)((const char *)base + (size_t)((i >> 3) * (unsigned)NCH) * 128u + (size_t)(i & 7u) * 16u);
+}
 
 struct Coord { int x, y, z, t; };
 
@@ -95,7 +124,7 @@ __device__ __forceinline__ int cbindex(const Geom &g, int x, int y, int z, int t
 struct SpinorPtr {
   void *data;
   float *norm;   // FP16 only
-  long stride;   // sites in the field (chunk stride)
+  long stride;   // entries in the field
 };
 
 template <int P> struct PrecTraits;
@@ -124,11 +153,11 @@ __device__ __forceinline__ Spinor<typename PrecTraits<P>::real> load_spinor(cons
 
 template <>
 __device__ __forceinline__ Spinor<double> load_spinor<P64>(const SpinorPtr &f, long i) {
-  const double2 *b = (const double2 *)f.data;
+  const double2 *b = entry_ptr<12, const double2>(f.data, (unsigned)i);
   Spinor<double> s;
 #pragma unroll
   for (int k = 0; k < 12; k++) {
-    double2 v = __ldg(b + k * f.stride + i);
+    double2 v = __ldg(b + 8 * k);
     s.c[k / 3][k % 3] = mk(v.x, v.y);
   }
   return s;
@@ -136,11 +165,11 @@ __device__ __forceinline__ Spinor<double> load_spinor<P64>(const SpinorPtr &f, l
 
 template <>
 __device__ __forceinline__ Spinor<float> load_spinor<P32>(const SpinorPtr &f, long i) {
-  const float4 *b = (const float4 *)f.data;
+  const float4 *b = entry_ptr<6, const float4>(f.data, (unsigned)i);
   Spinor<float> s;
 #pragma unroll
   for (int k = 0; k < 6; k++) {
-    float4 v = __ldg(b + k * f.stride + i);
+    float4 v = __ldg(b + 8 * k);
     const int p = k / 3, c = k % 3;
     s.c[2 * p][c] = mk(v.x, v.z);
     s.c[2 * p + 1][c] = mk(v.y, v.w);
@@ -150,12 +179,12 @@ __device__ __forceinline__ Spinor<float> load_spinor<P32>(const SpinorPtr &f, lo
 
 template <>
 __device__ __forceinline__ Spinor<float> load_spinor<P16>(const SpinorPtr &f, long i) {
-  const uint4 *b = (const uint4 *)f.data;
+  const uint4 *b = entry_ptr<3, const uint4>(f.data, (unsigned)i);
   const float nrm = __ldg(f.norm + i);
   Spinor<float> s;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    uint4 v = __ldg(b + k * f.stride + i);
+    uint4 v = __ldg(b + 8 * k);
     const unsigned w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int j = 0; j < 4; j += 2) {
@@ -173,18 +202,18 @@ __device__ __forceinline__ void store_spinor(const SpinorPtr &f, long i, const S
 
 template <>
 __device__ __forceinline__ void store_spinor<P64>(const SpinorPtr &f, long i, const Spinor<double> &s) {
-  double2 *b = (double2 *)f.data;
+  double2 *b = entry_ptr<12, double2>(f.data, (unsigned)i);
 #pragma unroll
-  for (int k = 0; k < 12; k++) b[k * f.stride + i] = make_double2(s.c[k / 3][k % 3].re, s.c[k / 3][k % 3].im);
+  for (int k = 0; k < 12; k++) b[8 * k] = make_double2(s.c[k / 3][k % 3].re, s.c[k / 3][k % 3].im);
 }
 
 template <>
 __device__ __forceinline__ void store_spinor<P32>(const SpinorPtr &f, long i, const Spinor<float> &s) {
-  float4 *b = (float4 *)f.data;
+  float4 *b = entry_ptr<6, float4>(f.data, (unsigned)i);
 #pragma unroll
   for (int k = 0; k < 6; k++) {
     const int p = k / 3, c = k % 3;
-    b[k * f.stride + i] = make_float4(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, s.c[2 * p][c].im, s.c[2 * p + 1][c].im);
+    b[8 * k] = make_float4(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, s.c[2 * p][c].im, s.c[2 * p + 1][c].im);
   }
 }
 
@@ -197,7 +226,7 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
     for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf(s.c[a][c].re), fabsf(s.c[a][c].im)));
   const float scale = m > 0.f ? 32767.0f / m : 0.f;
   f.norm[i] = m * (1.0f / 32767.0f);
-  uint4 *b = (uint4 *)f.data;
+  uint4 *b = entry_ptr<3, uint4>(f.data, (unsigned)i);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     unsigned w[4];
@@ -208,7 +237,7 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
       w[j] = enc16x2(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, scale);
       w[j + 1] = enc16x2(s.c[2 * p][c].im, s.c[2 * p + 1][c].im, scale);
     }
-    b[k * f.stride + i] = make_uint4(w[0], w[1], w[2], w[3]);
+    b[8 * k] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 

@@ -28,9 +28,8 @@ struct DslashArgs {
   double bc_t_sign;       // -1: reconstructed links need the antiperiodic sign at the t boundary
   Reduce red;             // |out|^2 per RHS when requested
   const int *skip;        // per-RHS: nonzero skips that RHS (device memory), may be null
-  int sl;                 // slice lanes per block (set by the launcher)
-  // Fused CG residual update (parity-class FP32 / 16-bit kernels only): when
-  // cg is set, out = x + a D in is not stored; instead r -= alpha (out +
+  int rg;                 // right-hand sides per warp lane group (set by the launcher)
+  // Fused CG residual update: when cg is set, out = x + a D in is not stored; instead r -= alpha (out +
   // shift p) with alpha from cg, |r|^2 per RHS is reduced, and the last block
   // advances the recurrence scalars as the r-update kernel of blas.cu does.
   CgState *cg;
@@ -52,10 +51,10 @@ inline cudaError_t launched() {
 // Grid: blockIdx.y = right-hand side, blockIdx.x strides over the sites of one RHS.
 int grid_blocks(long sites_per_rhs, int nt);
 
-// variant: launch shape 0..NUM_DSLASH_VARIANTS-1 (dslash_impl.cuh: 0-6 for FP64;
-// dslash_x2.cuh: 0-11 for FP32 / 16-bit), chosen by the autotuner; a launcher
-// returns cudaErrorNotSupported for shapes it does not have.
-constexpr int NUM_DSLASH_VARIANTS = 12;
+// variant: launch shape 0..NUM_DSLASH_VARIANTS-1 of hop.cuh, chosen by the
+// autotuner; a launcher returns cudaErrorNotSupported for shapes that do not
+// fit the operator.
+constexpr int NUM_DSLASH_VARIANTS = 6;
 cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st);
 
 // ---------------------------------------------------------------- BLAS
@@ -64,8 +63,9 @@ cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int
 // CUDA graphs and need no host round trip.
 struct CgState;   // defined in cg_state.h
 
-cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, long nsites, cudaStream_t st);
-cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, long nsites, cudaStream_t st);
+// CPS-order vectors <-> device fields of geometry g (g.nsites entries).
+cudaError_t launch_pack(int prec, SpinorPtr dst, const double *src, const Geom &g, cudaStream_t st);
+cudaError_t launch_unpack(int prec, double *dst, SpinorPtr src, const Geom &g, cudaStream_t st);
 cudaError_t launch_convert(int pdst, SpinorPtr dst, int psrc, SpinorPtr src, long nsites, cudaStream_t st);
 cudaError_t launch_fconvert(double *out, const double *in, const int dims[4], int ls, int order, int direction,
                             cudaStream_t st);

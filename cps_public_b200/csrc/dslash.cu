@@ -1,4 +1,4 @@
-// dslash.cu -- precision dispatch of the hopping kernels (dslash_impl.cuh).
+// dslash.cu -- precision dispatch of the hopping kernel (hop.cuh).
 #include "cpsb_kernels.h"
 
 namespace cpsb {

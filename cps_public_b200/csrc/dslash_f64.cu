@@ -1,9 +1,9 @@
-// dslash_f64.cu -- instantiates the hopping kernels of dslash_impl.cuh for P64
-// storage (one translation unit per precision so they compile in parallel).
-#include "dslash_impl.cuh"
+// dslash_f64.cu -- instantiates the hopping kernel of hop.cuh for FP64
+// storage (one translation unit per precision, so they compile in parallel).
+#include "hop.cuh"
 
 namespace cpsb {
 cudaError_t launch_dslash_f64(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
-  return dslash_launch_p<P64>(A, xpay, norm, variant, st);
+  return hop_launch_p<P64>(A, xpay, norm, variant, st);
 }
 }  // namespace cpsb

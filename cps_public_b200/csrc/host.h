@@ -72,15 +72,21 @@ struct Field {
   Field(int prec, long nsites) { create(prec, nsites); }
   void create(int prec, long nsites);
   SpinorPtr ptr() const { return SpinorPtr{data.p, (float *)norm.p, nsites}; }
-  // The sites [off, off + n) of the field as a field of its own (same chunk
-  // stride): one right-hand side of a multi-RHS field.  Chunks are 16 bytes
-  // in every precision.
+  // The entries [off, off + n) of the field as a field of its own: one
+  // right-hand side of a multi-RHS field.  off is a multiple of 8 (a whole
+  // number of 8-entry blocks; every right-hand side is, since n4cb is).
   SpinorPtr view(long off) const {
-    return SpinorPtr{(char *)data.p + off * 16, norm.p ? (float *)norm.p + off : nullptr, nsites};
+    const long chunks = prec == P64 ? 12 : prec == P32 ? 6 : 3;
+    return SpinorPtr{(char *)data.p + off * chunks * 16, norm.p ? (float *)norm.p + off : nullptr, nsites - off};
   }
   size_t bytes() const { return data.bytes + norm.bytes; }
 };
 size_t field_bytes(int prec, long nsites);
+
+// Geometry of the checkerboard fields of an operator on a lattice of dims:
+// Ls slices (1 for Wilson), nrhs right-hand sides, DWF 5-D checkerboarding
+// (five_d: two slice classes) or one class.
+Geom make_geom(const int dims[4], int ls, int nrhs, bool five_d);
 
 // Reduction slot: partials for every block of a launch, a ticket and results.
 struct RedSlot {
@@ -133,10 +139,10 @@ struct Operator {
     mdagm(out.ptr(), in.ptr(), red, skip, st);
   }
   // MatPcDagMatPc p with the CG residual update fused into its last hop
-  // (Wilson / DWF in FP32 or 16-bit): |MatPc p|^2 -> red_d, then
+  // (Wilson / DWF, every precision): |MatPc p|^2 -> red_d, then
   // r -= alpha (A p + shift p), |r|^2 and the recurrence scalars in S; A p is
   // not stored (scratch receives it only while a launch shape is being tuned).
-  bool can_fuse_cg_r() const { return prec != P64 && (p.action == CPSB_WILSON || p.action == CPSB_DWF); }
+  bool can_fuse_cg_r() const { return p.action == CPSB_WILSON || p.action == CPSB_DWF; }
   bool mobius_like() const { return p.action == CPSB_MOBIUS || p.action == CPSB_ZMOBIUS; }
   void matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
                      cudaStream_t st);

@@ -6,103 +6,39 @@
 // a forward and a backward sweep along s per 4-D site and chirality with the
 // domain-wall wall correction, and the mixing  b*psi_s + c*(P+ psi_{s-1} +
 // P- psi_{s+1})  with -m_f walls of zmobius_kappa_dslash_5_plus_cmplx
-// (zmobius_dslash_5_plus.C:125-376).  The sweeps are independent for every
-// complex spinor component, so one thread owns one (site, storage chunk) column
-// of Ls values in registers and the pass reads and writes each value once.
+// (zmobius_dslash_5_plus.C:125-376); and the zMobius form with complex
+// per-slice coefficients from a table.  The sweeps are independent for every
+// complex spinor component.
 //
 //   dag 0:  out = scale * mix(M5^-1 in)                 (precedes D_W in MatPc)
 //   dag 1:  out = [x +] scale * M5^-dag(mix^dag(in))    (follows D_W^dag in MatPcDag)
 //
-// 16-bit storage: a chunk is one (chirality pair, colour) of both spins, half
-// of a stored uint4 -- the same values as an FP32 chunk -- so the column
-// arithmetic is shared.  The site's quantum is the maximum over its six
-// chunks, so a site's chunks sit in one 8-lane group of a warp (two lanes
-// idle) and the group agrees on the maximum by shuffles before encoding.
+// In the column layout (cpsb_device.cuh) the Ls slices of a 4-D site are
+// consecutive entries, so a block moves a tile of whole columns between HBM
+// and shared memory with coalesced 16-byte accesses (one entry per thread),
+// and the sweeps run from shared memory, one thread per (site, storage chunk)
+// with the column of Ls values in registers: every value is read from HBM and
+// written once.  16-bit storage is decoded on the way in and encoded per site
+// (its quantum is the site's maximum) on the way out; the sweep arithmetic is
+// FP32.
+#include <string.h>
+
 #include "blas.h"
 
 namespace cpsb {
 
+// Per storage precision: the real type of the sweeps, the complex values a
+// chunk holds (NC) and the chunks of a site (NCH).  FP64 chunk k is component
+// (spin k/3, colour k%3); FP32 / 16-bit chunk k = 3p + c holds colour c of the
+// spins 2p and 2p+1.  Chunks k < NCH/2 are the upper chirality (spins 0, 1).
 template <int P> struct ChunkT;
 template <> struct ChunkT<P64> { static const int NCH = 12, NC = 1; typedef double T; };
 template <> struct ChunkT<P32> { static const int NCH = 6, NC = 2; typedef float T; };
 template <> struct ChunkT<P16> { static const int NCH = 6, NC = 2; typedef float T; };
 
-template <int P>
-__device__ __forceinline__ void ld_chunk(const SpinorPtr &f, long i, int k, cplx<typename ChunkT<P>::T> *v);
-template <>
-__device__ __forceinline__ void ld_chunk<P64>(const SpinorPtr &f, long i, int k, cplx<double> *v) {
-  double2 a = __ldg((const double2 *)f.data + k * f.stride + i);
-  v[0] = mk(a.x, a.y);
-}
-template <>
-__device__ __forceinline__ void ld_chunk<P32>(const SpinorPtr &f, long i, int k, cplx<float> *v) {
-  float4 a = __ldg((const float4 *)f.data + k * f.stride + i);  // spin-paired chunk
-  v[0] = mk(a.x, a.z);
-  v[1] = mk(a.y, a.w);
-}
-// A 16-bit column of Ls slices, chunk j = 3p + c (words 2j (Re) and 2j+1 (Im)
-// of each site, both spins in each word): all raw loads issued first, then
-// decoded, so the Ls loads are in flight together.
-template <int LS>
-__device__ __forceinline__ void ld_column16(const SpinorPtr &f, long base, long step, int j, cplx<float> (&v)[LS][2]) {
-  uint2 w[LS];
-  float q[LS];
-#pragma unroll
-  for (int s = 0; s < LS; s++) {
-    const long i = base + (long)s * step;
-    w[s] = __ldg((const uint2 *)((const uint4 *)f.data + (long)(j >> 1) * f.stride + i) + (j & 1));
-    q[s] = __ldg(f.norm + i);
-  }
-#pragma unroll
-  for (int s = 0; s < LS; s++) {
-    v[s][0] = mk(dec16(w[s].x, 0) * q[s], dec16(w[s].y, 0) * q[s]);
-    v[s][1] = mk(dec16(w[s].x, 1) * q[s], dec16(w[s].y, 1) * q[s]);
-  }
-}
-template <int P>
-__device__ __forceinline__ void st_chunk(const SpinorPtr &f, long i, int k, const cplx<typename ChunkT<P>::T> *v);
-template <>
-__device__ __forceinline__ void st_chunk<P64>(const SpinorPtr &f, long i, int k, const cplx<double> *v) {
-  ((double2 *)f.data)[k * f.stride + i] = make_double2(v[0].re, v[0].im);
-}
-template <>
-__device__ __forceinline__ void st_chunk<P32>(const SpinorPtr &f, long i, int k, const cplx<float> *v) {
-  ((float4 *)f.data)[k * f.stride + i] = make_float4(v[0].re, v[1].re, v[0].im, v[1].im);
-}
-// Stores the column y[0..LS) of chunk j (16-bit), slice s at base + s*step:
-// the site maxima of all slices first, combined across the 8-lane group by
-// independent shuffles (pipelined over s rather than one dependent round trip
-// per slice), then encode and store.  Every lane of the warp calls it.
-// Returns the sum of |stored values|^2 of this lane.
-template <int LS>
-__device__ __forceinline__ double st_column16(const SpinorPtr &f, long base, long step, int j,
-                                              const cplx<float> (&y)[LS][2], bool active) {
-  float m[LS];
-#pragma unroll
-  for (int s = 0; s < LS; s++)
-    m[s] = active ? fmaxf(fmaxf(fabsf(y[s][0].re), fabsf(y[s][0].im)), fmaxf(fabsf(y[s][1].re), fabsf(y[s][1].im)))
-                  : 0.f;
-#pragma unroll
-  for (int d = 1; d < 8; d <<= 1)
-#pragma unroll
-    for (int s = 0; s < LS; s++) m[s] = fmaxf(m[s], __shfl_xor_sync(0xffffffffu, m[s], d));
-  double acc = 0;
-  if (!active) return acc;
-#pragma unroll
-  for (int s = 0; s < LS; s++) {
-    const float scale = m[s] > 0.f ? 32767.0f / m[s] : 0.f;
-    const float nq = m[s] * (1.0f / 32767.0f);
-    const long i = base + (long)s * step;
-    const unsigned wx = enc16x2(y[s][0].re, y[s][1].re, scale), wy = enc16x2(y[s][0].im, y[s][1].im, scale);
-    ((uint2 *)((uint4 *)f.data + (long)(j >> 1) * f.stride + i))[j & 1] = make_uint2(wx, wy);
-    if (j == 0) f.norm[i] = nq;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const float a = dec16(wx, h) * nq, b = dec16(wy, h) * nq;
-      acc += (double)(a * a + b * b);
-    }
-  }
-  return acc;
+template <int NC, typename T>
+__device__ __forceinline__ cplx<T> &chunk_elem(Spinor<T> &s, int k, int q) {
+  return NC == 1 ? s.c[k / 3][k % 3] : s.c[2 * (k / 3) + q][k % 3];
 }
 
 // v[s] += f * w[s] on one chunk
@@ -189,135 +125,6 @@ __device__ __forceinline__ void m5_norm_epilogue(double acc, const Geom &g, Redu
   }
 }
 
-template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
-__global__ void __launch_bounds__(NT) m5_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
-                                                Reduce red, const int *skip) {
-  typedef typename ChunkT<P>::T T;
-  const int NCH = ChunkT<P>::NCH, NC = ChunkT<P>::NC;
-  __shared__ double sh[NT / 32];
-  const int rhs = blockIdx.y;
-  const long per = (long)g.n4cb * LS;
-  const long work = (long)g.n4cb * NCH;
-  double acc = 0;
-  const T sc = (T)cf.scale;
-  const bool sk = skip && skip[rhs];
-  for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
-    const int x = (int)(w % g.n4cb);
-    const int k = (int)(w / g.n4cb);
-    const long base = rhs * per + x;
-    cplx<T> v[LS][NC];
-#pragma unroll
-    for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    m5_column<LS, DAG, NC, T>(v, k < NCH / 2, cf);
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      cplx<T> o[NC];
-      if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
-#pragma unroll
-      for (int q = 0; q < NC; q++) {
-        if (XPAY) o[q] = o[q] + cscale(sc, v[s][q]);
-        else o[q] = cscale(sc, v[s][q]);
-        if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
-      }
-      st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
-    }
-  }
-  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
-}
-
-// 16-bit storage: four sites per warp, 8 lanes per site (chunks 0..5, lanes
-// 6 and 7 idle); the loop is warp-uniform so every shuffle has the full warp.
-template <int LS, int DAG, bool XPAY, bool NORM, int NT>
-__global__ void __launch_bounds__(NT) m5h_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
-                                                 Reduce red, const int *skip) {
-  __shared__ double sh[NT / 32];
-  const int rhs = blockIdx.y;
-  const long per = (long)g.n4cb * LS;
-  const int lane = threadIdx.x & 31, j = lane & 7;
-  const long nw = (long)gridDim.x * (NT / 32);
-  double acc = 0;
-  const float sc = (float)cf.scale;
-  const bool sk = skip && skip[rhs];
-  for (long x0 = ((long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5)) * 4; !sk && x0 < g.n4cb; x0 += nw * 4) {
-    const long x = x0 + (lane >> 3);
-    const bool active = j < 6 && x < g.n4cb;
-    const int jj = active ? j : 0;
-    const long base = rhs * per + (active ? x : 0);
-    cplx<float> v[LS][2];
-    // inactive lanes read a valid chunk of site 0 and store nothing
-    ld_column16<LS>(in, base, g.n4cb, jj, v);
-    m5_column<LS, DAG, 2, float>(v, jj < 3, cf);
-    if (XPAY) {
-      cplx<float> o[LS][2];
-      ld_column16<LS>(xv, base, g.n4cb, jj, o);
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < 2; q++) v[s][q] = o[s][q] + cscale(sc, v[s][q]);
-    } else {
-#pragma unroll
-      for (int s = 0; s < LS; s++)
-#pragma unroll
-        for (int q = 0; q < 2; q++) v[s][q] = cscale(sc, v[s][q]);
-    }
-    const double n = st_column16<LS>(out, base, g.n4cb, jj, v, active);
-    if (NORM) acc += n;
-  }
-  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
-}
-
-template <int P, int LS>
-static cudaError_t m5_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
-                                int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
-  const int NT = 128;
-  if constexpr (P == P16) {
-    dim3 grid(grid_blocks((long)g.n4cb * 8, NT), g.nrhs);
-#define M5H(D, XP, NR)                                                                              \
-    if (dag == D && !!xpay == XP && !!norm == NR) {                                                 \
-      m5h_kernel<LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
-      return launched();                                                                            \
-    }
-    M5H(0, false, false) M5H(0, true, false) M5H(0, true, true) M5H(0, false, true)
-    M5H(1, false, false) M5H(1, true, false) M5H(1, true, true) M5H(1, false, true)
-#undef M5H
-    return cudaErrorInvalidValue;
-  } else {
-  dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
-#define M5L(D, XP, NR)                                                                              \
-  if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
-    m5_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, cf, red, skip);             \
-    return launched();                                                                              \
-  }
-  M5L(0, false, false) M5L(0, true, false) M5L(0, true, true) M5L(0, false, true)
-  M5L(1, false, false) M5L(1, true, false) M5L(1, true, true) M5L(1, false, true)
-#undef M5L
-  return cudaErrorInvalidValue;
-  }
-}
-
-template <int P>
-static cudaError_t m5_launch_p(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
-                               int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
-  switch (g.ls) {
-    case 4: return m5_launch_ls<P, 4>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 8: return m5_launch_ls<P, 8>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 12: return m5_launch_ls<P, 12>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 16: return m5_launch_ls<P, 16>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 20: return m5_launch_ls<P, 20>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 24: return m5_launch_ls<P, 24>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    case 32: return m5_launch_ls<P, 32>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
-                      int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
-  if (prec == P64) return m5_launch_p<P64>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-  if (prec == P32) return m5_launch_p<P32>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-  if (prec == P16) return m5_launch_p<P16>(dag, g, out, in, x, cf, xpay, norm, red, skip, st);
-  return cudaErrorInvalidValue;
-}
-
 // ----------------------------------------------------------------- zMobius
 template <typename T> __device__ __forceinline__ cplx<T> ldz(const double2 *p) {
   const double2 v = __ldg(p);
@@ -395,125 +202,127 @@ __device__ __forceinline__ void m5z_column(cplx<T> (&v)[LS][NC], int h, const ZM
   }
 }
 
-template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT>
-__global__ void __launch_bounds__(NT) m5z_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv,
+// Sites per tile of the tiled kernels: one sweep thread per (site, chunk).
+template <int P, int NT> struct M5Tile { static const int TX = NT / ChunkT<P>::NCH; };
+
+// The tiled kernel: Z = false applies m5_column with the real coefficients cf,
+// Z = true m5z_column with the table tab.  out = [x +] sc * v (sc = cf.scale
+// for Z = false, 1 for Z = true).
+template <int P, int LS, int DAG, bool XPAY, bool NORM, int NT, bool Z>
+__global__ void __launch_bounds__(NT) m5t_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv, M5Coef cf,
                                                  const ZM5Tab *tab, Reduce red, const int *skip) {
   typedef typename ChunkT<P>::T T;
-  const int NCH = ChunkT<P>::NCH, NC = ChunkT<P>::NC;
+  constexpr int NCH = ChunkT<P>::NCH, NC = ChunkT<P>::NC, TX = M5Tile<P, NT>::TX;
+  extern __shared__ __align__(16) unsigned char m5sh[];
+  Spinor<T> *buf = (Spinor<T> *)m5sh;  // [TX * LS] entries of the tile
   __shared__ double sh[NT / 32];
   const int rhs = blockIdx.y;
   const long per = (long)g.n4cb * LS;
-  const long work = (long)g.n4cb * NCH;
+  const int ntiles = (g.n4cb + TX - 1) / TX;
+  const T sc = Z ? T(1) : (T)cf.scale;
   double acc = 0;
   const bool sk = skip && skip[rhs];
-  for (long w = (long)blockIdx.x * NT + threadIdx.x; !sk && w < work; w += (long)gridDim.x * NT) {
-    const int x = (int)(w % g.n4cb);
-    const int k = (int)(w / g.n4cb);
-    const long base = rhs * per + x;
-    cplx<T> v[LS][NC];
-#pragma unroll
-    for (int s = 0; s < LS; s++) ld_chunk<P>(in, base + (long)s * g.n4cb, k, v[s]);
-    m5z_column<LS, DAG, NC, T>(v, k < NCH / 2 ? 0 : 1, tab);
-#pragma unroll
-    for (int s = 0; s < LS; s++) {
-      cplx<T> o[NC];
-      if (XPAY) ld_chunk<P>(xv, base + (long)s * g.n4cb, k, o);
-#pragma unroll
-      for (int q = 0; q < NC; q++) {
-        o[q] = XPAY ? o[q] + v[s][q] : v[s][q];
-        if (NORM) acc += (double)o[q].re * o[q].re + (double)o[q].im * o[q].im;
-      }
-      st_chunk<P>(out, base + (long)s * g.n4cb, k, o);
-    }
-  }
-  if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
-}
-
-// 16-bit zMobius: the lane layout of m5h_kernel.
-template <int LS, int DAG, bool XPAY, bool NORM, int NT>
-__global__ void __launch_bounds__(NT) m5zh_kernel(Geom g, SpinorPtr out, SpinorPtr in, SpinorPtr xv,
-                                                  const ZM5Tab *tab, Reduce red, const int *skip) {
-  __shared__ double sh[NT / 32];
-  const int rhs = blockIdx.y;
-  const long per = (long)g.n4cb * LS;
-  const int lane = threadIdx.x & 31, j = lane & 7;
-  const long nw = (long)gridDim.x * (NT / 32);
-  double acc = 0;
-  const bool sk = skip && skip[rhs];
-  for (long x0 = ((long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5)) * 4; !sk && x0 < g.n4cb; x0 += nw * 4) {
-    const long x = x0 + (lane >> 3);
-    const bool active = j < 6 && x < g.n4cb;
-    const int jj = active ? j : 0;
-    const long base = rhs * per + (active ? x : 0);
-    cplx<float> v[LS][2];
-    // inactive lanes read a valid chunk of site 0 and store nothing
-    ld_column16<LS>(in, base, g.n4cb, jj, v);
-    m5z_column<LS, DAG, 2, float>(v, jj < 3 ? 0 : 1, tab);
-    if (XPAY) {
-      cplx<float> o[LS][2];
-      ld_column16<LS>(xv, base, g.n4cb, jj, o);
+  for (int tile = blockIdx.x; !sk && tile < ntiles; tile += gridDim.x) {
+    const int nx = min(TX, g.n4cb - tile * TX);
+    const long base = rhs * per + (long)tile * TX * LS;  // first entry of the tile
+    __syncthreads();  // the previous tile's store phase is done with buf
+    for (int t = threadIdx.x; t < nx * LS; t += NT) buf[t] = load_spinor<P>(in, base + t);
+    __syncthreads();
+    if (threadIdx.x < nx * NCH) {
+      const int xl = threadIdx.x / NCH, k = threadIdx.x - xl * NCH;
+      cplx<T> v[LS][NC];
 #pragma unroll
       for (int s = 0; s < LS; s++)
 #pragma unroll
-        for (int q = 0; q < 2; q++) v[s][q] = o[s][q] + v[s][q];
+        for (int q = 0; q < NC; q++) v[s][q] = chunk_elem<NC>(buf[xl * LS + s], k, q);
+      if (Z) m5z_column<LS, DAG, NC, T>(v, k < NCH / 2 ? 0 : 1, tab);
+      else m5_column<LS, DAG, NC, T>(v, k < NCH / 2, cf);
+#pragma unroll
+      for (int s = 0; s < LS; s++)
+#pragma unroll
+        for (int q = 0; q < NC; q++) chunk_elem<NC>(buf[xl * LS + s], k, q) = v[s][q];
     }
-    const double n = st_column16<LS>(out, base, g.n4cb, jj, v, active);
-    if (NORM) acc += n;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nx * LS; t += NT) {
+      Spinor<T> o = buf[t];
+      if (XPAY) {
+        const Spinor<T> xo = load_spinor<P>(xv, base + t);
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) o.c[a][c] = xo.c[a][c] + cscale(sc, o.c[a][c]);
+      } else if (!Z) {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) o.c[a][c] = cscale(sc, o.c[a][c]);
+      }
+      store_spinor<P>(out, base + t, o);
+      if (NORM) acc += norm2(rounded<P>(o));
+    }
   }
   if (NORM) m5_norm_epilogue<NT>(acc, g, red, skip, sh);
 }
 
-template <int P, int LS>
-static cudaError_t m5z_launch_ls(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
-                                 const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip,
-                                 cudaStream_t st) {
-  const int NT = 128;
-  if constexpr (P == P16) {
-    dim3 grid(grid_blocks((long)g.n4cb * 8, NT), g.nrhs);
-#define M5ZH(D, XP, NR)                                                                             \
-    if (dag == D && !!xpay == XP && !!norm == NR) {                                                 \
-      m5zh_kernel<LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, tab, red, skip);           \
-      return launched();                                                                            \
-    }
-    M5ZH(0, false, false) M5ZH(0, true, false) M5ZH(0, true, true)
-    M5ZH(1, false, false) M5ZH(1, true, false) M5ZH(1, true, true)
-#undef M5ZH
-    return cudaErrorInvalidValue;
-  } else {
-  dim3 grid(grid_blocks((long)g.n4cb * ChunkT<P>::NCH, NT), g.nrhs);
-#define M5ZL(D, XP, NR)                                                                             \
-  if (dag == D && !!xpay == XP && !!norm == NR) {                                                   \
-    m5z_kernel<P, LS, D, XP, NR, NT><<<grid, NT, 0, st>>>(g, out, in, x, tab, red, skip);           \
-    return launched();                                                                              \
+template <int P, int LS, bool Z>
+static cudaError_t m5t_launch(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                              const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  constexpr int NT = 128;
+  typedef typename ChunkT<P>::T T;
+  constexpr int TX = M5Tile<P, NT>::TX;
+  if (g.ncls != 1 || g.ls != LS) return cudaErrorInvalidValue;
+  const size_t shm = sizeof(Spinor<T>) * TX * LS;
+  const int ntiles = (g.n4cb + TX - 1) / TX;
+  dim3 grid(ntiles < 148 * 8 ? ntiles : 148 * 8, g.nrhs);
+#define CPSB_M5T(D, XP, NR)                                                                            \
+  if (dag == D && !!xpay == XP && !!norm == NR) {                                                      \
+    static bool attr = false;                                                                          \
+    if (!attr && shm > 48 * 1024) {                                                                    \
+      const cudaError_t e = cudaFuncSetAttribute((const void *)m5t_kernel<P, LS, D, XP, NR, NT, Z>,    \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm); \
+      if (e != cudaSuccess) return e;                                                                  \
+      attr = true;                                                                                     \
+    }                                                                                                  \
+    m5t_kernel<P, LS, D, XP, NR, NT, Z><<<grid, NT, shm, st>>>(g, out, in, x, cf, tab, red, skip);     \
+    return launched();                                                                                 \
   }
-  M5ZL(0, false, false) M5ZL(0, true, false) M5ZL(0, true, true)
-  M5ZL(1, false, false) M5ZL(1, true, false) M5ZL(1, true, true)
-#undef M5ZL
+  CPSB_M5T(0, false, false) CPSB_M5T(0, true, false) CPSB_M5T(0, true, true) CPSB_M5T(0, false, true)
+  CPSB_M5T(1, false, false) CPSB_M5T(1, true, false) CPSB_M5T(1, true, true) CPSB_M5T(1, false, true)
+#undef CPSB_M5T
   return cudaErrorInvalidValue;
-  }
 }
 
-template <int P>
-static cudaError_t m5z_launch_p(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
+template <int P, bool Z>
+static cudaError_t m5t_launch_p(int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
                                 const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip,
                                 cudaStream_t st) {
   switch (g.ls) {
-    case 4: return m5z_launch_ls<P, 4>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 8: return m5z_launch_ls<P, 8>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 12: return m5z_launch_ls<P, 12>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 16: return m5z_launch_ls<P, 16>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 20: return m5z_launch_ls<P, 20>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 24: return m5z_launch_ls<P, 24>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-    case 32: return m5z_launch_ls<P, 32>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+    case 4: return m5t_launch<P, 4, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 8: return m5t_launch<P, 8, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 12: return m5t_launch<P, 12, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 16: return m5t_launch<P, 16, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 20: return m5t_launch<P, 20, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 24: return m5t_launch<P, 24, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
+    case 32: return m5t_launch<P, 32, Z>(dag, g, out, in, x, cf, tab, xpay, norm, red, skip, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
+cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
+                      int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
+  if (prec == P64) return m5t_launch_p<P64, false>(dag, g, out, in, x, cf, nullptr, xpay, norm, red, skip, st);
+  if (prec == P32) return m5t_launch_p<P32, false>(dag, g, out, in, x, cf, nullptr, xpay, norm, red, skip, st);
+  if (prec == P16) return m5t_launch_p<P16, false>(dag, g, out, in, x, cf, nullptr, xpay, norm, red, skip, st);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_m5z(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x,
                        const ZM5Tab *tab, int xpay, int norm, Reduce red, const int *skip, cudaStream_t st) {
-  if (prec == P64) return m5z_launch_p<P64>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-  if (prec == P32) return m5z_launch_p<P32>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
-  if (prec == P16) return m5z_launch_p<P16>(dag, g, out, in, x, tab, xpay, norm, red, skip, st);
+  M5Coef none;
+  memset(&none, 0, sizeof(none));
+  if (prec == P64) return m5t_launch_p<P64, true>(dag, g, out, in, x, none, tab, xpay, norm, red, skip, st);
+  if (prec == P32) return m5t_launch_p<P32, true>(dag, g, out, in, x, none, tab, xpay, norm, red, skip, st);
+  if (prec == P16) return m5t_launch_p<P16, true>(dag, g, out, in, x, none, tab, xpay, norm, red, skip, st);
   return cudaErrorInvalidValue;
 }
 

@@ -64,6 +64,25 @@ size_t field_bytes(int prec, long nsites) {
   return (size_t)nsites * 48 + (size_t)nsites * 4;
 }
 
+Geom make_geom(const int dims[4], int ls, int nrhs, bool five_d) {
+  Geom g;
+  memset(&g, 0, sizeof(g));
+  g.lx = dims[0];
+  g.ly = dims[1];
+  g.lz = dims[2];
+  g.lt = dims[3];
+  g.lxh = g.lx / 2;
+  g.n4cb = g.lx * g.ly * g.lz * g.lt / 2;
+  g.ls = ls;
+  g.nrhs = nrhs;
+  g.nsites = (long)g.n4cb * ls * nrhs;
+  g.ncls = five_d ? 2 : 1;
+  g.cs[0] = five_d ? (ls + 1) / 2 : ls;
+  g.cs[1] = five_d ? ls / 2 : 0;
+  g.kb1 = g.n4cb * g.cs[0];
+  return g;
+}
+
 void Field::create(int pr, long n) {
   prec = pr;
   nsites = n;
@@ -319,15 +338,7 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   const int ls = p.action == CPSB_WILSON ? 1 : p.ls;
   if (ls < 1 || ls > 64) throw Error{CPSB_ERR_ARG, "ls out of range"};
   if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
-  geom.lx = G->dims[0];
-  geom.ly = G->dims[1];
-  geom.lz = G->dims[2];
-  geom.lt = G->dims[3];
-  geom.lxh = geom.lx / 2;
-  geom.n4cb = (int)G->n4cb;
-  geom.ls = ls;
-  geom.nrhs = nrhs;
-  geom.nsites = (long)geom.n4cb * ls * nrhs;
+  geom = make_geom(G->dims, ls, nrhs, p.action == CPSB_DWF);
   if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
   if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
   if (mobius_like()) {
@@ -653,7 +664,7 @@ void Operator::mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const 
 
 void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip,
                           CgState *S, const SpinorPtr &r, const Reduce *red_r, cudaStream_t st) {
-  if (!can_fuse_cg_r()) throw Error{CPSB_ERR_UNSUPPORTED, "fused residual update needs Wilson / DWF in FP32 / 16-bit"};
+  if (!can_fuse_cg_r()) throw Error{CPSB_ERR_UNSUPPORTED, "fused residual update needs the Wilson or DWF operator"};
   matpc(t2.ptr(), in, 0, red_d, skip, st);  // |MatPc p|^2 -> d
   hop(t1.ptr(), t2.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
   // the last hop of MatPcDag: out = t2 - kappa^2 D t1 = A p, consumed in registers

@@ -143,6 +143,7 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
   ServeRequest &r = *it.req;
   Gauge *G = &r.h->g;
   const long n = cb_sites(r.h, &r.p);
+  const Geom g1 = geom_of(r.h, &r.p, 1);
   const size_t each = (size_t)n * 24 * sizeof(double);
   if (r.multishift) {
     const int nshift = (int)r.shift.size();
@@ -150,7 +151,7 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
     Field chi(P64, n);
     DevBuf stage(each);
     CK(cudaMemcpyAsync(stage.p, r.b[0], each, cudaMemcpyHostToDevice, st));
-    CK(launch_pack(P64, chi.ptr(), (const double *)stage.p, n, st));
+    CK(launch_pack(P64, chi.ptr(), (const double *)stage.p, g1, st));
     std::vector<Field> xs(nvec);
     for (int i = 0; i < nvec; i++) {
       xs[i].create(P64, n);
@@ -162,7 +163,7 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
     const int rc = multishift(G, r.p, r.a, chi, xs, r.shift.data(), nshift, r.rsd, r.ms_type,
                               r.alpha.empty() ? nullptr : r.alpha.data(), r.res.data(), st, refiner.get());
     for (int i = 0; i < nvec; i++) {
-      CK(launch_unpack(P64, (double *)stage.p, xs[i].ptr(), n, st));
+      CK(launch_unpack(P64, (double *)stage.p, xs[i].ptr(), g1, st));
       CK(cudaMemcpyAsync(r.x[i], stage.p, each, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaStreamSynchronize(st));
@@ -173,13 +174,13 @@ void Server::run_item(const ServeItem &it, cudaStream_t st) {
   DevBuf stage(each);
   for (int q = 0; q < it.nrhs; q++) {
     CK(cudaMemcpyAsync(stage.p, r.x[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
-    CK(launch_pack(P64, s.x64.view((long)q * n), (const double *)stage.p, n, st));
+    CK(launch_pack(P64, s.x64.view((long)q * n), (const double *)stage.p, g1, st));
     CK(cudaMemcpyAsync(stage.p, r.b[it.rhs0 + q], each, cudaMemcpyHostToDevice, st));
-    CK(launch_pack(P64, s.b64.view((long)q * n), (const double *)stage.p, n, st));
+    CK(launch_pack(P64, s.b64.view((long)q * n), (const double *)stage.p, g1, st));
   }
   const int rc = s.solve(r.a, r.res.data() + it.rhs0, st);
   for (int q = 0; q < it.nrhs; q++) {
-    CK(launch_unpack(P64, (double *)stage.p, s.x64.view((long)q * n), n, st));
+    CK(launch_unpack(P64, (double *)stage.p, s.x64.view((long)q * n), g1, st));
     CK(cudaMemcpyAsync(r.x[it.rhs0 + q], stage.p, each, cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));

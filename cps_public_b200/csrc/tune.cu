@@ -94,6 +94,8 @@ int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_
     CK(cudaEventSynchronize(e1));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (getenv("CPSB_TUNE_VERBOSE"))
+      fprintf(stderr, "cpsb tune:   variant %d %.4f ms\n", v, ms / reps);
     if (ms < best_ms) {
       best_ms = ms;
       best = v;

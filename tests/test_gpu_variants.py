@@ -5,8 +5,10 @@ exercise only the winners; here each shape is pinned in a fresh process
 (CPSB_TUNE_FORCE) and Dslash / MatPcDagMatPc are compared with the oracle for
 Wilson, DWF and Mobius at FP64 (tolerance 1e-13), FP32 (2e-6 per hop) and
 16-bit storage (5e-4 per hop), on two non-cubic
-antiperiodic lattices: 4x6x4x8 (tiles of consecutive sites) and 8x8x4x6 (32
-sites per (z, t) plane, so the multi-plane tiles are used).
+antiperiodic lattices, 4x6x4x8 and 8x8x4x6 (columns of 1, 4 and 8 entries;
+tiles that end inside a lattice row).  A shape that does not fit an operator
+(link tables need columns of at least NT/32 entries) falls back to the tuned
+one.
 """
 import json
 import os
@@ -48,7 +50,7 @@ def _child():
     print(json.dumps(out))
 
 
-@pytest.mark.parametrize("variant", list(range(12)))
+@pytest.mark.parametrize("variant", list(range(6)))
 def test_launch_shape_matches_oracle(variant):
     env = dict(os.environ, CPSB_TUNE_FORCE=str(variant))
     p = subprocess.run([sys.executable, "-c", "import tests.test_gpu_variants as t; t._child()"], cwd=ROOT, env=env,
