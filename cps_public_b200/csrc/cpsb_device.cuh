@@ -14,9 +14,12 @@
 //             spins of a pair sit in the two lanes of a float2 (packed FP32x2 math)
 //      16-bit: 3 chunks of 8 fixed-point values (uint4), the same spin-paired
 //             order (32-bit word w = (3p+c)*2 + re/im holds spins 2p, 2p+1),
-//             plus one float per site (max-abs / 32767, the quantum) in a
+//             plus one float per site (max-abs / 16383, the quantum) in a
 //             separate norm array.  A value v is stored as the biased integer
-//             rint(v/quantum) + 32768 (15 bits of mantissa against IEEE fp16's 11).
+//             rint(v/quantum) + 16384, in [1, 32767] (14 bits of mantissa and a
+//             sign, against IEEE fp16's 11): two stored values add or subtract
+//             inside their 16-bit lane without overflow, so the hop kernel can
+//             spin-project on the packed integers before decoding.
 //  * gauge field, one 4-D checkerboard index x per parity p and direction mu:
 //      FP64 (18 reals): 9 double2 chunks, chunk k = U[k/3][k%3], at
 //                       data[((p*4+mu)*9 + k)*n4cb + x]
@@ -147,6 +150,20 @@ __device__ __forceinline__ unsigned q16(float v, float scale) {
 __device__ __forceinline__ unsigned enc16x2(float a, float b, float scale) {
   return q16(a, scale) | (q16(b, scale) << 16);
 }
+// Spinor storage: values in [-16383, 16383] with bias 16384.
+constexpr float S16_MAX = 16383.0f;
+__device__ __forceinline__ float dec16s(unsigned w, int hi) {
+  const unsigned bits = __byte_perm(w, 0x4B00u, hi ? 0x5432u : 0x5410u);
+  return __int_as_float((int)bits) - 8404992.0f;  // 2^23 + 16384
+}
+__device__ __forceinline__ unsigned q16s(float v, float scale) {
+  int q = __float2int_rn(v * scale);
+  q = max(-16383, min(16383, q));
+  return (unsigned)(q + 16384);
+}
+__device__ __forceinline__ unsigned enc16x2s(float a, float b, float scale) {
+  return q16s(a, scale) | (q16s(b, scale) << 16);
+}
 
 template <int P>
 __device__ __forceinline__ Spinor<typename PrecTraits<P>::real> load_spinor(const SpinorPtr &f, long i);
@@ -190,8 +207,8 @@ __device__ __forceinline__ Spinor<float> load_spinor<P16>(const SpinorPtr &f, lo
     for (int j = 0; j < 4; j += 2) {
       const int pc = (4 * k + j) / 2;  // = 3p + c
       const int p = pc / 3, c = pc % 3;
-      s.c[2 * p][c] = mk(dec16(w[j], 0) * nrm, dec16(w[j + 1], 0) * nrm);
-      s.c[2 * p + 1][c] = mk(dec16(w[j], 1) * nrm, dec16(w[j + 1], 1) * nrm);
+      s.c[2 * p][c] = mk(dec16s(w[j], 0) * nrm, dec16s(w[j + 1], 0) * nrm);
+      s.c[2 * p + 1][c] = mk(dec16s(w[j], 1) * nrm, dec16s(w[j + 1], 1) * nrm);
     }
   }
   return s;
@@ -224,8 +241,8 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf(s.c[a][c].re), fabsf(s.c[a][c].im)));
-  const float scale = m > 0.f ? 32767.0f / m : 0.f;
-  f.norm[i] = m * (1.0f / 32767.0f);
+  const float scale = m > 0.f ? S16_MAX / m : 0.f;
+  f.norm[i] = m * (1.0f / S16_MAX);
   uint4 *b = entry_ptr<3, uint4>(f.data, (unsigned)i);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -234,8 +251,8 @@ __device__ __forceinline__ void store_spinor<P16>(const SpinorPtr &f, long i, co
     for (int j = 0; j < 4; j += 2) {
       const int pc = (4 * k + j) / 2;
       const int p = pc / 3, c = pc % 3;
-      w[j] = enc16x2(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, scale);
-      w[j + 1] = enc16x2(s.c[2 * p][c].im, s.c[2 * p + 1][c].im, scale);
+      w[j] = enc16x2s(s.c[2 * p][c].re, s.c[2 * p + 1][c].re, scale);
+      w[j + 1] = enc16x2s(s.c[2 * p][c].im, s.c[2 * p + 1][c].im, scale);
     }
     b[8 * k] = make_uint4(w[0], w[1], w[2], w[3]);
   }
@@ -250,15 +267,15 @@ template <int P, typename T> __device__ __forceinline__ Spinor<T> rounded(const 
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf((float)s.c[a][c].re), fabsf((float)s.c[a][c].im)));
-  const float scale = m > 0.f ? 32767.0f / m : 0.f;
-  const float nq = m * (1.0f / 32767.0f);
+  const float scale = m > 0.f ? S16_MAX / m : 0.f;
+  const float nq = m * (1.0f / S16_MAX);
   Spinor<T> o;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const unsigned w = enc16x2((float)s.c[a][c].re, (float)s.c[a][c].im, scale);
-      o.c[a][c] = mk((T)(dec16(w, 0) * nq), (T)(dec16(w, 1) * nq));
+      const unsigned w = enc16x2s((float)s.c[a][c].re, (float)s.c[a][c].im, scale);
+      o.c[a][c] = mk((T)(dec16s(w, 0) * nq), (T)(dec16s(w, 1) * nq));
     }
   return o;
 }

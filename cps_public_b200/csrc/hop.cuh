@@ -68,27 +68,34 @@ struct SpX2 { float2 re[2][3], im[2][3]; };
 // A half spinor (spins h0, h1 in the lanes) per colour.
 struct HfX2 { float2 re[3], im[3]; };
 
-// Two biased 16-bit values of one word as a float2 of exact integers in
-// [-32767, 32767]: the integer is placed under the exponent byte 0x4B (the
-// float 2^23 + u) and 2^23 + 32768 is subtracted.
-__device__ __forceinline__ float2 dec16x2(unsigned w) {
+// Two biased 16-bit values of one word as a float2 of exact integers: the
+// integer is placed under the exponent byte 0x4B (the float 2^23 + u) and
+// 2^23 + bias is subtracted.  Stored spinor words carry bias 16384 (values in
+// [-16383, 16383]); sums and differences of two stored words carry 32768.
+template <int BIAS> __device__ __forceinline__ float2 dec16x2b(unsigned w) {
   return add2(f2(__int_as_float((int)__byte_perm(w, 0x4B00u, 0x5410u)),
                  __int_as_float((int)__byte_perm(w, 0x4B00u, 0x5432u))),
-              f2b(-8421376.0f));
+              f2b(-(8388608.0f + (float)BIAS)));
 }
-// dec16x2 with the two lanes exchanged (high half in .x).
-__device__ __forceinline__ float2 swp_dec16x2(unsigned w) {
-  return add2(f2(__int_as_float((int)__byte_perm(w, 0x4B00u, 0x5432u)),
-                 __int_as_float((int)__byte_perm(w, 0x4B00u, 0x5410u))),
-              f2b(-8421376.0f));
-}
+__device__ __forceinline__ float2 dec16x2(unsigned w) { return dec16x2b<16384>(w); }
 // Biased encodings of round(v.x*scale), round(v.y*scale) in one word: adding
-// 1.5*2^23 + 2^15 leaves the rounded, biased integer in the low mantissa bits
-// (|v|*scale <= 32767 by construction of scale).
+// 1.5*2^23 + 2^14 leaves the rounded, biased integer in the low mantissa bits
+// (|v|*scale <= 16383 by construction of scale).
 __device__ __forceinline__ unsigned enc16x2p(float2 v, float2 scale) {
-  const float2 r = fma2(v, scale, f2b(12615680.0f));
+  const float2 r = fma2(v, scale, f2b(12599296.0f));
   return __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x5410u);
 }
+
+// Lane-wise sums and differences of two packed words of biased 16-bit values
+// (each in [1, 32767]); every result lane is v_a +- v_b + 32768 in [2, 65534],
+// so no lane carries or borrows into the other.
+__device__ __forceinline__ unsigned pk_add(unsigned a, unsigned b) { return a + b; }
+__device__ __forceinline__ unsigned pk_sub(unsigned a, unsigned b) { return a + 0x80008000u - b; }
+// low lane a - b, high lane a + b (b ^ 0x7FFF = 32767 - b in the low lane)
+__device__ __forceinline__ unsigned pk_subadd(unsigned a, unsigned b) { return a + (b ^ 0x00007FFFu) + 1u; }
+// low lane a + b, high lane a - b
+__device__ __forceinline__ unsigned pk_addsub(unsigned a, unsigned b) { return a + (b ^ 0x7FFF0000u) + 0x10000u; }
+__device__ __forceinline__ unsigned pk_swap(unsigned b) { return __byte_perm(b, 0u, 0x1032u); }
 
 // ---------------------------------------------------------------- raw entries
 // An entry as loaded, before unpacking, so loads can be issued ahead of the
@@ -141,30 +148,6 @@ __device__ __forceinline__ SpX2 unpack(const Raw<P16> &r, float *nrm) {
     s.im[pa / 3][pa % 3] = dec16x2(r.c[k].y);
     s.re[pb / 3][pb % 3] = dec16x2(r.c[k].z);
     s.im[pb / 3][pb % 3] = dec16x2(r.c[k].w);
-  }
-  *nrm = r.nrm;
-  return s;
-}
-// The same with the lower pair (spins 2, 3) decoded into swapped lanes (spins
-// 3, 2), the order in which the x and y projections combine it with the upper
-// pair: swapping the byte-permute selectors makes the swap free.
-__device__ __forceinline__ SpX2 unpack_sw(const Raw<P16> &r, float *nrm) {
-  SpX2 s;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const int pa = 2 * k, pb = 2 * k + 1;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int pc = h ? pb : pa;
-      const unsigned wr = h ? r.c[k].z : r.c[k].x, wi = h ? r.c[k].w : r.c[k].y;
-      if (pc / 3 == 0) {
-        s.re[0][pc % 3] = dec16x2(wr);
-        s.im[0][pc % 3] = dec16x2(wi);
-      } else {
-        s.re[1][pc % 3] = swp_dec16x2(wr);
-        s.im[1][pc % 3] = swp_dec16x2(wi);
-      }
-    }
   }
   *nrm = r.nrm;
   return s;
@@ -234,8 +217,8 @@ template <> __device__ __forceinline__ double store_x2<P16>(const SpinorPtr &f, 
     for (int c = 0; c < 3; c++)
       m = fmaxf(fmaxf(m, fmaxf(fabsf(s.re[p][c].x), fabsf(s.re[p][c].y))),
                 fmaxf(fabsf(s.im[p][c].x), fabsf(s.im[p][c].y)));
-  const float scale = m > 0.f ? 32767.0f / m : 0.f;
-  const float q = m * (1.0f / 32767.0f);
+  const float scale = m > 0.f ? S16_MAX / m : 0.f;
+  const float q = m * (1.0f / S16_MAX);
   f.norm[i] = q;
   const float2 sc = f2b(scale);
   uint4 *b = (uint4 *)entry_ptr<3, uint4>(f.data, i);
@@ -261,9 +244,9 @@ template <> __device__ __forceinline__ double store_x2<P16>(const SpinorPtr &f, 
 // ---------------------------------------------------------------- packed hop pieces
 // (1 + sg*gamma_mu) psi -> half spinor (h0, h1) in the lanes; the gamma
 // matrices of project() in cpsb_device.cuh written per spin pair: re[1] is
-// (psi2, psi3) and swp(re[1]) is (psi3, psi2).  SW: the lower pair of s is
-// already in swapped order (unpack_sw), which the x and y projections use.
-template <int MU, bool SW = false> __device__ __forceinline__ HfX2 project_x2(const SpX2 &s, float sg) {
+// (psi2, psi3) and swp(re[1]) is (psi3, psi2).
+template <int MU> __device__ __forceinline__ HfX2 project_x2(const SpX2 &s, float sg) {
+  constexpr bool SW = false;
   HfX2 h;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -280,6 +263,40 @@ template <int MU, bool SW = false> __device__ __forceinline__ HfX2 project_x2(co
       h.re[c] = fma2(f2b(sg), s.re[1][c], s.re[0][c]);
       h.im[c] = fma2(f2b(sg), s.im[1][c], s.im[0][c]);
     }
+  }
+  return h;
+}
+
+// (1 + sg*gamma_mu) psi of a 16-bit neighbour (POS: sg = +1), projected on
+// the stored integers: each word of the half spinor is one (or, with a lane
+// swap or a lane-dependent sign, two or three) integer operations on two
+// stored words, and only the 6 projected words are decoded (bias 32768) --
+// against decoding all 12 words and 6 packed FMAs.  The combinations are those
+// of project_x2.
+template <int MU, bool POS> __device__ __forceinline__ HfX2 iproject(const Raw<P16> &r) {
+  const unsigned w[12] = {r.c[0].x, r.c[0].y, r.c[0].z, r.c[0].w, r.c[1].x, r.c[1].y,
+                          r.c[1].z, r.c[1].w, r.c[2].x, r.c[2].y, r.c[2].z, r.c[2].w};
+  HfX2 h;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    // upper pair (spins 0, 1) and lower pair (spins 2, 3), re and im words
+    const unsigned are = w[c * 2], aim = w[c * 2 + 1], bre = w[(3 + c) * 2], bim = w[(3 + c) * 2 + 1];
+    unsigned hre, him;
+    if (MU == 0) {         // re: (a0 - sg b3.im, a1 - sg b2.im); im: (a0 + sg b3.re, a1 + sg b2.re)
+      hre = POS ? pk_sub(are, pk_swap(bim)) : pk_add(are, pk_swap(bim));
+      him = POS ? pk_add(aim, pk_swap(bre)) : pk_sub(aim, pk_swap(bre));
+    } else if (MU == 1) {  // (a0 - sg b3, a1 + sg b2), re and im alike
+      hre = POS ? pk_subadd(are, pk_swap(bre)) : pk_addsub(are, pk_swap(bre));
+      him = POS ? pk_subadd(aim, pk_swap(bim)) : pk_addsub(aim, pk_swap(bim));
+    } else if (MU == 2) {  // re: (a0 - sg b2.im, a1 + sg b3.im); im: (a0 + sg b2.re, a1 - sg b3.re)
+      hre = POS ? pk_subadd(are, bim) : pk_addsub(are, bim);
+      him = POS ? pk_addsub(aim, bre) : pk_subadd(aim, bre);
+    } else {               // (a0 + sg b2, a1 + sg b3)
+      hre = POS ? pk_add(are, bre) : pk_sub(are, bre);
+      him = POS ? pk_add(aim, bim) : pk_sub(aim, bim);
+    }
+    h.re[c] = dec16x2b<32768>(hre);
+    h.im[c] = dec16x2b<32768>(him);
   }
   return h;
 }
@@ -470,7 +487,7 @@ __device__ __forceinline__ void load_unit(const DslashArgs &A, int tile, int k, 
 // every link read is a broadcast).  The grid holds no more blocks than are
 // resident at once, so the units in flight are one contiguous run of tiles and
 // their neighbour columns are read while they are in L2.
-template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, bool CGR, bool DAG>
+template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, bool CGR, bool DAG, int DEPTH>
 __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const Geom &g = A.g;
   extern __shared__ __align__(16) unsigned char dsh[];
@@ -526,11 +543,18 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         const double2 *l64 = (const double2 *)lk;
         Spinor<double> acc;
         zero(acc);
-        Raw<P64> nxt = load_raw<P64>(A.in, rb + (unsigned)nb[0]);
+        // DEPTH: neighbours whose loads are in flight ahead of the one computed
+        Raw<P64> nxt;
+        if (DEPTH >= 1) nxt = load_raw<P64>(A.in, rb + (unsigned)nb[0]);
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-          const Raw<P64> cur = nxt;
-          if (j < 7) nxt = load_raw<P64>(A.in, rb + (unsigned)nb[j + 1]);
+          Raw<P64> cur;
+          if (DEPTH >= 1) {
+            cur = nxt;
+            if (j < 7) nxt = load_raw<P64>(A.in, rb + (unsigned)nb[j + 1]);
+          } else {
+            cur = load_raw<P64>(A.in, rb + (unsigned)nb[j]);
+          }
           const int mu = j & 3;
           const double sg = j < 4 ? -(double)sdag : (double)sdag;
           const Half<double> h = project(unpack64(cur), mu, sg);
@@ -611,20 +635,25 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         const float4 *l32 = (const float4 *)lk;
         AccX2 acc;
         zero_x2(acc);
-        Raw<P> nxt = load_raw<P>(A.in, rb + (unsigned)nb[0]);
-        Raw<P> nx2 = load_raw<P>(A.in, rb + (unsigned)nb[1]);
+        // DEPTH (1 or 2): neighbours whose loads are in flight ahead of the one computed
+        Raw<P> nxt, nx2;
+        nxt = load_raw<P>(A.in, rb + (unsigned)nb[0]);
+        if (DEPTH >= 2) nx2 = load_raw<P>(A.in, rb + (unsigned)nb[1]);
 #pragma unroll
         for (int j = 0; j < 8; j++) {
           const Raw<P> cur = nxt;
-          nxt = nx2;
-          if (j < 6) nx2 = load_raw<P>(A.in, rb + (unsigned)nb[j + 2]);
-          // 16-bit x and y neighbours are decoded with the lower pair swapped
-          constexpr bool SWD = P == P16;
+          if (DEPTH >= 2) {
+            nxt = nx2;
+            if (j < 6) nx2 = load_raw<P>(A.in, rb + (unsigned)nb[j + 2]);
+          } else if (j < 7) {
+            nxt = load_raw<P>(A.in, rb + (unsigned)nb[j + 1]);
+          }
           float nrm;
-          SpX2 v;
-          if constexpr (SWD) v = (j & 3) < 2 ? unpack_sw(cur, &nrm) : unpack(cur, &nrm);
-          else v = unpack(cur, &nrm);
           const float sg = j < 4 ? -sdag : sdag;
+          // FP32: unpack, then project; 16-bit: project on the integers (iproject)
+          SpX2 v;
+          if constexpr (P == P32) v = unpack(cur, &nrm);
+          else nrm = cur.nrm;
           const float4 *lj = l32 + j * 9;
           Link<float> lr;
           if (!LC) {
@@ -633,7 +662,9 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           }
 #define CPSB_NB(MU)                                                                              \
   {                                                                                              \
-    const HfX2 h = project_x2<MU, SWD && (MU < 2)>(v, sg);                                       \
+    HfX2 h;                                                                                      \
+    if constexpr (P == P16) h = sg > 0.f ? iproject<MU, true>(cur) : iproject<MU, false>(cur);   \
+    else h = project_x2<MU>(v, sg);                                                              \
     const HfX2 uh = LC ? (j < 4 ? umul_x2<false>(lj, h) : umul_x2<true>(lj, h))                  \
                        : (j < 4 ? umul_x2r<false>(lr, h) : umul_x2r<true>(lr, h));               \
     accum_x2<MU>(acc, uh, sg, nrm);                                                              \
@@ -801,7 +832,7 @@ static int resident_blocks(const void *fn, int nt, size_t shm) {
 // table (LC), right-hand-side grouping (GRP: as many right-hand sides per warp
 // as divide it, else one).  The fused residual update (A.cg) needs the xpay
 // form.
-template <int P, int NT, int MINB, bool LC, bool GRP>
+template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH>
 static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
   const int C0 = A.g.cs[0];
   if (C0 < 1 || C0 > NT) return cudaErrorNotSupported;
@@ -827,12 +858,12 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
   cudaError_t e = cudaSuccess;
 #define CPSB_HOP(XP, NR, CG, D)                                                            \
   {                                                                                        \
-    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D>;             \
+    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH>;             \
     static bool done = false;                                                              \
     e = opt_in(fn, done);                                                                  \
     if (e != cudaSuccess) return e;                                                        \
     const long nb = std::min(units, (long)resident_blocks(fn, NT, L.total));                \
-    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D><<<(unsigned)nb, NT, L.total, st>>>(A);      \
+    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH><<<(unsigned)nb, NT, L.total, st>>>(A);      \
   }
 #define CPSB_HOP_D(XP, NR, CG)          \
   if (A.dag) CPSB_HOP(XP, NR, CG, true) \
@@ -853,12 +884,15 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
 template <int P>
 static cudaError_t hop_launch_p(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
   switch (variant) {
-    case 0: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, true>(A, xpay, norm, st);
-    case 1: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, false>(A, xpay, norm, st);
-    case 2: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, true>(A, xpay, norm, st);
-    case 3: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, false>(A, xpay, norm, st);
-    case 4: return hop_launch_v<P, 128, P == P64 ? 2 : 4, false, true>(A, xpay, norm, st);
-    case 5: return hop_launch_v<P, 128, P == P64 ? 2 : 4, false, false>(A, xpay, norm, st);
+    // FP64: (2, 3, 1) / (4, 6) blocks per SM; FP32 and 16-bit: (4, 5, 2) / (5, 6)
+    case 0: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st);
+    case 1: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
+    case 2: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
+    case 3: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
+    case 4: return hop_launch_v<P, 128, P == P64 ? 2 : 4, false, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
+    case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
+    case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
+    case 7: return hop_launch_v<P, 256, P == P64 ? 2 : 3, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
     default: return cudaErrorNotSupported;
   }
 }
