@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other BASELINE workloads (Wilson 8^4, Mobius x12, multishift, serving)")
     return ap.parse_args()
 
 
@@ -311,12 +313,95 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(u, srcs[0], out["f64"]["iters"])
+    if world == 1 and not args.no_configs:
+        # The other workloads of the reference's benchmark set, each with its own
+        # small, stated number of timed runs (not --steps); the headline's
+        # workspaces are released first.
+        g.free()
+        del pool, b_dev, x_dev
+        torch.cuda.empty_cache()
+        line["configs"] = run_configs(args.no_cpu_baseline)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(line, default=_plain))
+
+
+def config0_wilson(with_cpu=True):
+    """Plain Wilson even-odd CG, FP64, 8^4 periodic, mass 0.1, stop 1e-10 (links
+    eps 0.3, Gaussian odd-checkerboard source): 3 warm-up and 20 timed solves
+    through the device-pointer entry point; the compiled reference's own solve of
+    the same system on one host core beside it."""
+    import ctypes as C
+
+    import torch
+    import cps_public_b200 as cb
+    from cps_public_b200 import _lib, fields
+    dims = (8, 8, 8, 8)
+    u = fields.random_gauge(dims, 0.3, 2020)
+    src = fields.random_source(int(np.prod(dims)) // 2, 2021)
+    g = cb.Gauge(u, dims)
+    op = cb.DiracOp(g, "wilson", mass=0.1)
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    b = torch.from_numpy(src).to(dev)
+    x = torch.zeros_like(b)
+    res = cb.SolveResult()
+    st = torch.cuda.current_stream(dev)
+    lat = []
+    for k in range(23):
+        x.zero_()
+        a = cb.CgArg(STOP, 5000, cb.F64, 0.0, 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc = lib.cpsb_invcg_dev(g.h, C.byref(op.p), C.byref(a), C.c_void_p(x.data_ptr()), C.c_void_p(b.data_ptr()),
+                                C.byref(res), C.c_void_p(st.cuda_stream))
+        e1.record(st)
+        torch.cuda.synchronize()
+        assert rc == 0 and res.true_rsd <= STOP
+        if k >= 3:
+            lat.append(e0.elapsed_time(e1))
+    g.free()
+    out = {"workload": "wilson_eo_cg_fp64_8x8x8x8", "mass": 0.1, "stop_true_rsd": STOP, "timed_solves": len(lat),
+           "solves_per_s": 1000.0 * len(lat) / sum(lat), "p50_ms": float(np.percentile(lat, 50)),
+           "p99_ms": float(np.percentile(lat, 99)), "iters": res.iters, "true_rsd": res.true_rsd}
+    if with_cpu:
+        from oracle import refrun
+        if refrun.available():
+            t0 = time.perf_counter()
+            it, rp, _ = refrun.run(refrun.OP_INVCG, "wilson", dims, u, [src, np.zeros_like(src)], mass=0.1,
+                                   stop_rsd=STOP, max_iter=5000, threads=1)
+            out["cpu_reference"] = {"seconds_per_solve": float(rp[10]), "solves_per_s": 1.0 / float(rp[10]),
+                                    "iters": it, "cores": 1,
+                                    "sample": "one CPS noarch InvCg solve (compiled reference), its own timing"}
+    return out
+
+
+def run_configs(no_cpu=False):
+    """BASELINE's other configurations, each with a stated small sample."""
+    from cps_public_b200 import config_bench, serve_bench
+    cfg = {}
+    t0 = time.perf_counter()
+    cfg["config0"] = config0_wilson(with_cpu=not no_cpu)
+    cfg["config2"] = dict(config_bench.mobius12_run(STOP, arms=("f16", "f64"), e2e=False),
+                          sample="one timed 12-RHS 16-bit mixed solve and one FP64 solve, each after a 40-iteration "
+                                 "warm-up")
+    cfg["config3"] = dict(config_bench.multishift_run(STOP, e2e=False),
+                          sample="one timed multishift solve per arm after a 30-iteration warm-up")
+    gauges = serve_bench.make_gauges()
+    sat = serve_bench.run(requests=12, rate=20.0, slots=4, precision="f32", seed=4, gauges=gauges)
+    alone = serve_bench.run(requests=4, rate=20.0, slots=4, precision="f32", seed=5, gauges=gauges,
+                            one_at_a_time=True)
+    for d in (sat, alone):
+        d.pop("per_request", None)
+    cfg["config4"] = {"poisson_20_per_s": sat, "one_at_a_time": alone,
+                      "sample": "12 Poisson arrivals at 20/s (saturated: one GPU serves ~0.3 requests/s of this mix) "
+                                "and 4 requests submitted one at a time (latency = service time, no queueing)"}
+    del gauges
+    cfg["seconds"] = time.perf_counter() - t0
+    return cfg
 
 
 def _ref_mdagm_seconds(u, src, nproc, threads_per_proc=1):
@@ -339,7 +424,7 @@ def _ref_mdagm_seconds(u, src, nproc, threads_per_proc=1):
     ts = [r[0] for r in res]
     starts, ends = [r[1] for r in res], [r[2] for r in res]
     overlap = {"union_s": max(ends) - min(starts), "common_s": max(0.0, min(ends) - max(starts)),
-               "all_overlap": min(ends) > max(starts)}
+               "all_overlap": bool(min(ends) > max(starts))}
     return ts, overlap
 
 
@@ -424,7 +509,16 @@ def run_reference(args):
                                        f"solves the {NRHS} right-hand sides one after another, so the "
                                        f"per-right-hand-side rate is the solve rate{conc}"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(line, default=_plain))
+
+
+def _plain(o):
+    """JSON form of numpy scalars and arrays in a result line."""
+    if isinstance(o, np.generic):
+        return o.item()
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(f"not JSON serializable: {type(o).__name__}")
 
 
 def main():

@@ -18,7 +18,8 @@ Each prints one JSON line: solves/s (right-hand sides or shift systems per
 second) with sources and solutions resident in device memory (the *_dev entry
 points; torch provides the device buffers), the same through the host-pointer
 entry points ("e2e", host copies included), iteration counts and the worst
-FP64 true residual.
+FP64 true residual.  bench.py calls mobius12_run / multishift_run with
+arms=... and e2e=False to add these workloads to its line.
 """
 from __future__ import annotations
 
@@ -36,6 +37,13 @@ DIMS = (24, 24, 24, 64)
 
 
 def mobius12(a):
+    print(json.dumps(mobius12_run(a.stop)))
+
+
+def mobius12_run(stop=1e-10, arms=("f16", "f32", "f64"), e2e=True):
+    """Runs the Mobius 12-point-source workload; arms: inner precisions of the
+    12-RHS mixed solves ("f16", "f32") and "f64" (the plain FP64 CG on one
+    source).  Returns the result dict."""
     init(0)
     u = fields.random_gauge(DIMS, 0.15, 2401)
     rng = np.random.default_rng(2402)
@@ -61,7 +69,7 @@ def mobius12(a):
         def solve_dev(maxit):
             x_d.zero_()
             torch.cuda.synchronize()
-            arg = CgArg(a.stop, maxit, prec, 0.1, 0)
+            arg = CgArg(stop, maxit, prec, 0.1, 0)
             t0 = time.perf_counter()
             rc = lib.cpsb_invcg_multi_dev(g.h, C.byref(op.p), C.byref(arg), nrhs, C.c_void_p(x_d.data_ptr()),
                                           C.c_void_p(b_d.data_ptr()), res, None)
@@ -75,45 +83,55 @@ def mobius12(a):
         g.free()
         return dt, rr, x0
 
-    t_f16, r_f16, _ = arm(nr, F16)
-    t_mixed, r_mixed, x_mixed0 = arm(nr, F32)
-    t_f64, r_f64, x64 = arm(1, F64)
-    agree = float(np.linalg.norm(x_mixed0 - x64) / np.linalg.norm(x64))
+    def mixed_rec(t, rr):
+        return {"solves_per_s": nr / t, "seconds": t, "iters": max(r["iters"] for r in rr),
+                "max_true_rsd": max(r["true_rsd"] for r in rr),
+                "reliable_updates": max(r["reliable_updates"] for r in rr)}
+
+    out = {"workload": "mobius_multi_rhs_24x24x24x64_ls16", "rhs": nr, "site": site, "stop_true_rsd": stop}
+    x_mixed0 = {}
+    if "f64" in arms:
+        t_f64, r_f64, x64 = arm(1, F64)
+        out["f64_x1"] = {"solves_per_s": 1.0 / t_f64, "seconds": t_f64, "iters": r_f64[0]["iters"],
+                         "true_rsd": r_f64[0]["true_rsd"]}
+    for name, prec in (("f16", F16), ("f32", F32)):
+        if name not in arms:
+            continue
+        t, rr, x0 = arm(nr, prec)
+        x_mixed0[name] = x0
+        out[f"mixed_{name}_x12"] = mixed_rec(t, rr)
+        if "f64" in arms:
+            out[f"mixed_{name}_vs_fp64"] = (nr / t) * t_f64
+            out[f"rhs0_mixed_{name}_vs_fp64_rel_diff"] = float(np.linalg.norm(x0 - x64) / np.linalg.norm(x64))
     del b_d, x_d
     torch.cuda.empty_cache()
-    g = Gauge(u, DIMS)
-    op = DiracOp(g, "mobius", mass=0.005, ls=16, m5=1.8, b=1.5, c=0.5)
-    t0 = time.perf_counter()
-    xs, rs = op.InvCgMulti(srcs, stop_rsd=a.stop, max_num_iter=100000, precision=F16)
-    t_e2e = time.perf_counter() - t0
-    out = {"workload": "mobius_multi_rhs_24x24x24x64_ls16", "rhs": nr, "site": site,
-           "mixed_f16_x12": {"solves_per_s": nr / t_f16, "seconds": t_f16,
-                             "iters": max(r["iters"] for r in r_f16),
-                             "max_true_rsd": max(r["true_rsd"] for r in r_f16),
-                             "reliable_updates": max(r["reliable_updates"] for r in r_f16)},
-           "mixed_f16_vs_fp64": (nr / t_f16) * t_f64,
-           "mixed_f32_x12": {"solves_per_s": nr / t_mixed, "seconds": t_mixed,
-                             "iters": max(r["iters"] for r in r_mixed),
-                             "max_true_rsd": max(r["true_rsd"] for r in r_mixed),
-                             "reliable_updates": max(r["reliable_updates"] for r in r_mixed)},
-           "f64_x1": {"solves_per_s": 1.0 / t_f64, "seconds": t_f64, "iters": r_f64[0]["iters"],
-                      "true_rsd": r_f64[0]["true_rsd"]},
-           "mixed_vs_fp64": (nr / t_mixed) * t_f64,
-           "rhs0_mixed_vs_fp64_rel_diff": agree,
-           "e2e_mixed_f16_x12": {"solves_per_s": nr / t_e2e, "seconds": t_e2e,
-                                 "max_true_rsd": max(r.true_rsd for r in rs),
-                                 "path": "cpsb_invcg_multi (host vectors, copies included)"}}
-    print(json.dumps(out))
+    if e2e:
+        g = Gauge(u, DIMS)
+        op = DiracOp(g, "mobius", mass=0.005, ls=16, m5=1.8, b=1.5, c=0.5)
+        t0 = time.perf_counter()
+        xs, rs = op.InvCgMulti(srcs, stop_rsd=stop, max_num_iter=100000, precision=F16)
+        t_e2e = time.perf_counter() - t0
+        out["e2e_mixed_f16_x12"] = {"solves_per_s": nr / t_e2e, "seconds": t_e2e,
+                                    "max_true_rsd": max(r.true_rsd for r in rs),
+                                    "path": "cpsb_invcg_multi (host vectors, copies included)"}
+        g.free()
+    return out
 
 
 def multishift(a):
+    print(json.dumps(multishift_run(a.stop)))
+
+
+def multishift_run(stop=1e-10, e2e=True):
+    """Runs the 12-shift multishift workload, FP32 Krylov + refinement and FP64;
+    returns the result dict."""
     init(0)
     u = fields.random_gauge(DIMS, 0.15, 2403)
     g = Gauge(u, DIMS)
     op = DiracOp(g, "dwf", mass=0.01, ls=12, m5=1.8)
     src = fields.random_source(op.n // 24, 2404)
     shifts = list(np.logspace(-4, 1, 12))
-    rsd = [a.stop] * 12
+    rsd = [stop] * 12
     import torch
     dev = torch.device("cuda", 0)
     lib = _lib.load()
@@ -126,7 +144,7 @@ def multishift(a):
 
     def minv_dev(prec, maxit):
         rs_ = np.array(rsd, np.float64)
-        arg = CgArg(a.stop, maxit, prec, 0.1, 0)
+        arg = CgArg(stop, maxit, prec, 0.1, 0)
         r = SolveResult()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -150,14 +168,16 @@ def multishift(a):
                      "max_reported_rsd": float(np.max(rs_)), "checked_true_rsd": worst}
     del b_d, x_d
     torch.cuda.empty_cache()
-    t0 = time.perf_counter()
-    op.MInvCG(src, shifts, rsd, ms_type=MULTI, max_num_iter=100000, precision=F32)
-    t_e2e = time.perf_counter() - t0
     out = {"workload": "dwf_multishift_24x24x24x64_ls12", "shifts": shifts, **res,
-           "mixed_vs_fp64": res["f64"]["seconds"] / res["f32_krylov_refined"]["seconds"],
-           "e2e_f32_krylov_refined": {"seconds": t_e2e, "shift_systems_per_s": ns / t_e2e,
-                                      "path": "cpsb_minvcg (host vectors, copies included)"}}
-    print(json.dumps(out))
+           "mixed_vs_fp64": res["f64"]["seconds"] / res["f32_krylov_refined"]["seconds"]}
+    if e2e:
+        t0 = time.perf_counter()
+        op.MInvCG(src, shifts, rsd, ms_type=MULTI, max_num_iter=100000, precision=F32)
+        t_e2e = time.perf_counter() - t0
+        out["e2e_f32_krylov_refined"] = {"seconds": t_e2e, "shift_systems_per_s": ns / t_e2e,
+                                         "path": "cpsb_minvcg (host vectors, copies included)"}
+    g.free()
+    return out
 
 
 def main():

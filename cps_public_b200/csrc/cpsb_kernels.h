@@ -29,6 +29,8 @@ struct DslashArgs {
   Reduce red;             // |out|^2 per RHS when requested
   const int *skip;        // per-RHS: nonzero skips that RHS (device memory), may be null
   int rg;                 // right-hand sides per warp lane group (set by the launcher)
+  int rgroup;             // right-hand sides per work unit (set by the launcher)
+  int torder;             // 1: tiles visited t-fastest where they are whole rows (set by the launcher)
   // Fused CG residual update: when cg is set, out = x + a D in is not stored; instead r -= alpha (out +
   // shift p) with alpha from cg, |r|^2 per RHS is reduced, and the last block
   // advances the recurrence scalars as the r-update kernel of blas.cu does.

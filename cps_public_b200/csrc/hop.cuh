@@ -477,6 +477,20 @@ __device__ __forceinline__ void load_unit(const DslashArgs &A, int tile, int k, 
   }
 }
 
+// The tile processed as the u-th unit.  A tile is TX consecutive checkerboard
+// sites; when it is a whole number of x-rows of one (z, t) plane, tiles are
+// visited with t fastest, then z, then the block of rows, so a tile's t and z
+// neighbours are processed by blocks resident at the same time (their shared
+// input columns are read while in L2); otherwise in site order.
+__device__ __forceinline__ int tile_order(const Geom &g, int u, int TX, int torder) {
+  const int plane = g.lxh * g.ly;
+  if (!torder || TX % g.lxh != 0 || plane % TX != 0) return u;
+  const int nyb = plane / TX;
+  const int t = u % g.lt, r = u / g.lt;
+  const int z = r % g.lz, yb = r / g.lz;
+  return yb + nyb * (z + g.lz * t);
+}
+
 // LC: links from the unit's shared-memory table (otherwise each entry loads
 // and reconstructs its own, which suits columns of one or two entries).
 //
@@ -504,12 +518,16 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const int xl = threadIdx.x / (C0 * RG);          // column of the tile
   const int ntiles = (g.n4cb + TX - 1) / TX;
   const int ncls = g.ncls;
-  const int nunits = ntiles * ncls;
+  // units: (group of A.rgroup right-hand sides, tile, class), the group slowest
+  const int G = A.rgroup;
+  const int per_group = ntiles * ncls;
+  const int nunits = per_group * ((g.nrhs + G - 1) / G);
   const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
   constexpr float sdag = DAG ? -1.f : 1.f;
   const int *nbo_sh = (const int *)(dsh + L.nbo);
   for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
-    const int tile = unit / ncls, k = unit - tile * ncls;
+    const int grp = unit / per_group, rem = unit - grp * per_group;
+    const int k = rem % ncls, tile = tile_order(g, rem / ncls, TX, A.torder);
     const int par_out = A.five_d ? ((1 - A.cb + k) & 1) : 1 - A.cb;
     __syncthreads();  // the previous unit is done with the tables
     load_unit<P, LC>(A, tile, k, par_out, TX, NT, dsh);
@@ -534,7 +552,8 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
     const unsigned e5m = site_entry(g, sm, x), e5p = site_entry(g, sq, x);
     const double f5m = s == 0 ? A.hop5_wall : A.hop5_fact, f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
     const void *lk = dsh + L.links + (size_t)xl * LSTR * 16;
-    for (int rhs = rl; rhs < g.nrhs; rhs += RG) {
+    const int rhs_end = min(g.nrhs, (grp + 1) * G);
+    for (int rhs = grp * G + rl; rhs < rhs_end; rhs += RG) {
       if (A.skip && A.skip[rhs]) continue;
       const unsigned rb = (unsigned)rhs * per;
       const unsigned i = rb + own;
@@ -833,7 +852,7 @@ static int resident_blocks(const void *fn, int nt, size_t shm) {
 // as divide it, else one).  The fused residual update (A.cg) needs the xpay
 // form.
 template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH>
-static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st) {
+static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st, int rgroup, int torder) {
   const int C0 = A.g.cs[0];
   if (C0 < 1 || C0 > NT) return cudaErrorNotSupported;
   int rg = 1;
@@ -841,13 +860,18 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
     while (rg * 2 <= A.g.nrhs && C0 * rg * 2 <= 32 && 32 % (C0 * rg * 2) == 0) rg *= 2;
   if (GRP && rg == 1) return cudaErrorNotSupported;  // the same as the ungrouped shape
   A.rg = rg;
+  A.torder = torder;
+  // right-hand sides per unit: all, or groups of rgroup (a multiple of rg), so
+  // that the blocks resident at one time touch only a few right-hand sides
+  A.rgroup = rgroup > 0 ? std::max(rg, rgroup / rg * rg) : A.g.nrhs;
+  if (rgroup > 0 && A.rgroup >= A.g.nrhs) return cudaErrorNotSupported;  // the same as all
   const int TX = NT / (C0 * rg);
   if (TX < 1 || (LC && TX > 32)) return cudaErrorNotSupported;  // link tables of more than 32 columns: use !LC
   const bool cgr = A.cg != nullptr;
   if (cgr && !xpay) return cudaErrorInvalidValue;
   const HopShm L = hop_shm(TX, NT, A.g.nrhs, norm || cgr, LC);
   if (L.total > 200 * 1024) return cudaErrorNotSupported;
-  const long units = (long)((A.g.n4cb + TX - 1) / TX) * A.g.ncls;
+  const long units = (long)((A.g.n4cb + TX - 1) / TX) * A.g.ncls * ((A.g.nrhs + A.rgroup - 1) / A.rgroup);
   // the opt-in above the 48 KB default is set once per instantiation
   auto opt_in = [&](const void *f, bool &done) -> cudaError_t {
     if (done || L.total + 1024 <= 48 * 1024) return cudaSuccess;
@@ -884,15 +908,17 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
 template <int P>
 static cudaError_t hop_launch_p(const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st) {
   switch (variant) {
-    // FP64: (2, 3, 1) / (4, 6) blocks per SM; FP32 and 16-bit: (4, 5, 2) / (5, 6)
-    case 0: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st);
-    case 1: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
-    case 2: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
-    case 3: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
-    case 4: return hop_launch_v<P, 128, P == P64 ? 2 : 4, false, false, P == P64 ? 1 : 2>(A, xpay, norm, st);
-    case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
-    case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
-    case 7: return hop_launch_v<P, 256, P == P64 ? 2 : 3, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st);
+    // (threads, blocks per SM, link table, RHS per warp lane group, prefetch
+    // depth; RHS per unit, t-fastest tile order).  FP64 keeps fewer blocks
+    // (more registers) and one neighbour less in flight.
+    case 0: return hop_launch_v<P, 128, P == P64 ? 2 : 4, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st, 0, 0);
+    case 1: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st, 0, 0);
+    case 2: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st, 0, 0);
+    case 3: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, false, P == P64 ? 1 : 2>(A, xpay, norm, st, 0, 1);
+    case 4: return hop_launch_v<P, 128, P == P64 ? 2 : 4, false, false, P == P64 ? 1 : 2>(A, xpay, norm, st, 0, 0);
+    case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
+    case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
+    case 7: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st, 4, 0);
     default: return cudaErrorNotSupported;
   }
 }

@@ -43,11 +43,27 @@ def main():
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--hbm-fraction", type=float, default=0.85)
     a = ap.parse_args()
+    print(json.dumps(run(a.requests, a.rate, a.slots, a.precision, a.seed, a.hbm_fraction)))
+
+
+def make_gauges():
+    """The 8 resident seeded gauge fields (8^4, 16^3x32, 24^3x64 in turn)."""
     init(0)
     gauges = []
     for i in range(8):
         dims, eps = LATTICES[i % 3]
         gauges.append(Gauge(fields.random_gauge(dims, eps, 5000 + i), dims))
+    return gauges
+
+
+def run(requests=16, rate=20.0, slots=4, precision="f32", seed=4, hbm_fraction=0.85, gauges=None,
+        one_at_a_time=False):
+    """Serves `requests` Poisson arrivals at `rate` per second and returns the
+    result dict.  one_at_a_time: each request is submitted only after the
+    previous one has completed (latency = service time, no queueing)."""
+    gauges = gauges if gauges is not None else make_gauges()
+    a = argparse.Namespace(requests=requests, rate=rate, slots=slots, precision=precision, seed=seed,
+                           hbm_fraction=hbm_fraction)
     reqs = make_requests(a.requests, a.rate, a.seed)
     # Right-hand sides: per (gauge, Ls) one Gaussian base vector 11 sites longer
     # than a solve's vector; right-hand side i is the window starting at site i
@@ -62,16 +78,19 @@ def main():
         srcs.append([bases[key][24 * i:24 * i + op.n] for i in range(r["nrhs"])])
     srv = Server(slots=a.slots, hbm_fraction=a.hbm_fraction)
     t0 = time.perf_counter()
-    ids = []
+    ids, done = [], {}
     for r, op, s in zip(reqs, ops, srcs):
         dt = r["arrival"] - (time.perf_counter() - t0)
-        if dt > 0:
+        if dt > 0 and not one_at_a_time:
             time.sleep(dt)
-        ids.append(srv.submit(op, s, stop_rsd=r["tol"], precision=PRECS[a.precision]))
+        rid = srv.submit(op, s, stop_rsd=r["tol"], precision=PRECS[a.precision])
+        ids.append(rid)
+        if one_at_a_time:
+            done[rid] = srv.wait(rid)
     per = []
     worst = 0.0
     for r, op, s, rid in zip(reqs, ops, srcs, ids):
-        xs, res, lat = srv.wait(rid)
+        xs, res, lat = done[rid] if rid in done else srv.wait(rid)
         del xs
         tr = max(float(q.true_rsd) / r["tol"] for q in res)
         worst = max(worst, tr)
@@ -81,13 +100,15 @@ def main():
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    out = {"metric": "dwf_serving", "requests": a.requests, "offered_rate_per_s": a.rate, "slots": a.slots,
+    out = {"metric": "dwf_serving", "requests": a.requests,
+           "offered_rate_per_s": None if one_at_a_time else a.rate, "one_at_a_time": one_at_a_time,
+           "slots": a.slots,
            "precision": a.precision, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
            "requests_per_s": st["requests_per_s"], "rhs_solves_per_s": st["rhs_per_s"],
            "completed": st["completed"], "failed": st["failed"], "peak_running": st["peak_running"],
            "hbm_budget_gb": st["budget_bytes"] / 1e9, "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
            "wall_s": wall, "max_true_rsd_over_tol": worst, "per_request": per}
-    print(json.dumps(out))
+    return out
 
 
 if __name__ == "__main__":

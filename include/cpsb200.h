@@ -263,9 +263,11 @@ int cpsb_mdagm_ex(cpsb_gauge h, const cpsb_dirac_params *p, int precision, doubl
 int cpsb_kernel_launches(unsigned long long *count);
 
 /* Times `reps` applications of the device Dslash of the given precision on
- * internally resident data (one checkerboard, dag 0); reports the mean kernel
- * time in ms measured with CUDA events on the launching stream, and the bytes
- * each application must move (spinors in + out + links).  No counterpart in the
+ * internally resident data (one checkerboard, dag 0, nrhs right-hand sides of
+ * seeded random spinors; consecutive applications cycle through enough field
+ * pairs to touch more than twice the L2); reports the mean kernel time in ms
+ * measured with CUDA events on the launching stream, and the bytes each
+ * application must move (spinors in + out + links).  No counterpart in the
  * reference. */
 int cpsb_bench_dslash(cpsb_gauge h, const cpsb_dirac_params *p, int precision, int nrhs, int reps, double *ms,
                       double *bytes);
