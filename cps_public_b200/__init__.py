@@ -238,6 +238,28 @@ class DiracOp:
         r.rc = rc
         return xs, r, rs
 
+    def MInvCGMulti(self, srcs, shifts, rsd, ms_type=MULTI, alpha=None, max_num_iter=5000, precision=F64):
+        """Batched MInvCG over the source vectors srcs (the pseudofermions of one
+        RHMC evaluation), sharing the shifts; rsd: per shift, or per vector and
+        shift (nvec x nshift).  Returns (xs[q][s], results[q], rsd[q][s])."""
+        nvec, ns = len(srcs), len(shifts)
+        nsol = 1 if ms_type == SINGLE else ns
+        xs = [[np.zeros(self.n) for _ in range(nsol)] for _ in range(nvec)]
+        xp = (_lib._dp * (nvec * nsol))(*[ptr(x) for row in xs for x in row])
+        bs = [self._v(b) for b in srcs]
+        bp = (_lib._dp * nvec)(*[ptr(b) for b in bs])
+        rs = np.array(np.broadcast_to(np.asarray(rsd, np.float64), (nvec, ns)))
+        sh = np.array(shifts, np.float64)
+        al = np.ones(ns) if alpha is None else np.array(alpha, np.float64)
+        a = CgArg(float(np.min(rs)), max_num_iter, precision, 0.1, 0)
+        res = (SolveResult * nvec)()
+        rc = check(_lib.load().cpsb_minvcg_multi(self.gauge.h, C.byref(self.p), C.byref(a), nvec, xp, bp, ptr(sh), ns,
+                                                 ptr(rs), ms_type, ptr(al), res), "cpsb_minvcg_multi")
+        out = list(res)
+        for r in out:
+            r.rc = rc
+        return xs, out, rs
+
 
 def fmat_evl_inv(op: DiracOp, f_in, cg_arg: dict, f_out=None):
     """Lattice::FmatEvlInv: returns (iterations, f_out, true_res)."""

@@ -27,7 +27,8 @@ SYMBOLS = [
     "cpsb_invcg_multi_dev", "cpsb_mdagm_dev", "cpsb_minvcg_dev", "cpsb_dslash_ex", "cpsb_mdagm_ex", "cpsb_bench_dslash",
     "cpsb_kernel_launches", "cpsb_dslash_multi_dev", "cpsb_mdagm_multi_dev",
     "cpsb_redot_noalloc", "cpsb_serve_create", "cpsb_serve_submit", "cpsb_serve_poll", "cpsb_serve_wait",
-    "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert", "cpsb_minresext",
+    "cpsb_serve_stats", "cpsb_serve_destroy", "cpsb_fermion_convert", "cpsb_minresext", "cpsb_minvcg_multi",
+    "cpsb_minvcg_multi_dev",
 ]
 
 
@@ -95,6 +96,10 @@ def load():
     lib.cpsb_mdagm_dev.argtypes = [C.c_void_p, P, C.c_void_p, C.c_void_p, _dp, C.c_void_p]
     lib.cpsb_minvcg_dev.argtypes = [C.c_void_p, P, A, C.POINTER(C.c_void_p), C.c_void_p, _dp, C.c_int, _dp, C.c_int,
                                     _dp, R, C.c_void_p]
+    lib.cpsb_minvcg_multi.argtypes = [C.c_void_p, P, A, C.c_int, C.POINTER(_dp), C.POINTER(_dp), _dp, C.c_int, _dp,
+                                      C.c_int, _dp, R]
+    lib.cpsb_minvcg_multi_dev.argtypes = [C.c_void_p, P, A, C.c_int, C.POINTER(C.c_void_p), C.c_void_p, _dp, C.c_int,
+                                          _dp, C.c_int, _dp, R, C.c_void_p]
     lib.cpsb_dslash_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, C.c_int, C.c_int]
     lib.cpsb_mdagm_ex.argtypes = [C.c_void_p, P, C.c_int, _dp, _dp, _dp]
     lib.cpsb_dslash_multi_dev.argtypes = [C.c_void_p, P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,

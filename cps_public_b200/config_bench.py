@@ -14,6 +14,13 @@
       FP32 Krylov vectors with per-shift mixed-precision refinement to the FP64
       true residual, against the FP64 MInvCG.
 
+  python -m cps_public_b200.config_bench multishift_batch [--nvec 2]
+      The same multishift system for nvec pseudofermion sources at once (the
+      RHMC batch): cpsb_minvcg_multi (FP32 Krylov + refinement, and FP64)
+      against nvec one-source cpsb_minvcg calls in sequence, and, through the
+      host-pointer entry points, against nvec concurrent requests of the
+      serving loop (cpsb_serve_submit_minvcg on nvec slots).
+
 Each prints one JSON line: solves/s (right-hand sides or shift systems per
 second) with sources and solutions resident in device memory (the *_dev entry
 points; torch provides the device buffers), the same through the host-pointer
@@ -180,12 +187,110 @@ def multishift_run(stop=1e-10, e2e=True):
     return out
 
 
+def multishift_batch(a):
+    print(json.dumps(multishift_batch_run(a.stop, a.nvec)))
+
+
+def multishift_batch_run(stop=1e-10, nvec=2, e2e=True):
+    """Runs the 12-shift multishift workload on nvec sources at once and one at a
+    time; returns the result dict."""
+    init(0)
+    u = fields.random_gauge(DIMS, 0.15, 2403)
+    g = Gauge(u, DIMS)
+    op = DiracOp(g, "dwf", mass=0.01, ls=12, m5=1.8)
+    srcs = [fields.random_source(op.n // 24, 2404 + q) for q in range(nvec)]
+    shifts = list(np.logspace(-4, 1, 12))
+    ns = len(shifts)
+    import torch
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    b_d = torch.from_numpy(np.stack(srcs)).to(dev)
+    x_d = torch.zeros((nvec, ns, op.n), dtype=torch.float64, device=dev)
+    xptr = (C.c_void_p * (nvec * ns))(*[C.c_void_p(x_d[q, s].data_ptr()) for q in range(nvec) for s in range(ns)])
+    sh = np.array(shifts)
+    al = np.ones(ns)
+
+    def batched(prec, maxit):
+        rs_ = np.full((nvec, ns), stop)
+        arg = CgArg(stop, maxit, prec, 0.1, 0)
+        res = (SolveResult * nvec)()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = lib.cpsb_minvcg_multi_dev(g.h, C.byref(op.p), C.byref(arg), nvec, xptr, C.c_void_p(b_d.data_ptr()),
+                                       _lib.ptr(sh), ns, _lib.ptr(rs_), MULTI, _lib.ptr(al), res, None)
+        dt = time.perf_counter() - t0
+        _lib.check(rc, "cpsb_minvcg_multi_dev")
+        return dt, list(res), rs_
+
+    def one_at_a_time(prec, maxit):
+        t0 = time.perf_counter()
+        iters = []
+        for q in range(nvec):
+            rs_ = np.full(ns, stop)
+            arg = CgArg(stop, maxit, prec, 0.1, 0)
+            r = SolveResult()
+            xq = (C.c_void_p * ns)(*[C.c_void_p(x_d[q, s].data_ptr()) for s in range(ns)])
+            rc = lib.cpsb_minvcg_dev(g.h, C.byref(op.p), C.byref(arg), xq,
+                                     C.c_void_p(b_d[q].data_ptr()), _lib.ptr(sh), ns, _lib.ptr(rs_), MULTI,
+                                     _lib.ptr(al), C.byref(r), None)
+            _lib.check(rc, "cpsb_minvcg_dev")
+            iters.append(r.iters)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, iters
+
+    def worst_true(q_list):
+        worst = 0.0
+        for q in q_list:
+            for k in (0, 11):
+                xk = x_d[q, k].cpu().numpy()
+                ax, _ = op.MatPcDagMatPc(xk)
+                worst = max(worst, float(np.linalg.norm(srcs[q] - ax - shifts[k] * xk) / np.linalg.norm(srcs[q])))
+        return worst
+
+    batched(F32, 30)   # warm-up / tuning
+    batched(F64, 30)
+    one_at_a_time(F32, 30)
+    out = {"workload": f"dwf_multishift_24x24x24x64_ls12_x{nvec}_sources", "nvec": nvec, "shifts": shifts}
+    for name, prec in (("f32_krylov_refined", F32), ("f64", F64)):
+        dt, res, rs_ = batched(prec, 100000)
+        out["batched_" + name] = {"seconds": dt, "shift_systems_per_s": nvec * ns / dt,
+                                  "iters": [r.iters for r in res], "max_reported_rsd": float(np.max(rs_)),
+                                  "checked_true_rsd": worst_true(range(nvec))}
+        dt1, iters1 = one_at_a_time(prec, 100000)
+        out["one_at_a_time_" + name] = {"seconds": dt1, "shift_systems_per_s": nvec * ns / dt1, "iters": iters1}
+        out["batched_speedup_" + name] = dt1 / dt
+    out["batched_mixed_vs_batched_f64"] = out["batched_f64"]["seconds"] / out["batched_f32_krylov_refined"]["seconds"]
+    del b_d, x_d
+    torch.cuda.empty_cache()
+    if e2e:
+        # host-pointer paths, copies included: the batched call against nvec
+        # concurrent requests of the serving loop
+        t0 = time.perf_counter()
+        op.MInvCGMulti(srcs, shifts, [stop] * ns, max_num_iter=100000, precision=F32)
+        t_b = time.perf_counter() - t0
+        from . import Server
+        srv = Server(slots=nvec)
+        t0 = time.perf_counter()
+        rids = [srv.submit_minvcg(op, s_, shifts, [stop] * ns, max_num_iter=100000, precision=F32) for s_ in srcs]
+        for rid in rids:
+            srv.wait_minvcg(rid)
+        t_c = time.perf_counter() - t0
+        srv.close()
+        out["e2e_batched_f32_krylov_refined"] = {"seconds": t_b, "path": "cpsb_minvcg_multi (host vectors)"}
+        out["e2e_concurrent_requests_f32_krylov_refined"] = {
+            "seconds": t_c, "path": f"{nvec} cpsb_serve_submit_minvcg requests on {nvec} slots (host vectors)"}
+        out["batched_vs_concurrent_requests"] = t_c / t_b
+    g.free()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["mobius12", "multishift"])
+    ap.add_argument("workload", choices=["mobius12", "multishift", "multishift_batch"])
     ap.add_argument("--stop", type=float, default=1e-10)
+    ap.add_argument("--nvec", type=int, default=2)
     a = ap.parse_args()
-    {"mobius12": mobius12, "multishift": multishift}[a.workload](a)
+    {"mobius12": mobius12, "multishift": multishift, "multishift_batch": multishift_batch}[a.workload](a)
 
 
 if __name__ == "__main__":

@@ -34,6 +34,13 @@ struct M5Coef {
 };
 cudaError_t launch_m5(int prec, int dag, const Geom &g, SpinorPtr out, SpinorPtr in, SpinorPtr x, const M5Coef &cf,
                       int xpay, int norm, Reduce red, const int *skip, cudaStream_t st);
+// The Mobius hop with the M5 sweeps of its output fused in (hop_m5.cuh), A as
+// for launch_dslash with A.a the output scale:
+//   A.dag 0: out = a mix(M5^-1 (D in))   (cf the dag-0 coefficients; no xpay, no norm)
+//   A.dag 1: out = [x +] a M5^-dag(mix^dag(D^dag in))  [, |out|^2 into A.red]
+// cudaErrorNotSupported where no fused form exists; the caller then runs
+// launch_dslash and launch_m5.
+cudaError_t launch_hop_m5(int prec, const DslashArgs &A, const M5Coef &cf, int xpay, int norm, cudaStream_t st);
 
 // zMobius form (complex per-slice coefficients, zmobius_m5inv.C:247-400 and
 // :403-686, zmobius_dslash_5_plus.C:125-376): one table per launch shape, in

@@ -543,6 +543,76 @@ int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg 
   });
 }
 
+static void check_minvcg_multi(int nvec, const void *x, const void *b, const double *shift, int nshift,
+                               const double *rsd, int type, const double *alpha, const cpsb_solve_result *res) {
+  if (nvec < 1 || nvec > MAX_RHS) throw Error{CPSB_ERR_ARG, "nvec must be in [1, 16]"};
+  if (!x || !b || !shift || !rsd || !res || nshift < 1 || nshift > 32) throw Error{CPSB_ERR_ARG, "bad multishift arguments"};
+  if (type != CPSB_MULTI && type != CPSB_SINGLE) throw Error{CPSB_ERR_UNSUPPORTED, "only MULTI and SINGLE are implemented"};
+  if (type == CPSB_SINGLE && !alpha) throw Error{CPSB_ERR_ARG, "SINGLE needs alpha"};
+}
+
+int cpsb_minvcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nvec, double **x,
+                      const double *const *b, const double *shift, int nshift, double *rsd, int type,
+                      const double *alpha, cpsb_solve_result *res) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    check_minvcg_multi(nvec, x, b, shift, nshift, rsd, type, alpha, res);
+    const int nsol = type == CPSB_SINGLE ? 1 : nshift;
+    for (int i = 0; i < nvec * nsol; i++)
+      if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
+    for (int q = 0; q < nvec; q++)
+      if (!b[q]) throw Error{CPSB_ERR_ARG, "null source vector"};
+    cudaStream_t st = ctx().stream;
+    const long n1 = cb_sites(h, p);
+    const Geom g1 = geom_of(h, p, 1);
+    Field chi(P64, n1 * nvec);
+    upload(chi, b, nvec, g1, st);
+    std::vector<Field> xs(nsol);
+    for (int s = 0; s < nsol; s++) {
+      xs[s].create(P64, n1 * nvec);
+      CK(cudaMemsetAsync(xs[s].data.p, 0, xs[s].data.bytes, st));
+    }
+    const int rc = multishift_multi(&h->g, *p, *a, nvec, chi, xs, shift, nshift, rsd, type, alpha, res, st);
+    std::vector<double *> hx(nvec);
+    for (int s = 0; s < nsol; s++) {
+      for (int q = 0; q < nvec; q++) hx[q] = x[q * nsol + s];
+      download(hx.data(), nvec, g1, xs[s], st);
+    }
+    return rc;
+  });
+}
+
+int cpsb_minvcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nvec,
+                          double *const *x, const double *b, const double *shift, int nshift, double *rsd, int type,
+                          const double *alpha, cpsb_solve_result *res, void *stream) {
+  return guarded([&] {
+    need_init();
+    check_params(h, p);
+    check_cg(a);
+    check_minvcg_multi(nvec, x, b, shift, nshift, rsd, type, alpha, res);
+    const int nsol = type == CPSB_SINGLE ? 1 : nshift;
+    for (int i = 0; i < nvec * nsol; i++)
+      if (!x[i]) throw Error{CPSB_ERR_ARG, "null solution vector"};
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    const long n1 = cb_sites(h, p);
+    const Geom g1 = geom_of(h, p, 1);
+    Field chi(P64, n1 * nvec);
+    CK(launch_pack(P64, chi.ptr(), b, geom_of(h, p, nvec), st));
+    std::vector<Field> xs(nsol);
+    for (int s = 0; s < nsol; s++) {
+      xs[s].create(P64, n1 * nvec);
+      CK(cudaMemsetAsync(xs[s].data.p, 0, xs[s].data.bytes, st));
+    }
+    const int rc = multishift_multi(&h->g, *p, *a, nvec, chi, xs, shift, nshift, rsd, type, alpha, res, st);
+    for (int s = 0; s < nsol; s++)
+      for (int q = 0; q < nvec; q++) CK(launch_unpack(P64, x[q * nsol + s], xs[s].view((long)q * n1), g1, st));
+    CK(cudaStreamSynchronize(st));
+    return rc;
+  });
+}
+
 // out = fa x + fb y (y optional) on FP64 fields of one right-hand side.
 static void lin64(const Geom &g, const Field &o, double fa, const Field &x, double fb, const Field *y,
                   cudaStream_t st) {

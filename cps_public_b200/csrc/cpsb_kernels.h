@@ -36,6 +36,7 @@ struct DslashArgs {
   // advances the recurrence scalars as the r-update kernel of blas.cu does.
   CgState *cg;
   SpinorPtr cg_r, cg_p;
+  int cg_shift;           // nonzero: the solve's shift is nonzero (the update reads p)
 };
 
 // Kernel-launch accounting (cpsb_kernel_launches): every launcher calls

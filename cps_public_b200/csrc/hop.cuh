@@ -12,30 +12,36 @@
 // Work decomposition (the column layout of cpsb_device.cuh).  A field is a
 // set of columns, one per (4-D checkerboard site x, slice class k), each
 // holding the class's slices of that site as consecutive entries.  A work unit
-// is a tile of TX consecutive columns of one class; a block sweeps its unit's
-// columns x slices for every right-hand side.  Thread t of the block owns
-// column t / C and slice t % C (C the column height), so:
-//  * the 32 lanes of a warp read 32/C whole neighbour columns per 16-byte
-//    chunk -- contiguous 128-byte segments that start on 128-byte boundaries
-//    when C is a multiple of 8 (DWF Ls 16: 4 columns x 8 slices per warp);
+// is a tile of TX consecutive columns of one class, taken for a group of RG
+// right-hand sides at a time (RG = 1 or all of them; A.rg); a block sweeps its
+// unit's columns x slices x right-hand sides of the group.  Thread t owns
+// slice t % C (C the column height), right-hand side (t / C) % RG and column
+// t / (C RG), so:
+//  * the 32 lanes of a warp read whole neighbour columns per 16-byte chunk --
+//    contiguous 128-byte segments that start on 128-byte boundaries when C is
+//    a multiple of 8 (DWF Ls 16: 4 columns x 8 slices per warp);
 //  * the unit's 8*TX links are loaded, reconstructed (recon-12 storage) and
 //    written to shared memory once, with the antiperiodic time sign folded in,
 //    and every slice and right-hand side of the unit reads them from there,
 //    C lanes at a time on the same address (a broadcast); for FP32 / 16-bit
 //    each element is stored as (re, re, im, im) so that it is one operand pair
-//    of the packed FP32x2 instructions;
+//    of the packed FP32x2 instructions (launch shapes without the table, LC
+//    false, read recon-12 links from global memory per thread instead);
 //  * neighbour column offsets are computed once per unit;
-//  * units run in column order over every right-hand side in turn, so the
-//    columns that blocks resident together touch -- their own and their
-//    neighbours' up to one time slice away -- stay in L2 while every
-//    neighbour that needs them reads them (each input is fetched from DRAM
-//    once even when the right-hand sides together exceed L2).
+//  * units run in tile order, optionally inside groups of A.rgroup right-hand
+//    sides (the group slowest), and the grid holds only the blocks resident at
+//    once, so the columns that blocks in flight touch -- their own and their
+//    neighbours' up to one time slice away -- are read while they sit in L2.
 //
 // FP32 and 16-bit storage keep spins (2p, 2p+1) of one colour in the two lanes
 // of a float2 and run every step of the hop in Blackwell's packed FP32x2
-// arithmetic (FFMA2 / FADD2 / FMUL2).  16-bit values are decoded to exact
-// integers; the quantum of each neighbour is folded into the FMA that
-// accumulates it, and the output is re-encoded with its own quantum.
+// arithmetic (FFMA2 / FADD2 / FMUL2).  16-bit spinors are stored as biased
+// 15-bit integers (value + 16384, in [1, 32767]) with one float quantum per
+// entry; the spin projection of each 16-bit neighbour is done on the packed
+// integers themselves (two 16-bit lanes per 32-bit add, exact because the sum
+// of two biased values stays below 2^16), decoded once per half spinor, and the
+// neighbour's quantum is folded into the FMA that accumulates it.  The output is
+// re-encoded with its own quantum.
 //
 // Epilogues (no extra pass over memory): out = x + a*D in (XPAY) or a*D in,
 // optionally |out|^2 per right-hand side (NORM), or the CG residual update
@@ -491,6 +497,189 @@ __device__ __forceinline__ int tile_order(const Geom &g, int u, int TX, int tord
   return yb + nyb * (z + g.lz * t);
 }
 
+// ---------------------------------------------------------------- one entry
+// Per-entry context of the hop: the unit's link table column, the neighbour
+// column offsets and checkerboard indices, and the 5th-direction neighbours.
+struct HopCtx {
+  const void *lk;
+  int nb[8], xn[8];
+  int par_out, x;
+  bool flip_f, flip_b;
+  unsigned e5m, e5p;
+  double f5m, f5p;
+};
+
+// The hop of one FP64 entry (right-hand side at entry offset rb): the 8
+// neighbours with links from the table (LC) or global memory, and with A.hop5
+// the 5th-direction neighbours; no scaling.
+template <int P, bool LC, bool DAG, int DEPTH>
+__device__ __forceinline__ Spinor<double> hop_entry_64(const DslashArgs &A, const HopCtx &hc, unsigned rb) {
+  constexpr float sdag = DAG ? -1.f : 1.f;
+  const void *lk = hc.lk;
+  const int par_out = hc.par_out, x = hc.x;
+  const double2 *l64 = (const double2 *)lk;
+  Spinor<double> acc;
+  zero(acc);
+  // DEPTH: neighbours whose loads are in flight ahead of the one computed
+  Raw<P64> nxt;
+  if (DEPTH >= 1) nxt = load_raw<P64>(A.in, rb + (unsigned)hc.nb[0]);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    Raw<P64> cur;
+    if (DEPTH >= 1) {
+      cur = nxt;
+      if (j < 7) nxt = load_raw<P64>(A.in, rb + (unsigned)hc.nb[j + 1]);
+    } else {
+      cur = load_raw<P64>(A.in, rb + (unsigned)hc.nb[j]);
+    }
+    const int mu = j & 3;
+    const double sg = j < 4 ? -(double)sdag : (double)sdag;
+    const Half<double> h = project(unpack64(cur), mu, sg);
+    Link<double> l;
+    if (LC) {
+#pragma unroll
+      for (int e = 0; e < 9; e++) {
+        const double2 v = l64[j * 9 + e];
+        l.u[e / 3][e % 3] = mk(v.x, v.y);
+      }
+    } else {
+      l = j < 4 ? load_link<P64>(A.U, par_out, mu, x) : load_link<P64>(A.U, 1 - par_out, mu, hc.xn[j]);
+    }
+    accum_reconstruct(acc, j < 4 ? umul(l, h) : umul_dag(l, h), mu, sg);
+  }
+  if (A.hop5) {
+    // dwf_dslash_5_plus: upper (lower) chirality from s-1 (s+1) at dag 0, swapped at dag 1
+    const double2 *bm = entry_ptr<12, const double2>(A.in.data, rb + hc.e5m);
+    const double2 *bp = entry_ptr<12, const double2>(A.in.data, rb + hc.e5p);
+    // chunks 0-5 are spins 0, 1 (the upper chirality), 6-11 spins 2, 3
+    const int um = DAG ? 6 : 0, up = DAG ? 0 : 6;  // pair taken from s-1 / s+1
+    double2 vm[6], vp[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      vm[q] = __ldg(bm + 8 * (um + q));
+      vp[q] = __ldg(bp + 8 * (up + q));
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const cplx<double> lo = cscale(hc.f5m, mk(vm[q].x, vm[q].y)), hi = cscale(hc.f5p, mk(vp[q].x, vp[q].y));
+      cplx<double> &u = acc.c[q / 3][q % 3], &l = acc.c[2 + q / 3][q % 3];
+      if (!DAG) {
+        u = u + lo;
+        l = l + hi;
+      } else {
+        l = l + lo;
+        u = u + hi;
+      }
+    }
+  }
+  return acc;
+}
+
+// The same for FP32 / 16-bit storage in packed FP32x2 arithmetic.
+template <int P, bool LC, bool DAG, int DEPTH>
+__device__ __forceinline__ SpX2 hop_entry_x2(const DslashArgs &A, const HopCtx &hc, unsigned rb) {
+  constexpr float sdag = DAG ? -1.f : 1.f;
+  const void *lk = hc.lk;
+  const int par_out = hc.par_out, x = hc.x;
+  const float4 *l32 = (const float4 *)lk;
+  AccX2 acc;
+  zero_x2(acc);
+  // DEPTH (1 or 2): neighbours whose loads are in flight ahead of the one computed
+  Raw<P> nxt, nx2;
+  nxt = load_raw<P>(A.in, rb + (unsigned)hc.nb[0]);
+  if (DEPTH >= 2) nx2 = load_raw<P>(A.in, rb + (unsigned)hc.nb[1]);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const Raw<P> cur = nxt;
+    if (DEPTH >= 2) {
+      nxt = nx2;
+      if (j < 6) nx2 = load_raw<P>(A.in, rb + (unsigned)hc.nb[j + 2]);
+    } else if (j < 7) {
+      nxt = load_raw<P>(A.in, rb + (unsigned)hc.nb[j + 1]);
+    }
+    float nrm;
+    const float sg = j < 4 ? -sdag : sdag;
+    // FP32: unpack, then project; 16-bit: project on the integers (iproject)
+    SpX2 v;
+    if constexpr (P == P32) v = unpack(cur, &nrm);
+    else nrm = cur.nrm;
+    const float4 *lj = l32 + j * 9;
+    Link<float> lr;
+    if (!LC) {
+      lr = j < 4 ? load_link<P>(A.U, par_out, j & 3, x) : load_link<P>(A.U, 1 - par_out, j & 3, hc.xn[j]);
+      if ((j == 3 && hc.flip_f) || (j == 7 && hc.flip_b)) nrm = -nrm;
+    }
+#define CPSB_NB(MU)                                                                            \
+  {                                                                                            \
+    HfX2 h;                                                                                    \
+    if constexpr (P == P16) h = sg > 0.f ? iproject<MU, true>(cur) : iproject<MU, false>(cur); \
+    else h = project_x2<MU>(v, sg);                                                            \
+    const HfX2 uh = LC ? (j < 4 ? umul_x2<false>(lj, h) : umul_x2<true>(lj, h))                \
+                       : (j < 4 ? umul_x2r<false>(lr, h) : umul_x2r<true>(lr, h));             \
+    accum_x2<MU>(acc, uh, sg, nrm);                                                            \
+  }
+    switch (j & 3) {
+      case 0: CPSB_NB(0) break;
+      case 1: CPSB_NB(1) break;
+      case 2: CPSB_NB(2) break;
+      default: CPSB_NB(3) break;
+    }
+#undef CPSB_NB
+  }
+  if (A.hop5) {
+    // upper pair from s-1 and lower from s+1 at dag 0 (swapped at dag 1),
+    // scaled by 2 a5_inv or, across the walls, -2 m_f a5_inv
+    const int pm = DAG ? 1 : 0;
+    float nm, np;
+    const HfX2 vm = load_pair<P>(A.in, rb + hc.e5m, pm, &nm);
+    const HfX2 vp = load_pair<P>(A.in, rb + hc.e5p, 1 - pm, &np);
+    const float2 cm = f2b((float)hc.f5m * nm), cp = f2b((float)hc.f5p * np);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (!DAG) {
+        acc.ure[c] = fma2(cm, vm.re[c], acc.ure[c]);
+        acc.uim[c] = fma2(cm, vm.im[c], acc.uim[c]);
+        acc.lnre[c] = fma2(cp, vp.re[c], acc.lnre[c]);
+        acc.lnim[c] = fma2(cp, vp.im[c], acc.lnim[c]);
+      } else {
+        acc.lnre[c] = fma2(cm, vm.re[c], acc.lnre[c]);
+        acc.lnim[c] = fma2(cm, vm.im[c], acc.lnim[c]);
+        acc.ure[c] = fma2(cp, vp.re[c], acc.ure[c]);
+        acc.uim[c] = fma2(cp, vp.im[c], acc.uim[c]);
+      }
+    }
+  }
+  return merge_x2(acc);
+}
+
+// The context of slice sp of tile column xl (checkerboard site x, class k)
+// from the unit's tables.
+template <int P, bool LC>
+__device__ __forceinline__ void entry_ctx(HopCtx &hc, const DslashArgs &A, const unsigned char *dsh, const HopShm &L,
+                                          int xl, int x, int k, int sp, int par_out) {
+  const Geom &g = A.g;
+  const int *nbo_sh = (const int *)(dsh + L.nbo);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    hc.nb[j] = nbo_sh[xl * 8 + j] + sp;
+    hc.xn[j] = LC ? 0 : ((const int *)(dsh + L.xn))[xl * 8 + j];
+  }
+  hc.par_out = par_out;
+  hc.x = x;
+  // !LC: the antiperiodic sign of reconstructed links at the t boundary
+  const Coord cx = decode(g, x, par_out);
+  hc.flip_f = !LC && P != P64 && A.bc_t_sign < 0 && cx.t == g.lt - 1;
+  hc.flip_b = !LC && P != P64 && A.bc_t_sign < 0 && cx.t == 0;
+  // 5th-direction neighbours (DWF): slices s-1, s+1 of the same 4-D site
+  const int s = g.ncls == 2 ? k + 2 * sp : sp;
+  const int sm = s == 0 ? g.ls - 1 : s - 1, sq = s == g.ls - 1 ? 0 : s + 1;
+  hc.e5m = site_entry(g, sm, x);
+  hc.e5p = site_entry(g, sq, x);
+  hc.f5m = s == 0 ? A.hop5_wall : A.hop5_fact;
+  hc.f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
+  hc.lk = dsh + L.links + (size_t)xl * LSTR * 16;
+}
+
 // LC: links from the unit's shared-memory table (otherwise each entry loads
 // and reconstructs its own, which suits columns of one or two entries).
 //
@@ -501,11 +690,20 @@ __device__ __forceinline__ int tile_order(const Geom &g, int u, int TX, int tord
 // every link read is a broadcast).  The grid holds no more blocks than are
 // resident at once, so the units in flight are one contiguous run of tiles and
 // their neighbour columns are read while they are in L2.
-template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, bool CGR, bool DAG, int DEPTH>
+// CGR: 0 none, 1 the fused residual update r -= alpha A p, 2 the same for the
+// shifted operator, r -= alpha (A p + shift p).
+template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, int CGR, bool DAG, int DEPTH>
 __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const Geom &g = A.g;
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ double red[NT / 32];
+  // alpha = |r|^2 / (<p, A p> + shift |p|^2) per right-hand side, once per block
+  // (the loop over units starts with a barrier)
+  __shared__ double cg_alpha[MAX_RHS];
+  if (CGR && threadIdx.x < g.nrhs) {
+    const CgState *S = A.cg;
+    cg_alpha[threadIdx.x] = S->rr[threadIdx.x] / (S->d[threadIdx.x] + S->shift * S->pp[threadIdx.x]);
+  }
   const int C0 = g.cs[0];
   const int RG = A.rg;
   const int TX = NT / (C0 * RG);
@@ -523,8 +721,6 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const int per_group = ntiles * ncls;
   const int nunits = per_group * ((g.nrhs + G - 1) / G);
   const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
-  constexpr float sdag = DAG ? -1.f : 1.f;
-  const int *nbo_sh = (const int *)(dsh + L.nbo);
   for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
     const int grp = unit / per_group, rem = unit - grp * per_group;
     const int k = rem % ncls, tile = tile_order(g, rem / ncls, TX, A.torder);
@@ -535,23 +731,9 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
     const int x = tile * TX + xl;
     const int C = g.cs[k];
     if (xl >= TX || x >= g.n4cb || sp >= C) continue;
-    int nb[8], xn[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      nb[j] = nbo_sh[xl * 8 + j] + sp;
-      xn[j] = LC ? 0 : ((const int *)(dsh + L.xn))[xl * 8 + j];
-    }
-    // !LC: the antiperiodic sign of reconstructed links at the t boundary
-    const Coord cx = decode(g, x, par_out);
-    const bool flip_f = !LC && P != P64 && A.bc_t_sign < 0 && cx.t == g.lt - 1;
-    const bool flip_b = !LC && P != P64 && A.bc_t_sign < 0 && cx.t == 0;
+    HopCtx hc;
+    entry_ctx<P, LC>(hc, A, dsh, L, xl, x, k, sp, par_out);
     const unsigned own = (k ? (unsigned)g.kb1 : 0u) + (unsigned)x * (unsigned)C + (unsigned)sp;
-    // 5th-direction neighbours (DWF): slices s-1, s+1 of the same 4-D site
-    const int s = ncls == 2 ? k + 2 * sp : sp;
-    const int sm = s == 0 ? g.ls - 1 : s - 1, sq = s == g.ls - 1 ? 0 : s + 1;
-    const unsigned e5m = site_entry(g, sm, x), e5p = site_entry(g, sq, x);
-    const double f5m = s == 0 ? A.hop5_wall : A.hop5_fact, f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
-    const void *lk = dsh + L.links + (size_t)xl * LSTR * 16;
     const int rhs_end = min(g.nrhs, (grp + 1) * G);
     for (int rhs = grp * G + rl; rhs < rhs_end; rhs += RG) {
       if (A.skip && A.skip[rhs]) continue;
@@ -559,61 +741,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
       const unsigned i = rb + own;
       if constexpr (P == P64) {
         // ------------------------------------------------ FP64
-        const double2 *l64 = (const double2 *)lk;
-        Spinor<double> acc;
-        zero(acc);
-        // DEPTH: neighbours whose loads are in flight ahead of the one computed
-        Raw<P64> nxt;
-        if (DEPTH >= 1) nxt = load_raw<P64>(A.in, rb + (unsigned)nb[0]);
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          Raw<P64> cur;
-          if (DEPTH >= 1) {
-            cur = nxt;
-            if (j < 7) nxt = load_raw<P64>(A.in, rb + (unsigned)nb[j + 1]);
-          } else {
-            cur = load_raw<P64>(A.in, rb + (unsigned)nb[j]);
-          }
-          const int mu = j & 3;
-          const double sg = j < 4 ? -(double)sdag : (double)sdag;
-          const Half<double> h = project(unpack64(cur), mu, sg);
-          Link<double> l;
-          if (LC) {
-#pragma unroll
-            for (int e = 0; e < 9; e++) {
-              const double2 v = l64[j * 9 + e];
-              l.u[e / 3][e % 3] = mk(v.x, v.y);
-            }
-          } else {
-            l = j < 4 ? load_link<P64>(A.U, par_out, mu, x) : load_link<P64>(A.U, 1 - par_out, mu, xn[j]);
-          }
-          accum_reconstruct(acc, j < 4 ? umul(l, h) : umul_dag(l, h), mu, sg);
-        }
-        if (A.hop5) {
-          // dwf_dslash_5_plus: upper (lower) chirality from s-1 (s+1) at dag 0, swapped at dag 1
-          const double2 *bm = entry_ptr<12, const double2>(A.in.data, rb + e5m);
-          const double2 *bp = entry_ptr<12, const double2>(A.in.data, rb + e5p);
-          // chunks 0-5 are spins 0, 1 (the upper chirality), 6-11 spins 2, 3
-          const int um = DAG ? 6 : 0, up = DAG ? 0 : 6;  // pair taken from s-1 / s+1
-          double2 vm[6], vp[6];
-#pragma unroll
-          for (int q = 0; q < 6; q++) {
-            vm[q] = __ldg(bm + 8 * (um + q));
-            vp[q] = __ldg(bp + 8 * (up + q));
-          }
-#pragma unroll
-          for (int q = 0; q < 6; q++) {
-            const cplx<double> lo = cscale(f5m, mk(vm[q].x, vm[q].y)), hi = cscale(f5p, mk(vp[q].x, vp[q].y));
-            cplx<double> &u = acc.c[q / 3][q % 3], &l = acc.c[2 + q / 3][q % 3];
-            if (!DAG) {
-              u = u + lo;
-              l = l + hi;
-            } else {
-              l = l + lo;
-              u = u + hi;
-            }
-          }
-        }
+        Spinor<double> acc = hop_entry_64<P, LC, DAG, DEPTH>(A, hc, rb);
         const double a = A.a;
         if (XPAY) {
           const Spinor<double> xv = unpack64(load_raw<P64>(A.x, i));
@@ -628,11 +756,10 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
             for (int r = 0; r < 3; r++) acc.c[s2][r] = cscale(a, acc.c[s2][r]);
         }
         if (CGR) {
-          const CgState *S = A.cg;
-          const double sigma = S->shift;
-          const double alpha = S->rr[rhs] / (S->d[rhs] + sigma * S->pp[rhs]);
+          const double alpha = cg_alpha[rhs];
           Spinor<double> rv = unpack64(load_raw<P64>(A.cg_r, i));
-          if (sigma != 0.0) {
+          if (CGR == 2) {
+            const double sigma = A.cg->shift;
             const Spinor<double> pv = unpack64(load_raw<P64>(A.cg_p, i));
 #pragma unroll
             for (int s2 = 0; s2 < 4; s2++)
@@ -651,75 +778,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         }
       } else {
         // ------------------------------------------------ FP32 / 16-bit, packed
-        const float4 *l32 = (const float4 *)lk;
-        AccX2 acc;
-        zero_x2(acc);
-        // DEPTH (1 or 2): neighbours whose loads are in flight ahead of the one computed
-        Raw<P> nxt, nx2;
-        nxt = load_raw<P>(A.in, rb + (unsigned)nb[0]);
-        if (DEPTH >= 2) nx2 = load_raw<P>(A.in, rb + (unsigned)nb[1]);
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const Raw<P> cur = nxt;
-          if (DEPTH >= 2) {
-            nxt = nx2;
-            if (j < 6) nx2 = load_raw<P>(A.in, rb + (unsigned)nb[j + 2]);
-          } else if (j < 7) {
-            nxt = load_raw<P>(A.in, rb + (unsigned)nb[j + 1]);
-          }
-          float nrm;
-          const float sg = j < 4 ? -sdag : sdag;
-          // FP32: unpack, then project; 16-bit: project on the integers (iproject)
-          SpX2 v;
-          if constexpr (P == P32) v = unpack(cur, &nrm);
-          else nrm = cur.nrm;
-          const float4 *lj = l32 + j * 9;
-          Link<float> lr;
-          if (!LC) {
-            lr = j < 4 ? load_link<P>(A.U, par_out, j & 3, x) : load_link<P>(A.U, 1 - par_out, j & 3, xn[j]);
-            if ((j == 3 && flip_f) || (j == 7 && flip_b)) nrm = -nrm;
-          }
-#define CPSB_NB(MU)                                                                              \
-  {                                                                                              \
-    HfX2 h;                                                                                      \
-    if constexpr (P == P16) h = sg > 0.f ? iproject<MU, true>(cur) : iproject<MU, false>(cur);   \
-    else h = project_x2<MU>(v, sg);                                                              \
-    const HfX2 uh = LC ? (j < 4 ? umul_x2<false>(lj, h) : umul_x2<true>(lj, h))                  \
-                       : (j < 4 ? umul_x2r<false>(lr, h) : umul_x2r<true>(lr, h));               \
-    accum_x2<MU>(acc, uh, sg, nrm);                                                              \
-  }
-          switch (j & 3) {
-            case 0: CPSB_NB(0) break;
-            case 1: CPSB_NB(1) break;
-            case 2: CPSB_NB(2) break;
-            default: CPSB_NB(3) break;
-          }
-#undef CPSB_NB
-        }
-        if (A.hop5) {
-          // upper pair from s-1 and lower from s+1 at dag 0 (swapped at dag 1),
-          // scaled by 2 a5_inv or, across the walls, -2 m_f a5_inv
-          const int pm = DAG ? 1 : 0;
-          float nm, np;
-          const HfX2 vm = load_pair<P>(A.in, rb + e5m, pm, &nm);
-          const HfX2 vp = load_pair<P>(A.in, rb + e5p, 1 - pm, &np);
-          const float2 cm = f2b((float)f5m * nm), cp = f2b((float)f5p * np);
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            if (!DAG) {
-              acc.ure[c] = fma2(cm, vm.re[c], acc.ure[c]);
-              acc.uim[c] = fma2(cm, vm.im[c], acc.uim[c]);
-              acc.lnre[c] = fma2(cp, vp.re[c], acc.lnre[c]);
-              acc.lnim[c] = fma2(cp, vp.im[c], acc.lnim[c]);
-            } else {
-              acc.lnre[c] = fma2(cm, vm.re[c], acc.lnre[c]);
-              acc.lnim[c] = fma2(cm, vm.im[c], acc.lnim[c]);
-              acc.ure[c] = fma2(cp, vp.re[c], acc.ure[c]);
-              acc.uim[c] = fma2(cp, vp.im[c], acc.uim[c]);
-            }
-          }
-        }
-        SpX2 o = merge_x2(acc);
+        SpX2 o = hop_entry_x2<P, LC, DAG, DEPTH>(A, hc, rb);
         const float2 a2 = f2b((float)A.a);
         if (XPAY) {
           float xn;
@@ -747,21 +806,23 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         }
         if (CGR) {
           // r -= alpha (A p + shift p), A p = o in registers (cg_r_update of blas.cu)
-          const CgState *S = A.cg;
-          const double sigma = S->shift;
-          const float alpha = (float)(S->rr[rhs] / (S->d[rhs] + sigma * S->pp[rhs]));
+          const float alpha = (float)cg_alpha[rhs];
           float rn;
           SpX2 rv = unpack(load_raw<P>(A.cg_r, i), &rn);
           float pn = 0.f;
           SpX2 pv;
-          if (sigma != 0.0) pv = unpack(load_raw<P>(A.cg_p, i), &pn);
+          double sigma = 0.0;
+          if (CGR == 2) {
+            sigma = A.cg->shift;
+            pv = unpack(load_raw<P>(A.cg_p, i), &pn);
+          }
           const float2 ma = f2b(-alpha), rs = f2b(rn), ps = f2b((float)sigma * pn);
 #pragma unroll
           for (int p = 0; p < 2; p++)
 #pragma unroll
             for (int cc = 0; cc < 3; cc++) {
               float2 are = o.re[p][cc], aim = o.im[p][cc];
-              if (sigma != 0.0) {
+              if (CGR == 2) {
                 are = fma2(ps, pv.re[p][cc], are);
                 aim = fma2(ps, pv.im[p][cc], aim);
               }
@@ -892,11 +953,12 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
 #define CPSB_HOP_D(XP, NR, CG)          \
   if (A.dag) CPSB_HOP(XP, NR, CG, true) \
   else CPSB_HOP(XP, NR, CG, false)
-  if (cgr) CPSB_HOP_D(true, false, true)
-  else if (xpay && norm) CPSB_HOP_D(true, true, false)
-  else if (xpay) CPSB_HOP_D(true, false, false)
-  else if (norm) CPSB_HOP_D(false, true, false)
-  else CPSB_HOP_D(false, false, false)
+  if (cgr && A.cg_shift) CPSB_HOP_D(true, false, 2)
+  else if (cgr) CPSB_HOP_D(true, false, 1)
+  else if (xpay && norm) CPSB_HOP_D(true, true, 0)
+  else if (xpay) CPSB_HOP_D(true, false, 0)
+  else if (norm) CPSB_HOP_D(false, true, 0)
+  else CPSB_HOP_D(false, false, 0)
 #undef CPSB_HOP_D
 #undef CPSB_HOP
   return launched();

@@ -118,6 +118,13 @@ struct Operator {
   // views (SpinorPtr) with nsites() sites each; the Field forms pass whole fields.
   void hop(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, double a, const SpinorPtr *x,
            const Reduce *red, const int *skip, cudaStream_t st);
+  // Mobius: the hop with the M5 operation that follows it fused in (launch_hop_m5):
+  // dag 0 out = a mix(M5^-1 D in), dag 1 out = [x +] a M5^-dag(mix^dag(D^dag in)).
+  // Returns false, launching nothing, where no fused form exists or fusion is
+  // switched off (CPSB_M5_FUSE=0 in the environment).
+  bool hop_m5(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, double a, const M5Coef &cf,
+              const SpinorPtr *x, const Reduce *red, const int *skip, cudaStream_t st);
+  bool fuse_m5 = true;
   // DiracOp::Dslash front end
   void dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, cudaStream_t st);
   // out = MatPc in (dag 0) or MatPcDag in (dag 1); |out|^2 into red when given.
@@ -147,7 +154,7 @@ struct Operator {
   void matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
                      cudaStream_t st);
   void mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip, CgState *S,
-                  const SpinorPtr &r, const Reduce *red_r, cudaStream_t st);
+                  const SpinorPtr &r, const Reduce *red_r, bool shifted, cudaStream_t st);
   // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
   // (zmobius_m5inv, dag 0); out = D4(cb) in (zmobius_dslash_4, dag 0);
   // out = x + f H5 in (zmobius_kappa_dslash_5_plus_cmplx with factor f, dag 0).
@@ -177,13 +184,16 @@ struct CgSolver {
   double shift = 0;                   // sigma of the solve in progress
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;
+  bool graph_shifted = false;
   unsigned long long graph_nodes = 0;
   std::mutex busy;
 
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
   ~CgSolver();
   // Solves with x64 (initial guess) and b64 already packed; fills res[nrhs].
-  int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma = 0.0);
+  // stop_q: per-right-hand-side stop_rsd (nullptr: a.stop_rsd for all).
+  int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma = 0.0,
+            const double *stop_q = nullptr);
 
  private:
   void launch_batch(int k, cudaStream_t st);
@@ -196,10 +206,16 @@ int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_
 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
 
-// refiner: the one-RHS solver for the per-shift refinement of reduced-precision
-// Krylov runs (nullptr: the library's cached one, taken under its lock).
+// refiner: the solver for the per-shift refinement of reduced-precision
+// Krylov runs, one right-hand side per source vector (nullptr: the library's
+// cached one, taken under its lock).
 int multishift(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, Field &b64, std::vector<Field> &x,
                const double *shift, int nshift, double *rsd, int type, const double *alpha, cpsb_solve_result *res,
                cudaStream_t st, CgSolver *refiner = nullptr);
+// nvec source vectors with the same shifts solved together (multishift.cu):
+// chi and every x[s] hold nvec x n sites; rsd[q * nshift + s]; res[nvec].
+int multishift_multi(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, int nvec, Field &chi,
+                     std::vector<Field> &x, const double *shift, int nshift, double *rsd, int type,
+                     const double *alpha, cpsb_solve_result *res, cudaStream_t st, CgSolver *refiner = nullptr);
 
 }  // namespace cpsb

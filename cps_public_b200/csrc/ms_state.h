@@ -2,16 +2,18 @@
 //
 // Mirrors the scalars of DiracOp::MInvCG (cps_pp/src/util/dirac_op/d_op_base/
 // noarch/minvcg.C:97-125): a, b, c, cp, d, the shifted z/bs recurrences and the
-// per-shift convergence flags.  The last block of the residual reduction
-// advances all of them, so an iteration is a fixed launch sequence.
+// per-shift convergence flags, one set per source vector of a batched solve.
+// The last block of the residual reduction advances all of them, so an
+// iteration is a fixed launch sequence.
 #pragma once
+#include "cg_state.h"
 
 namespace cpsb {
 
 constexpr int MAX_SHIFT = 32;
 
 struct MsState {
-  double a, b, bp, c, cp, d_mm, pp;   // d = d_mm + shift[0]*pp
+  double a, b, bp, c, cp, pp;         // d = d_mm + shift[0]*pp
   double z[2][MAX_SHIFT];
   double bs[MAX_SHIFT];
   double as[MAX_SHIFT];
@@ -28,8 +30,18 @@ struct MsState {
   int k;                              // iterations performed (the init step is k = 0)
   int max_iter;
   int done;                           // set when every shift converged or k reached max_iter
-  int done_applied;                   // set after the solution update of the final iteration
   int breakdown;
+};
+
+// The states of the source vectors solved together, with the per-vector
+// values that kernels read or write as arrays: |M p_0|^2 (the fused norm of
+// MatPcDagMatPc writes result[q]) and the flag set after the solution update
+// of a vector's final iteration (the operator's per-right-hand-side skip mask).
+struct MsBatch {
+  MsState s[MAX_RHS];
+  double d_mm[MAX_RHS];
+  int done_applied[MAX_RHS];
+  int nvec;
 };
 
 }  // namespace cpsb

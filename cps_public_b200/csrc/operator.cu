@@ -14,6 +14,7 @@
 //          (dwf_mdagm.C:32-62, mobius_mdagm.C:33-60, wilson_mdagm.C:83-160).
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <atomic>
@@ -339,6 +340,7 @@ Operator::Operator(Gauge *g, const cpsb_dirac_params &pp, int pr, int nr) : G(g)
   if (ls < 1 || ls > 64) throw Error{CPSB_ERR_ARG, "ls out of range"};
   if (nrhs < 1 || nrhs > MAX_RHS) throw Error{CPSB_ERR_ARG, "nrhs out of range"};
   geom = make_geom(G->dims, ls, nrhs, p.action == CPSB_DWF);
+  if (const char *f = getenv("CPSB_M5_FUSE")) fuse_m5 = atoi(f) != 0;
   if (p.action == CPSB_WILSON) kappa = 1.0 / (2.0 * (p.mass + 4.0));
   if (p.action == CPSB_DWF) kappa = 1.0 / (2 * (4 + p.a5_inv - p.m5));
   if (mobius_like()) {
@@ -395,6 +397,28 @@ void Operator::hop(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, d
   CK(launch_dslash(prec, A, x != nullptr, red != nullptr, v, st));
 }
 
+bool Operator::hop_m5(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, double a, const M5Coef &cf,
+                      const SpinorPtr *x, const Reduce *red, const int *skip, cudaStream_t st) {
+  if (!fuse_m5 || p.action != CPSB_MOBIUS) return false;
+  DslashArgs A;
+  memset(&A, 0, sizeof(A));
+  A.g = geom;
+  A.U = G->ptr(prec);
+  A.in = in;
+  A.out = out;
+  if (x) A.x = *x;
+  A.cb = cb;
+  A.dag = dag;
+  A.a = a;
+  A.bc_t_sign = (prec != P64 && G->bc_t) ? -1.0 : 1.0;
+  if (red) A.red = *red;
+  A.skip = skip;
+  const cudaError_t e = launch_hop_m5(prec, A, cf, x != nullptr, red != nullptr, st);
+  if (e == cudaErrorNotSupported) return false;
+  CK(e);
+  return true;
+}
+
 void Operator::dslash(const SpinorPtr &out, const SpinorPtr &in, int cb, int dag, cudaStream_t st) {
   if (p.action == CPSB_ZMOBIUS)
     throw Error{CPSB_ERR_UNSUPPORTED,
@@ -447,12 +471,21 @@ void Operator::matpc(const SpinorPtr &out, const SpinorPtr &in, int dag, const R
     matpc_orig_sym1(out, in, dag, red, skip, st);
     return;
   }
+  // Each hop that an M5 operation follows runs with it fused in where a fused
+  // form exists (hop_m5: the M5 output scale folded into the hop's).
   if (!dag) {
     CK(launch_m5(prec, 0, geom, t1.ptr(), in, SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
+    if (hop_m5(t3.ptr(), t1.ptr(), 1, 0, kappa_b * m5c[0].scale, m5c[0], nullptr, nullptr, skip, st)) {
+      hop(out, t3.ptr(), 0, 0, -kappa_b, &in, red, skip, st);
+      return;
+    }
     hop(t3.ptr(), t1.ptr(), 1, 0, kappa_b, nullptr, nullptr, skip, st);
     CK(launch_m5(prec, 0, geom, t1.ptr(), t3.ptr(), SpinorPtr{}, m5c[0], 0, 0, none, skip, st));
     hop(out, t1.ptr(), 0, 0, -kappa_b, &in, red, skip, st);
   } else {
+    if (hop_m5(t3.ptr(), in, 1, 1, -kappa_b * kappa_b, m5c[1], nullptr, nullptr, skip, st) &&
+        hop_m5(out, t3.ptr(), 0, 1, m5c[1].scale, m5c[1], &in, red, skip, st))
+      return;
     hop(t1.ptr(), in, 1, 1, -kappa_b, nullptr, nullptr, skip, st);
     M5Coef c = m5c[1];
     c.scale = kappa_b;
@@ -663,7 +696,7 @@ void Operator::mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const 
 }
 
 void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip,
-                          CgState *S, const SpinorPtr &r, const Reduce *red_r, cudaStream_t st) {
+                          CgState *S, const SpinorPtr &r, const Reduce *red_r, bool shifted, cudaStream_t st) {
   if (!can_fuse_cg_r()) throw Error{CPSB_ERR_UNSUPPORTED, "fused residual update needs the Wilson or DWF operator"};
   matpc(t2.ptr(), in, 0, red_d, skip, st);  // |MatPc p|^2 -> d
   hop(t1.ptr(), t2.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
@@ -690,6 +723,7 @@ void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const R
   A.cg = S;
   A.cg_r = r;
   A.cg_p = in;
+  A.cg_shift = shifted ? 1 : 0;
   CK(launch_dslash(prec, A, 1, 1, v, st));
 }
 

@@ -42,6 +42,9 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
     rS.create(sloppy, n);
     pS.create(sloppy, n);
     ApS.create(sloppy, n);
+    // the iterates' sum since the last reliable update, in FP32 for FP32 and
+    // 16-bit solves: a 16-bit sum's rounding noise, amplified by the condition
+    // number in the true residual, stalls ill-conditioned solves (DWF m_f 0.01)
     xS.create(P32, n);
   } else {
     rS.create(P64, n);  // r, p, Ap of the FP64 recurrence
@@ -73,7 +76,7 @@ static Scal2 sc2(int n, double a, double b) {
 void CgSolver::launch_batch(int k, cudaStream_t st) {
   CgState *S = (CgState *)state.p;
   Operator &op = opS ? *opS : *op64;
-  const int px = opS ? P32 : P64;
+  const int px = opS ? xS.prec : P64;
   Field &xx = opS ? xS : x64;
   Reduce rd = red_d.r(S->d);
   Reduce rr = red_r.r(nullptr);
@@ -82,7 +85,7 @@ void CgSolver::launch_batch(int k, cudaStream_t st) {
   for (int j = 0; j < k; j++) {
     if (fused) {
       // the residual update rides on the last hop of MatPcDagMatPc (A p stays in registers)
-      op.mdagm_cg_r(ApS.ptr(), pS.ptr(), &rd, S->halt, S, rS.ptr(), &rr, st);
+      op.mdagm_cg_r(ApS.ptr(), pS.ptr(), &rd, S->halt, S, rS.ptr(), &rr, shift != 0.0, st);
     } else {
       op.mdagm(ApS, pS, &rd, S->halt, st);
       CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), pS.ptr(), S, rr, st));
@@ -92,7 +95,10 @@ void CgSolver::launch_batch(int k, cudaStream_t st) {
 }
 
 void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool any) {
-  if (!graph || graph_batch != batch) {
+  // the captured iterations depend on whether the solve is shifted (the fused
+  // residual update then also reads p)
+  const bool shifted = shift != 0.0;
+  if (!graph || graph_batch != batch || graph_shifted != shifted) {
     if (graph) {
       cudaGraphExecDestroy(graph);
       graph = nullptr;
@@ -122,6 +128,7 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
     CK(cudaGraphInstantiate(&graph, g, 0));
     cudaGraphDestroy(g);
     graph_batch = batch;
+    graph_shifted = shifted;
   }
   for (;;) {
     CK(cudaGraphLaunch(graph, st));
@@ -168,7 +175,9 @@ void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t s
     if (!(skip_h && skip_h[q])) rr_out[q] = rr[q];
 }
 
-int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma) {
+int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma,
+                    const double *stop_q) {
+  auto stop = [&](int q) { return stop_q ? stop_q[q] : a.stop_rsd; };
   auto t0 = std::chrono::steady_clock::now();
   shift = sigma;
   const Geom &gg = geom;
@@ -195,7 +204,7 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   for (int q = 0; q < nrhs; q++) {
     hs.rr[q] = rr[q];
     hs.pp[q] = rr[q];  // p = r
-    hs.stp[q] = bnorm[q] * a.stop_rsd * a.stop_rsd;
+    hs.stp[q] = bnorm[q] * stop(q) * stop(q);
     hs.maxr[q] = sqrt(rr[q]);
     done[q] = (rr[q] <= hs.stp[q]) || (a.max_num_iter - 1 <= 0);
     hs.halt[q] = hs.halt_done[q] = done[q] ? 1 : 0;
@@ -209,6 +218,7 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   if (opS) {
     CK(launch_convert(sloppy, rS.ptr(), P64, r64.ptr(), gg.nsites, st));
     CK(cudaMemsetAsync(xS.data.p, 0, xS.data.bytes, st));
+    if (xS.norm.p) CK(cudaMemsetAsync(xS.norm.p, 0, xS.norm.bytes, st));  // quantum 0: every value 0
   } else {
     CK(cudaMemcpyAsync(rS.data.p, r64.data.p, r64.data.bytes, cudaMemcpyDeviceToDevice, st));
   }
@@ -245,8 +255,9 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
     CK(cudaMemcpyAsync(dskip, skip_h, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, st));
     Reduce none;
     memset(&none, 0, sizeof(none));
-    CK(launch_axpby(P64, x64.ptr(), P64, x64.ptr(), P32, xS.ptr(), gg, sc2(nrhs, 1.0, 1.0), dskip, none, 0, st));
-    CK(launch_axpby(P32, xS.ptr(), P32, xS.ptr(), P32, SpinorPtr{}, gg, sc2(nrhs, 0.0, 0.0), dskip, none, 0, st));
+    CK(launch_axpby(P64, x64.ptr(), P64, x64.ptr(), xS.prec, xS.ptr(), gg, sc2(nrhs, 1.0, 1.0), dskip, none, 0, st));
+    CK(launch_axpby(xS.prec, xS.ptr(), xS.prec, xS.ptr(), xS.prec, SpinorPtr{}, gg, sc2(nrhs, 0.0, 0.0), dskip, none, 0,
+                    st));
     // only the right-hand sides that paused need their FP64 residual
     true_residual(rr, bnorm, st, skip_h, dskip);
     Scal2 beta = sc2(nrhs, 1.0, 0.0);
@@ -306,8 +317,8 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
     res[q].seconds = secs;
     int stq = CPSB_OK;
     if (h.reason[q] == HALT_BREAKDOWN) stq = CPSB_ERR_BREAKDOWN;
-    else if (!(rr[q] <= bnorm[q] * a.stop_rsd * a.stop_rsd) && h.reason[q] != HALT_CONVERGED) stq = CPSB_NOT_CONVERGED;
-    else if (opS && !(rr[q] <= bnorm[q] * a.stop_rsd * a.stop_rsd)) stq = CPSB_NOT_CONVERGED;
+    else if (!(rr[q] <= bnorm[q] * stop(q) * stop(q)) && h.reason[q] != HALT_CONVERGED) stq = CPSB_NOT_CONVERGED;
+    else if (opS && !(rr[q] <= bnorm[q] * stop(q) * stop(q))) stq = CPSB_NOT_CONVERGED;
     res[q].status = stq;
     if (stq == CPSB_ERR_BREAKDOWN) status = stq;
     else if (stq == CPSB_NOT_CONVERGED && status == CPSB_OK) status = stq;

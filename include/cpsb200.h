@@ -244,6 +244,27 @@ int cpsb_mdagm_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, int precision
 int cpsb_minvcg_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, double *const *x,
                     const double *b, const double *shift, int nshift, double *rsd, int type, const double *alpha,
                     cpsb_solve_result *res, void *stream);
+/* Batched DiracOp::MInvCG: nvec source vectors with the same shifts solved
+ * together -- the pseudofermions of one RHMC force or action evaluation, which
+ * CPS solves one Lattice::FmatEvlMInv call after another
+ * (alg/alg_int/alg_action_rational.C:259-359; minvcg.C:47-353 per call).  Every
+ * vector keeps its own recurrences, convergence flags and reported residuals,
+ * exactly as its own cpsb_minvcg call would; each MatPcDagMatPc is one launch
+ * for all vectors that are still iterating, and with a->precision != F64 each
+ * shift's refinement is one multi-right-hand-side mixed CG over the vectors.
+ * b[q]: the nvec sources.  x[q * nsol + s] (nsol = nshift for CPSB_MULTI, 1 for
+ * CPSB_SINGLE): the solutions.  rsd[q * nshift + s]: stop_rsd of shift s for
+ * vector q on entry, its reported residual on return.  res[q]: the report of
+ * vector q.  nvec <= 16.  Device memory: (nshift + 3) Krylov vectors and nsol
+ * solutions per source vector, plus the FP64 inputs and outputs. */
+int cpsb_minvcg_multi(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nvec, double **x,
+                      const double *const *b, const double *shift, int nshift, double *rsd, int type,
+                      const double *alpha, cpsb_solve_result *res);
+/* The same with device vectors: b holds the nvec sources consecutively; x is a
+ * host array of device pointers, indexed as above. */
+int cpsb_minvcg_multi_dev(cpsb_gauge h, const cpsb_dirac_params *p, const cpsb_cg_arg *a, int nvec,
+                          double *const *x, const double *b, const double *shift, int nshift, double *rsd, int type,
+                          const double *alpha, cpsb_solve_result *res, void *stream);
 
 /* Dslash and MatPcDagMatPc evaluated with fields and links stored in the
  * given precision (CPSB_PREC_F32: FP32 spinors, recon-12 FP32 links;

@@ -1,0 +1,88 @@
+"""Batched multishift CG over several source vectors (cpsb_minvcg_multi).
+
+The pseudofermions of one RHMC evaluation share the shifts of their rational
+approximation (alg_action_rational.C:259-359 calls FmatEvlMInv once per
+pseudofermion); cpsb_minvcg_multi solves them together.  Every vector must get
+what its own cpsb_minvcg call returns:
+
+* FP64 Krylov, DWF 4^4 x Ls 4 and Mobius 4^4 x Ls 4 fixtures' lattices, three
+  vectors (the fixture's source, a second seeded source, and a source of zeros):
+  iteration counts within 1 of the one-vector solve, solutions within 1e-10
+  relative (the fused norms of the multi-vector MatPcDagMatPc sum their partials
+  over a different grid, so the recurrences agree to rounding, not bit for
+  bit), the reported residuals within 1e-6 relative, the zero source returns
+  zeros with the one-vector call's status;
+* FP32 and 16-bit Krylov with per-shift refinement, with a different tolerance
+  per vector and shift: every solution meets its own tolerance in the FP64 true
+  residual |chi - (A + shift) x| / |chi| computed here with the C oracle;
+* SINGLE: each vector's output is its alpha-weighted sum of the MULTI
+  solutions.
+"""
+import numpy as np
+import pytest
+
+from tests.golden_util import load, rel
+
+pytestmark = pytest.mark.gpu
+
+SHIFTS = [0.0, 0.01, 0.1, 0.5]
+
+
+def _setup(name, action):
+    import cps_public_b200 as cb
+    from cps_public_b200 import fields
+    from oracle import oracle
+    cb.init(0)
+    rec, u, src = load(name)
+    dims = tuple(int(d) for d in rec["dims"])
+    kw = dict(mass=float(rec["mass"]), ls=int(rec["ls"]))
+    for k in ("m5", "b", "c"):
+        if k in rec:
+            kw[k] = float(rec[k])
+    g = cb.Gauge(u, dims)
+    op = cb.DiracOp(g, action, **kw)
+    ref = oracle.Op(action, dims, u, **kw)
+    srcs = [src, fields.random_source(len(src) // 24, 77), np.zeros_like(src)]
+    return cb, op, ref, srcs
+
+
+@pytest.mark.parametrize("name,action", [("dwf_4x4x4x4_ls4", "dwf"), ("mobius_4x4x4x4_ls4", "mobius")])
+def test_multi_fp64_matches_one_vector_calls(name, action):
+    cb, op, ref, srcs = _setup(name, action)
+    xs, res, rs = op.MInvCGMulti(srcs, SHIFTS, [1e-10] * 4)
+    for q, src in enumerate(srcs):
+        x1, r1, rs1 = op.MInvCG(src, SHIFTS, [1e-10] * 4)
+        assert res[q].status == r1.status, (q, res[q].status, r1.status)
+        if not np.any(src):
+            assert all(not np.any(x) for x in xs[q])
+            continue
+        assert abs(res[q].iters - r1.iters) <= 1, (q, res[q].iters, r1.iters)
+        for s in range(4):
+            assert rel(xs[q][s], x1[s]) < 1e-10, (q, s)
+        np.testing.assert_allclose(rs[q], rs1, rtol=1e-6)
+
+
+@pytest.mark.parametrize("prec", ["F32", "F16"])
+def test_multi_reduced_precision_meets_each_tolerance(prec):
+    cb, op, ref, srcs = _setup("dwf_4x4x4x4_ls4", "dwf")
+    srcs = srcs[:2]
+    tol = np.array([[1e-10, 1e-9, 1e-10, 1e-8], [1e-8, 1e-10, 1e-9, 1e-10]])
+    xs, res, rs = op.MInvCGMulti(srcs, SHIFTS, tol, precision=getattr(cb, prec))
+    for q, src in enumerate(srcs):
+        assert res[q].status == 0, (q, res[q].as_dict())
+        for s, sh in enumerate(SHIFTS):
+            ax, _ = ref.mdagm(xs[q][s])
+            true = np.linalg.norm(src - ax - sh * xs[q][s]) / np.linalg.norm(src)
+            assert true <= tol[q, s] * 1.01, (q, s, true, tol[q, s])
+            assert rs[q, s] <= tol[q, s] * 1.01
+
+
+def test_multi_single_is_alpha_weighted_sum():
+    cb, op, ref, srcs = _setup("dwf_4x4x4x4_ls4", "dwf")
+    srcs = srcs[:2]
+    alpha = [0.3, -1.2, 2.0, 0.7]
+    xm, _, _ = op.MInvCGMulti(srcs, SHIFTS, [1e-10] * 4)
+    xsg, res, _ = op.MInvCGMulti(srcs, SHIFTS, [1e-10] * 4, ms_type=cb.SINGLE, alpha=alpha)
+    for q in range(2):
+        want = sum(a * x for a, x in zip(alpha, xm[q]))
+        assert rel(xsg[q][0], want) < 1e-10
