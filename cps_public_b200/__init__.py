@@ -248,7 +248,7 @@ class DiracOp:
         xp = (_lib._dp * (nvec * nsol))(*[ptr(x) for row in xs for x in row])
         bs = [self._v(b) for b in srcs]
         bp = (_lib._dp * nvec)(*[ptr(b) for b in bs])
-        rs = np.array(np.broadcast_to(np.asarray(rsd, np.float64), (nvec, ns)))
+        rs = np.ascontiguousarray(np.broadcast_to(np.asarray(rsd, np.float64), (nvec, ns)), np.float64)
         sh = np.array(shifts, np.float64)
         al = np.ones(ns) if alpha is None else np.array(alpha, np.float64)
         a = CgArg(float(np.min(rs)), max_num_iter, precision, 0.1, 0)

@@ -285,15 +285,17 @@ __global__ void __launch_bounds__(NT) cg_xp_update_kernel(Geom g, SpinorPtr x, S
     for (long j = (long)blockIdx.x * NT + threadIdx.x; j < per; j += (long)gridDim.x * NT) {
       const long i = rhs * per + j;
       Spinor<T> pv = load_spinor<P>(p, i);
-      Spinor<TX> xv = load_spinor<PX>(x, i);
+      if (x.data) {  // x == null: the residual-update hop has made this update
+        Spinor<TX> xv = load_spinor<PX>(x, i);
 #pragma unroll
-      for (int s = 0; s < 4; s++)
+        for (int s = 0; s < 4; s++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          xv.c[s][c].re = (TX)(alpha * (double)pv.c[s][c].re) + xv.c[s][c].re;
-          xv.c[s][c].im = (TX)(alpha * (double)pv.c[s][c].im) + xv.c[s][c].im;
-        }
-      store_spinor<PX>(x, i, xv);
+          for (int c = 0; c < 3; c++) {
+            xv.c[s][c].re = (TX)(alpha * (double)pv.c[s][c].re) + xv.c[s][c].re;
+            xv.c[s][c].im = (TX)(alpha * (double)pv.c[s][c].im) + xv.c[s][c].im;
+          }
+        store_spinor<PX>(x, i, xv);
+      }
       if (upd_p) {
         Spinor<T> rv = load_spinor<P>(r, i);
         const T b = (T)beta;

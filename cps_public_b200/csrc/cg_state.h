@@ -32,3 +32,19 @@ struct CgState {
 };
 
 }  // namespace cpsb
+
+namespace cpsb {
+
+// Control block of a device-side loop over batches of iterations (the body of a
+// CUDA-graph WHILE node, graph_loop.cu).  Before each launch the host sets
+// count = 0, cap and done[]; the condition kernel that ends every batch counts
+// it and ends the loop once every right-hand side has halted, or (when the
+// host has per-RHS work, `any`) one that is not in done[] has halted, or cap
+// batches have run.
+struct LoopCtl {
+  unsigned count;
+  unsigned cap;
+  int done[MAX_RHS];
+};
+
+}  // namespace cpsb

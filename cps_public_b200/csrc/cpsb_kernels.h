@@ -36,6 +36,7 @@ struct DslashArgs {
   // advances the recurrence scalars as the r-update kernel of blas.cu does.
   CgState *cg;
   SpinorPtr cg_r, cg_p;
+  SpinorPtr cg_x;         // when set: also x += alpha p (x FP64 for FP64 storage, else FP32)
   int cg_shift;           // nonzero: the solve's shift is nonzero (the update reads p)
 };
 

@@ -46,7 +46,8 @@
 // Epilogues (no extra pass over memory): out = x + a*D in (XPAY) or a*D in,
 // optionally |out|^2 per right-hand side (NORM), or the CG residual update
 // r -= alpha (D-output + sigma p) with |r|^2 and the recurrence scalars (CGR),
-// where the D output is consumed in registers and not stored.  Reductions are
+// where the D output is consumed in registers and not stored, together with
+// the solution update x += alpha p when A.cg_x is set.  Reductions are
 // deterministic (partials in block order, summed by the last block).
 #pragma once
 #include <algorithm>
@@ -758,13 +759,24 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         if (CGR) {
           const double alpha = cg_alpha[rhs];
           Spinor<double> rv = unpack64(load_raw<P64>(A.cg_r, i));
-          if (CGR == 2) {
-            const double sigma = A.cg->shift;
+          if (CGR == 2 || A.cg_x.data) {
             const Spinor<double> pv = unpack64(load_raw<P64>(A.cg_p, i));
+            if (CGR == 2) {
+              const double sigma = A.cg->shift;
 #pragma unroll
-            for (int s2 = 0; s2 < 4; s2++)
+              for (int s2 = 0; s2 < 4; s2++)
 #pragma unroll
-              for (int r = 0; r < 3; r++) acc.c[s2][r] = acc.c[s2][r] + cscale(sigma, pv.c[s2][r]);
+                for (int r = 0; r < 3; r++) acc.c[s2][r] = acc.c[s2][r] + cscale(sigma, pv.c[s2][r]);
+            }
+            if (A.cg_x.data) {
+              // x += alpha p (the solution half of cg_xp_update, blas.cu)
+              Spinor<double> xv = unpack64(load_raw<P64>(A.cg_x, i));
+#pragma unroll
+              for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) xv.c[s2][r] = cscale(alpha, pv.c[s2][r]) + xv.c[s2][r];
+              store_spinor<P64>(A.cg_x, i, xv);
+            }
           }
 #pragma unroll
           for (int s2 = 0; s2 < 4; s2++)
@@ -812,9 +824,21 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           float pn = 0.f;
           SpX2 pv;
           double sigma = 0.0;
-          if (CGR == 2) {
-            sigma = A.cg->shift;
-            pv = unpack(load_raw<P>(A.cg_p, i), &pn);
+          if (CGR == 2 || A.cg_x.data) pv = unpack(load_raw<P>(A.cg_p, i), &pn);
+          if (CGR == 2) sigma = A.cg->shift;
+          if (A.cg_x.data) {
+            // x += alpha p in FP32 (the solution half of cg_xp_update, blas.cu)
+            float xn;
+            SpX2 xv = unpack(load_raw<P32>(A.cg_x, i), &xn);
+            const float2 ap = f2b(alpha * pn);
+#pragma unroll
+            for (int p = 0; p < 2; p++)
+#pragma unroll
+              for (int cc = 0; cc < 3; cc++) {
+                xv.re[p][cc] = fma2(ap, pv.re[p][cc], xv.re[p][cc]);
+                xv.im[p][cc] = fma2(ap, pv.im[p][cc], xv.im[p][cc]);
+              }
+            store_x2<P32>(A.cg_x, i, xv);
           }
           const float2 ma = f2b(-alpha), rs = f2b(rn), ps = f2b((float)sigma * pn);
 #pragma unroll

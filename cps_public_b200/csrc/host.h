@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <complex>
+#include <functional>
 
 #include <map>
 #include <memory>
@@ -147,14 +148,15 @@ struct Operator {
   }
   // MatPcDagMatPc p with the CG residual update fused into its last hop
   // (Wilson / DWF, every precision): |MatPc p|^2 -> red_d, then
-  // r -= alpha (A p + shift p), |r|^2 and the recurrence scalars in S; A p is
-  // not stored (scratch receives it only while a launch shape is being tuned).
+  // r -= alpha (A p + shift p), |r|^2 and the recurrence scalars in S, and with
+  // x given x += alpha p; A p is not stored (scratch receives it only while a
+  // launch shape is being tuned).
   bool can_fuse_cg_r() const { return p.action == CPSB_WILSON || p.action == CPSB_DWF; }
   bool mobius_like() const { return p.action == CPSB_MOBIUS || p.action == CPSB_ZMOBIUS; }
   void matpc_zmobius(const SpinorPtr &out, const SpinorPtr &in, int dag, const Reduce *red, const int *skip,
                      cudaStream_t st);
   void mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip, CgState *S,
-                  const SpinorPtr &r, const Reduce *red_r, bool shifted, cudaStream_t st);
+                  const SpinorPtr &r, const Reduce *red_r, bool shifted, const SpinorPtr *x, cudaStream_t st);
   // Mobius pieces of DiracOpMobius::MatInv (SYM2): out = M5^-1 in
   // (zmobius_m5inv, dag 0); out = D4(cb) in (zmobius_dslash_4, dag 0);
   // out = x + f H5 in (zmobius_kappa_dslash_5_plus_cmplx with factor f, dag 0).
@@ -180,12 +182,16 @@ struct CgSolver {
   DevBuf state;                       // CgState
   CgState *hstate = nullptr;          // pinned mirror
   DevBuf scal;                        // misc per-RHS scalars
+  double *hscal = nullptr;            // pinned: |b|^2 read back without its own synchronisation
   RedSlot red_d, red_r, red_p, red_misc;
   double shift = 0;                   // sigma of the solve in progress
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;
   bool graph_shifted = false;
-  unsigned long long graph_nodes = 0;
+  bool graph_loop = false;            // the graph is a device-side loop of batches
+  unsigned long long graph_nodes = 0;  // kernels per batch (per loop body)
+  DevBuf loop;                        // LoopCtl
+  LoopCtl *hloop = nullptr;           // pinned: [0] to the device, [1] read back
   std::mutex busy;
 
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
@@ -203,6 +209,20 @@ struct CgSolver {
 };
 
 int tuned_variant(const DslashArgs &A, int prec, int xpay, int norm, cudaStream_t st);
+
+// Device-side iteration loops (graph_loop.cu): record(h) records one batch
+// followed by a condition kernel for handle h into the body of a graph WHILE
+// node; returns false where the driver has no conditional nodes (the caller
+// then replays plain batches).  CPSB_GRAPH_LOOP=0 in the environment turns the
+// loops off.
+bool graph_loops_enabled();
+bool build_loop_graph(cudaStream_t st, const std::function<void(cudaGraphConditionalHandle)> &record,
+                      cudaGraphExec_t *exec, size_t *body_nodes);
+cudaError_t launch_cg_loop_cond(cudaGraphConditionalHandle h, const CgState *S, LoopCtl *L, int nrhs, int any,
+                                cudaStream_t st);
+struct MsBatch;
+cudaError_t launch_ms_loop_cond(cudaGraphConditionalHandle h, const MsBatch *B, LoopCtl *L, int nvec,
+                                cudaStream_t st);
 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
 

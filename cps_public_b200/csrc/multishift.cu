@@ -365,37 +365,62 @@ int multishift_multi(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a,
     const int *skip = B->done_applied;
     op.mdagm(Ap, pv[0], &rd, skip, st);  // uncaptured application: tunes the launch shapes
     CK(cudaMemcpyAsync(state.p, &init, sizeof(MsBatch), cudaMemcpyHostToDevice, st));
-    const int batch = a.batch > 0 ? a.batch : 16;
-    cudaGraph_t graph;
-    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    set_capturing(true);
-    try {
+    const int batch = a.batch > 0 ? a.batch : (graph_loops_enabled() ? 4 : 16);
+    auto record = [&]() {
       for (int j = 0; j < batch; j++) {
         op.mdagm(Ap, pv[0], &rd, skip, st);
         CK(launch_ms_r_update(prec, g, r.ptr(), Ap.ptr(), pv[0].ptr(), B, rr, st));
         CK(launch_ms_xp_update(prec, px, g, r.ptr(), pp_, xx_, B, rp, st));
       }
-    } catch (...) {
-      set_capturing(false);
-      cudaStreamEndCapture(st, &graph);
-      throw;
-    }
-    set_capturing(false);
-    CK(cudaStreamEndCapture(st, &graph));
+    };
+    // one graph launch runs batches on the device until every vector is done
+    // (graph_loop.cu); else the host replays single batches
+    DevBuf loopbuf(sizeof(LoopCtl));
+    LoopCtl *hl = nullptr;
+    CK(cudaMallocHost((void **)&hl, 2 * sizeof(LoopCtl)));
+    struct LoopPin {
+      LoopCtl *p;
+      ~LoopPin() { cudaFreeHost(p); }
+    } loop_pin{hl};
+    cudaGraphExec_t exec = nullptr;
     size_t nn = 0;
-    CK(cudaGraphGetNodes(graph, nullptr, &nn));
-    cudaGraphExec_t exec;
-    CK(cudaGraphInstantiate(&exec, graph, 0));
-    cudaGraphDestroy(graph);
+    const bool as_loop = graph_loops_enabled() &&
+                         build_loop_graph(st, [&](cudaGraphConditionalHandle h) {
+                           record();
+                           CK(launch_ms_loop_cond(h, B, (LoopCtl *)loopbuf.p, nvec, st));
+                         }, &exec, &nn);
+    if (!as_loop) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      set_capturing(true);
+      try {
+        record();
+      } catch (...) {
+        set_capturing(false);
+        cudaStreamEndCapture(st, &graph);
+        throw;
+      }
+      set_capturing(false);
+      CK(cudaStreamEndCapture(st, &graph));
+      CK(cudaGraphGetNodes(graph, nullptr, &nn));
+      CK(cudaGraphInstantiate(&exec, graph, 0));
+      cudaGraphDestroy(graph);
+    }
     struct ExecGuard {
       cudaGraphExec_t e;
       ~ExecGuard() { cudaGraphExecDestroy(e); }
     } exec_guard{exec};
     for (;;) {
+      if (as_loop) {
+        hl[0].count = 0;
+        hl[0].cap = (unsigned)((a.max_num_iter + batch - 1) / batch + 2);
+        CK(cudaMemcpyAsync(loopbuf.p, &hl[0], sizeof(LoopCtl), cudaMemcpyHostToDevice, st));
+      }
       CK(cudaGraphLaunch(exec, st));
-      count_launch(nn);
       CK(cudaMemcpyAsync(hb, state.p, sizeof(MsBatch), cudaMemcpyDeviceToHost, st));
+      if (as_loop) CK(cudaMemcpyAsync(&hl[1], loopbuf.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
+      count_launch(nn * (as_loop ? hl[1].count : 1));
       bool all = true;
       for (int q = 0; q < nvec; q++) all &= hb->done_applied[q] != 0;
       if (all) break;

@@ -696,7 +696,8 @@ void Operator::mobius_hop5_add(const SpinorPtr &out, const SpinorPtr &in, const 
 }
 
 void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const Reduce *red_d, const int *skip,
-                          CgState *S, const SpinorPtr &r, const Reduce *red_r, bool shifted, cudaStream_t st) {
+                          CgState *S, const SpinorPtr &r, const Reduce *red_r, bool shifted, const SpinorPtr *x,
+                          cudaStream_t st) {
   if (!can_fuse_cg_r()) throw Error{CPSB_ERR_UNSUPPORTED, "fused residual update needs the Wilson or DWF operator"};
   matpc(t2.ptr(), in, 0, red_d, skip, st);  // |MatPc p|^2 -> d
   hop(t1.ptr(), t2.ptr(), 1, 1, 1.0, nullptr, nullptr, skip, st);
@@ -724,6 +725,7 @@ void Operator::mdagm_cg_r(const SpinorPtr &scratch, const SpinorPtr &in, const R
   A.cg_r = r;
   A.cg_p = in;
   A.cg_shift = shifted ? 1 : 0;
+  if (x) A.cg_x = *x;
   CK(launch_dslash(prec, A, 1, 1, v, st));
 }
 

@@ -14,7 +14,10 @@
 //
 // Iterations are launched in batches captured as one CUDA graph: every scalar
 // lives in device memory (CgState) and a halting RHS turns the rest of the batch
-// into early exits, so the host only reads the state between batches.
+// into early exits.  The batch is the body of a device-side loop
+// (graph_loop.cu), so one graph launch runs batches until a right-hand side
+// needs the host (convergence, a reliable update, the iteration limit), and
+// the host reads the state only then.
 #include <math.h>
 #include <string.h>
 
@@ -53,6 +56,9 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
   }
   state.alloc(sizeof(CgState));
   CK(cudaMallocHost((void **)&hstate, sizeof(CgState)));
+  loop.alloc(sizeof(LoopCtl));
+  CK(cudaMallocHost((void **)&hloop, 2 * sizeof(LoopCtl)));
+  CK(cudaMallocHost((void **)&hscal, sizeof(double) * MAX_RHS));
   p.zmobius_b = p.zmobius_c = nullptr;  // the operators hold copies of the zMobius coefficients
   scal.alloc(sizeof(double) * MAX_RHS * 8);
 }
@@ -60,6 +66,8 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
 CgSolver::~CgSolver() {
   if (graph) cudaGraphExecDestroy(graph);
   if (hstate) cudaFreeHost(hstate);
+  if (hloop) cudaFreeHost(hloop);
+  if (hscal) cudaFreeHost(hscal);
 }
 
 static Scal2 sc2(int n, double a, double b) {
@@ -85,12 +93,14 @@ void CgSolver::launch_batch(int k, cudaStream_t st) {
   for (int j = 0; j < k; j++) {
     if (fused) {
       // the residual update rides on the last hop of MatPcDagMatPc (A p stays in registers)
-      op.mdagm_cg_r(ApS.ptr(), pS.ptr(), &rd, S->halt, S, rS.ptr(), &rr, shift != 0.0, st);
+      // and so does x += alpha p: the x/p kernel then updates p alone
+      const SpinorPtr xp = xx.ptr();
+      op.mdagm_cg_r(ApS.ptr(), pS.ptr(), &rd, S->halt, S, rS.ptr(), &rr, shift != 0.0, &xp, st);
     } else {
       op.mdagm(ApS, pS, &rd, S->halt, st);
       CK(launch_cg_r_update(op.prec, op.geom, rS.ptr(), ApS.ptr(), pS.ptr(), S, rr, st));
     }
-    CK(launch_cg_xp_update(px, op.prec, op.geom, xx.ptr(), pS.ptr(), rS.ptr(), S, rp, st));
+    CK(launch_cg_xp_update(px, op.prec, op.geom, fused ? SpinorPtr{} : xx.ptr(), pS.ptr(), rS.ptr(), S, rp, st));
   }
 }
 
@@ -110,31 +120,47 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
       Reduce rd = red_d.r(S->d);
       op.mdagm(ApS, pS, &rd, S->halt, st);
     }
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    set_capturing(true);
-    try {
-      launch_batch(batch, st);
-    } catch (...) {
-      set_capturing(false);
-      cudaStreamEndCapture(st, &g);
-      throw;
-    }
-    set_capturing(false);
-    CK(cudaStreamEndCapture(st, &g));
     size_t nn = 0;
-    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    graph_loop = graph_loops_enabled() &&
+                 build_loop_graph(st, [&](cudaGraphConditionalHandle h) {
+                   launch_batch(batch, st);
+                   CK(launch_cg_loop_cond(h, (const CgState *)state.p, (LoopCtl *)loop.p, nrhs, any ? 1 : 0, st));
+                 }, &graph, &nn);
+    if (!graph_loop) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      set_capturing(true);
+      try {
+        launch_batch(batch, st);
+      } catch (...) {
+        set_capturing(false);
+        cudaStreamEndCapture(st, &g);
+        throw;
+      }
+      set_capturing(false);
+      CK(cudaStreamEndCapture(st, &g));
+      CK(cudaGraphGetNodes(g, nullptr, &nn));
+      CK(cudaGraphInstantiate(&graph, g, 0));
+      cudaGraphDestroy(g);
+    }
     graph_nodes = nn;
-    CK(cudaGraphInstantiate(&graph, g, 0));
-    cudaGraphDestroy(g);
     graph_batch = batch;
     graph_shifted = shifted;
   }
   for (;;) {
+    if (graph_loop) {
+      // batches that can still do work, plus one: every launch ends
+      LoopCtl &c = hloop[0];
+      c.count = 0;
+      c.cap = (unsigned)((hstate->max_iter + batch - 1) / batch + 2);
+      for (int q = 0; q < MAX_RHS; q++) c.done[q] = q < nrhs && done[q] ? 1 : 0;
+      CK(cudaMemcpyAsync(loop.p, &c, sizeof(LoopCtl), cudaMemcpyHostToDevice, st));
+    }
     CK(cudaGraphLaunch(graph, st));
-    count_launch(graph_nodes);
     CK(cudaMemcpyAsync(hstate, state.p, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+    if (graph_loop) CK(cudaMemcpyAsync(&hloop[1], loop.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    count_launch(graph_nodes * (graph_loop ? hloop[1].count : 1));
     bool all = true, one = false;
     for (int q = 0; q < nrhs; q++) {
       all = all && hstate->halt_done[q];
@@ -183,15 +209,15 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   const Geom &gg = geom;
   double bnorm[MAX_RHS], rr[MAX_RHS];
   double *dres = (double *)scal.p;
-  // |b|^2
+  // |b|^2, read back by the synchronisation that ends the true residual
   {
-    Reduce rm = red_misc.r(dres);
+    Reduce rm = red_misc.r(dres + 7 * MAX_RHS);
     CK(launch_redot(P64, gg, b64.ptr(), b64.ptr(), rm, st));
-    CK(cudaMemcpyAsync(bnorm, dres, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(hscal, dres + 7 * MAX_RHS, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
   }
   // r = b - A x
   true_residual(rr, bnorm, st);
+  for (int q = 0; q < nrhs; q++) bnorm[q] = hscal[q];
   CgState hs;
   memset(&hs, 0, sizeof(hs));
   const double delta = sloppy == P64 ? 0.0 : (a.reliable_delta > 0 ? a.reliable_delta : 0.1);
@@ -236,6 +262,10 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   // (milliseconds) and a host round trip every couple of iterations costs
   // little, so the batch shrinks as the right-hand sides grow.
   int batch = a.batch > 0 ? a.batch : (nrhs >= 8 ? 2 : nrhs >= 2 ? 4 : 16);
+  // With the device-side loop a batch ends in a (cheap) condition check, not
+  // a host round trip: short batches leave less idle work after a right-hand
+  // side halts.
+  if (a.batch <= 0 && graph_loops_enabled()) batch = nrhs >= 8 ? 1 : nrhs >= 2 ? 2 : 4;
   int status = CPSB_OK;
   for (;;) {
     bool all = true;

@@ -3,6 +3,11 @@
 Times the 5-D Shamir DWF hop (one checkerboard, dag 0) on the 16^3x32, Ls=16
 workload with CUDA events over many launches and reports algorithmic GB/s
 (spinor in + out + links per application) against the measured HBM copy peak.
+
+--op mdagm times MatPcDagMatPc instead (cpsb_mdagm_multi_dev on nrhs device
+vectors, CUDA events over --reps applications), e.g. the Mobius operator with
+its fused hop + M5 kernels:
+  python -m cps_public_b200.dslash_bench --op mdagm --action mobius --prec f16 --nrhs 12
 """
 from __future__ import annotations
 
@@ -26,6 +31,7 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--action", default="dwf")
+    ap.add_argument("--op", default="hop", choices=["hop", "mdagm"])
     a = ap.parse_args()
     dims = tuple(int(x) for x in a.dims.split(","))
     init(0)
@@ -38,6 +44,30 @@ def main():
     except Exception:
         pass
     lib = _lib.load()
+    if a.op == "mdagm":
+        import torch
+        dev = torch.device("cuda", 0)
+        src = fields.random_source(op.n // 24, 11)
+        x = torch.from_numpy(np.tile(src, a.nrhs)).to(dev)
+        y = torch.empty_like(x)
+        for name in a.prec.split(","):
+            def apply():
+                _lib.check(lib.cpsb_mdagm_multi_dev(g.h, C.byref(op.p), PRECS[name], a.nrhs, C.c_void_p(y.data_ptr()),
+                                                    C.c_void_p(x.data_ptr()), None, None), "cpsb_mdagm_multi_dev")
+            for _ in range(3):
+                apply()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(a.reps):
+                apply()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / a.reps
+            print(json.dumps({"op": "mdagm", "action": a.action, "prec": name, "dims": dims, "ls": a.ls,
+                              "nrhs": a.nrhs, "ms_per_application": ms,
+                              "note": "includes packing the FP64 CPS-order vectors in and out"}))
+        return
     for name in a.prec.split(","):
         ms, by = C.c_double(), C.c_double()
         _lib.check(lib.cpsb_bench_dslash(g.h, C.byref(op.p), PRECS[name], a.nrhs, a.reps, C.byref(ms),

@@ -16,6 +16,7 @@
 //     (exactly what Lattice::FmatEvlInv reaches through InvCg(&true_res); the
 //      4-argument InvCg wrapper at inv_cg.C:449-454 has no return statement, so
 //      it is bypassed here)
+//   Lattice::FmatEvlInv                             f_dwf_base.C:189-209, f_mobius.C:582, f_wilson.C:159
 //   Lattice::FmatEvlMInv -> DiracOp::MInvCG         f_dwf_base.C:232-270, minvcg.C:47-353
 //   DiracOp*::MatInv (full-lattice solve)           d_op_wilson.C:257-334, d_op_dwf.C:316-507,
 //                                                   d_op_mobius.C:389-640
@@ -39,7 +40,11 @@
 //        15 fermion order for OP_FCONVERT (0 WILSON, 1 DWF_4D_EOPREC_EE),
 //        16 OP_FCONVERT direction (0 CANONICAL -> order, 1 order -> CANONICAL),
 //        17 OP_MINRESEXT degree (number of previous solutions),
-//        18 OP_FMATINV dminus flag
+//        18 OP_FMATINV dminus flag,
+//        19, 20 (the build with the B200 bridge, -DUSE_B200, only) the bridge's
+//        inner precision of FmatEvlInv / FmatInv and of FmatEvlMInv (-1: its default)
+//   rpar[44] = device kernels the B200 library launched during the request
+//   (-DUSE_B200 builds; 0 otherwise)
 //   rpar[10] = wall seconds spent inside the timed CPS call(s) (MINVCG: rpar[42],
 //   since rpar[0..nshift) holds the per-shift residuals); OP_BENCH also
 //   returns the start and end of that window (steady clock, seconds) in
@@ -65,12 +70,15 @@
 #include <util/error.h>
 #include <alg/do_arg.h>
 #include <alg/cg_arg.h>
+#ifdef USE_B200
+#include <util/b200_bridge.h>
+#endif
 
 USING_NAMESPACE_CPS
 
 enum { OP_DSLASH = 1, OP_MATPC = 2, OP_MDAGM = 3, OP_INVCG = 4, OP_MINVCG = 5,
        OP_M5INV = 6, OP_MOBIUS_D4 = 7, OP_BENCH = 8, OP_MATINV = 9, OP_FCONVERT = 10,
-       OP_MINRESEXT = 11, OP_DMINUS = 12, OP_FMATINV = 13 };
+       OP_MINRESEXT = 11, OP_DMINUS = 12, OP_FMATINV = 13, OP_FMATEVLINV = 14 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -185,6 +193,12 @@ int main(int argc, char **argv) {
   cg_arg.Inverter = CG;
 
   int64_t rhdr[8] = {0}; double rpar[64] = {0};
+#ifdef USE_B200
+  if (hdr[19] >= 0 || hdr[20] >= 0)
+    b200_set_precision(hdr[19] >= 0 ? (int)hdr[19] : CPSB_PREC_F16, hdr[20] >= 0 ? (int)hdr[20] : CPSB_PREC_F32);
+  unsigned long long launches0 = 0, launches1 = 0;
+  cpsb_kernel_launches(&launches0);
+#endif
   std::vector<double> out_payload;
 
   Vector *in = (Vector *)smalloc(fsz * sizeof(double));
@@ -256,6 +270,16 @@ int main(int argc, char **argv) {
     rpar[10] = now_s() - t0;
     delete d;
     rhdr[0] = iters; rpar[0] = true_res;
+    out_payload.assign((double *)out, (double *)out + fsz);
+  } else if (op == OP_FMATEVLINV) {
+    // Lattice::FmatEvlInv (the entry point CPS's algorithms call), source and guess in
+    read_all(fi, in, fsz * sizeof(double));
+    read_all(fi, out, fsz * sizeof(double));
+    Float true_res = 0;
+    double t0 = now_s();
+    rhdr[0] = lat.FmatEvlInv(out, in, &cg_arg, &true_res, CNV_FRM_NO);
+    rpar[10] = now_s() - t0;
+    rpar[0] = true_res;
     out_payload.assign((double *)out, (double *)out + fsz);
   } else if (op == OP_MINVCG) {
     read_all(fi, in, fsz * sizeof(double));
@@ -385,6 +409,10 @@ int main(int argc, char **argv) {
     die("unknown op");
   }
   fclose(fi);
+#ifdef USE_B200
+  cpsb_kernel_launches(&launches1);
+  rpar[44] = (double)(launches1 - launches0);
+#endif
   FILE *fo = fopen(argv[2], "wb");
   if (!fo) die("cannot open response");
   write_all(fo, rhdr, sizeof rhdr);

@@ -14,23 +14,27 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CPSREF = os.path.join(HERE, "_ref", "cpsref")
+# CPS built with the B200 bridge linked in (oracle/build_dropin.py)
+CPSREF_B200 = os.path.join(HERE, "_ref", "cpsref_b200")
 
 OP_DSLASH, OP_MATPC, OP_MDAGM, OP_INVCG, OP_MINVCG, OP_M5INV, OP_MOBIUS_D4, OP_BENCH, OP_MATINV, OP_FCONVERT, \
-    OP_MINRESEXT, OP_DMINUS, OP_FMATINV = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13
+    OP_MINRESEXT, OP_DMINUS, OP_FMATINV, OP_FMATEVLINV = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14
 ACTIONS = {"wilson": 0, "dwf": 1, "mobius": 2, "zmobius": 3}
 
 
-def available() -> bool:
-    return os.access(CPSREF, os.X_OK)
+def available(binary=CPSREF) -> bool:
+    return os.access(binary, os.X_OK)
 
 
 def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8, a5_inv=1.0,
         b=1.5, c=0.5, stop_rsd=1e-10, max_iter=5000, shifts=(), ms_type=0, pc_type=2,
-        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0, dminus=0, zb=None, zc=None):
+        bc_t=0, extra=(), reps=0, threads=None, timeout=3600, order=0, direction=0, degree=0, dminus=0, zb=None, zc=None, binary=CPSREF, bridge_prec=(-1, -1)):
     """Run one reference operation; returns (iters, rpar[64], payload array).
-    zMobius (action "zmobius") takes the complex per-slice coefficients zb, zc (ls each)."""
-    if not available():
-        raise RuntimeError("reference oracle not built (run oracle/build_ref.sh)")
+    zMobius (action "zmobius") takes the complex per-slice coefficients zb, zc (ls each).
+    binary: CPSREF, or CPSREF_B200 with bridge_prec the bridge's inner precisions
+    (FmatEvlInv / FmatInv, FmatEvlMInv; -1 keeps its default)."""
+    if not available(binary):
+        raise RuntimeError(f"{os.path.basename(binary)} not built (oracle/build_ref.sh, oracle/build_dropin.py)")
     hdr = np.zeros(32, np.int64)
     par = np.zeros(32, np.float64)
     hdr[0] = op
@@ -49,6 +53,7 @@ def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8
     hdr[16] = direction
     hdr[17] = degree
     hdr[18] = dminus
+    hdr[19], hdr[20] = bridge_prec
     par[0] = mass
     par[1] = m5
     par[2] = a5_inv
@@ -76,7 +81,7 @@ def run(op, action, dims, gauge, vectors=(), ls=1, cb=0, dag=0, mass=0.1, m5=1.8
                 f.write(np.ascontiguousarray(v, np.float64).tobytes())
             for v in extra:
                 f.write(np.ascontiguousarray(v, np.float64).tobytes())
-        p = subprocess.run([CPSREF, req, rsp], capture_output=True, text=True, env=env,
+        p = subprocess.run([binary, req, rsp], capture_output=True, text=True, env=env,
                            timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError(f"cpsref failed ({p.returncode}): {p.stderr[-2000:]}")

@@ -1,91 +1,79 @@
 """The CPS-side binding shown in INTEGRATION.md compiles against CPS's own
-headers: the bridge header and source as written there, and each USE_B200
-branch inside a member function of the CPS class it belongs to (FdwfBase for
-the lattice entry points, DiracOpDwf for the operator one), with CPS's
-parameter names.  Skipped where the reference tree is not present."""
+sources: the bridge header and source as written there, CPS's f_dwf_base.C,
+f_mobius.C and f_wilson.C with the USE_B200 branch blocks inserted at the top
+of the functions each block names (the patching oracle/build_dropin.py does for
+the linked build), and the operator-level branch inside a DiracOpDwf member.
+Every block must be used: each branch block names at least one function, and
+every named function is found on the line the block cites.  Skipped where the
+reference tree is not present."""
 import os
-import re
 import shutil
 import subprocess
 
 import pytest
 
+from oracle import build_dropin
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def reference_include():
+def reference():
     from __graft_entry__ import REFERENCE
-    inc = os.path.join(REFERENCE, "include")
-    if not os.path.isdir(inc):
+    if not os.path.isdir(os.path.join(REFERENCE, "include")):
         pytest.skip("reference tree not present")
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    return inc
+    return REFERENCE
 
 
-def cpp_blocks():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    return re.findall(r"```cpp\n(.*?)```", text, re.S)
-
-
-def compile_ok(tmp_path, name, source, extra_inc):
+def syntax_ok(tmp_path, name, source, ref):
     path = tmp_path / name
     path.write_text(source)
-    cmd = ["g++", "-std=gnu++11", "-fsyntax-only", "-w", "-DUSE_B200", f"-I{tmp_path / 'include'}",
-           f"-I{os.path.join(ROOT, 'oracle', 'ref_config')}", f"-I{extra_inc}", f"-I{os.path.join(ROOT, 'include')}",
-           str(path)]
+    cmd = ["g++", "-x", "c++", "-std=gnu++11", "-fsyntax-only", "-w", "-DUSE_B200", f"-I{tmp_path / 'include'}",
+           f"-I{os.path.join(ROOT, 'include')}", f"-I{os.path.join(ROOT, 'oracle', 'ref_config')}",
+           f"-I{os.path.join(ref, 'include')}", str(path)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
 
 
 @pytest.fixture
 def bridge(tmp_path):
-    inc = reference_include()
-    blocks = cpp_blocks()
-    hdr = [b for b in blocks if b.startswith("// include/util/b200_bridge.h")]
-    assert len(hdr) == 1
+    ref = reference()
+    blocks = build_dropin.cpp_blocks(open(os.path.join(ROOT, "INTEGRATION.md")).read())
+    hdr, src = build_dropin.bridge_sources(blocks)
     (tmp_path / "include" / "util").mkdir(parents=True)
-    (tmp_path / "include" / "util" / "b200_bridge.h").write_text("#pragma once\n" + hdr[0])
-    return tmp_path, inc, blocks
+    (tmp_path / "include" / "util" / "b200_bridge.h").write_text(hdr)
+    return tmp_path, ref, blocks, src
 
 
 def test_bridge_source_compiles(bridge):
-    tmp_path, inc, blocks = bridge
-    src = [b for b in blocks if b.startswith("// util/dirac_op/b200_bridge.C")]
-    assert len(src) == 1
-    compile_ok(tmp_path, "b200_bridge.C", src[0], inc)
+    tmp_path, ref, blocks, src = bridge
+    syntax_ok(tmp_path, "b200_bridge.C", src, ref)
 
 
-def test_branches_compile_in_their_cps_classes(bridge):
-    tmp_path, inc, blocks = bridge
-    frags = [m.group(1) for b in blocks for m in re.finditer(r"#ifdef USE_B200\n(.*?)#endif", b, re.S)]
-    inv = [f for f in frags if "b200_fmat_evl_inv" in f]
-    minv = [f for f in frags if "b200_fmat_evl_minv" in f]
-    matinv = [f for f in frags if "cpsb_matinv" in f]
+def test_branches_compile_in_the_cps_files(bridge):
+    tmp_path, ref, blocks, _ = bridge
+    branches = build_dropin.branch_blocks(blocks)
+    calls = {"b200_fmat_evl_inv", "b200_fmat_evl_minv", "b200_fmat_inv"}
+    assert calls == {c for _, body in branches for c in calls if c in body}
+    named = {(c, f) for targets, _ in branches for c, f, _ in targets}
+    assert len(named) == 9, named   # FmatEvlInv, FmatEvlMInv, FmatInv of three lattice classes
+    for rel, cls in build_dropin.FILES.items():
+        path = os.path.join(ref, "src", "util", "lattice", rel)
+        patched = build_dropin.patch(open(path).read(), path, cls, branches)
+        assert patched.count("#ifdef USE_B200") == 1 + sum(1 for t, _ in branches for c, _, _ in t if c == cls)
+        syntax_ok(tmp_path, os.path.basename(rel), patched, ref)
+
+
+def test_operator_branch_compiles(bridge):
+    tmp_path, ref, blocks, _ = bridge
     mdagm = [b for b in blocks if b.startswith("// DiracOpDwf::MatPcDagMatPc")]
-    assert len(inv) == len(minv) == len(matinv) == len(mdagm) == 1
-    # FdwfBase::FmatEvlInv / FmatEvlMInv / FmatInv and DiracOpDwf::MatPcDagMatPc signatures
-    # (lattice/f_dwf_base/f_dwf_base.C:189,232,576; dirac_op/d_op_dwf/d_op_dwf.C:174)
+    assert len(mdagm) == 1
     tu = f"""#include <config.h>
 #include <util/b200_bridge.h>
 #include <util/lattice.h>
 #include <util/dirac_op.h>
-#include <util/error.h>
 CPS_START_NAMESPACE
-struct BranchCheck : public FdwfBase {{
-  int inv(Vector *f_out, Vector *f_in, CgArg *cg_arg, CnvFrmType cnv_frm, Float *true_res) {{
-{inv[0]}    return 0;
-  }}
-  int minv(Vector **f_out, Vector *f_in, Float *shift, int Nshift, int isz, CgArg **cg_arg,
-           CnvFrmType cnv_frm, MultiShiftSolveType type, Float *alpha, Vector **f_out_d) {{
-{minv[0]}    return 0;
-  }}
-  int matinv(Vector *f_out, Vector *f_in, CgArg *cg_arg, Float *true_res, CnvFrmType cnv_frm,
-             PreserveType prs_f_in) {{
-    const char *cname = "BranchCheck", *fname = "matinv";
-{matinv[0]}    return 0;
-  }}
-}};
 struct OperatorCheck : public DiracOpDwf {{
   void mdagm(Vector *out, Vector *in, Float *dot_prd) {{
 {mdagm[0]}
@@ -93,4 +81,4 @@ struct OperatorCheck : public DiracOpDwf {{
 }};
 CPS_END_NAMESPACE
 """
-    compile_ok(tmp_path, "branches.C", tu, inc)
+    syntax_ok(tmp_path, "operator.C", tu, ref)
