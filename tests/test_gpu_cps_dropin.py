@@ -11,7 +11,9 @@ results are compared:
 
 * with the bridge's inner precision set to FP64: iteration counts within 1
   and solutions within 1e-9 relative of the CPU run (the bound the other
-  FP64 parity tests use), the reported true residuals below the tolerance;
+  FP64 parity tests use), the reported true residuals below the tolerance
+  (MInvCG's per-shift iterated residuals within 2%: a shift that freezes one
+  iteration apart reports the next iterate's residual);
 * with the bridge's defaults (16-bit inner CG for FmatEvlInv / FmatInv, FP32
   Krylov vectors for FmatEvlMInv): every FP64 true residual below the
   tolerance and the solutions within 3e-8 of the CPU run (the spread a 1e-10
@@ -75,7 +77,9 @@ def test_fmat_evl_minv_from_cps(name, action):
         assert rp_b[44] > 0, "the B200 build launched no kernels"
         if prec == F64:
             assert abs(it_b - it_c) <= 1, (it_b, it_c)
-            np.testing.assert_allclose(rp_b[:4], rp_c[:4], rtol=1e-5)
+            # each shift reports its iterated residual at the iteration it froze;
+            # reductions summed in another order can move that iteration by one
+            np.testing.assert_allclose(rp_b[:4], rp_c[:4], rtol=2e-2)
         else:
             assert np.all(rp_b[:4] <= 1e-10 * 1.01), rp_b[:4]
         n = len(src)
