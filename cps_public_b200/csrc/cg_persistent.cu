@@ -1,0 +1,305 @@
+// cg_persistent.cu -- every iteration of an FP64 CG solve on a small lattice in
+// one cooperative kernel.
+//
+// On lattices where one CG iteration is a few microseconds of device work (the
+// Wilson 8^4 workload has 2048 sites per checkerboard), the launch-per-step
+// loop of solver.cu is bound by launch and scheduling latency, not bandwidth.
+// Here a single cooperative launch runs the iterations of DiracOp::InvCg
+// (cps_pp/src/util/dirac_op/d_op_base/comsrc/inv_cg.C:293-364) until every
+// right-hand side halts: the four hops of MatPcDagMatPc (the residual update
+// r -= alpha A p, |r|^2 and x += alpha p fused into the last one, as in the
+// launch-per-step loop), then p = r + beta p, separated by grid barriers.
+// Every block keeps its own copy of the recurrence scalars (CgState) in shared
+// memory and sums the per-block partials of each reduction in block order, so
+// all blocks hold identical scalars and take the same branches; block 0
+// writes the state back when the loop ends.  Fields written inside the launch
+// are read through L2 (ld.global.cg), never through the read-only cache.
+//
+// Grid barriers spin on a generation counter with a time limit: a wait that
+// runs out sets the error flag, every other block leaves at its next wait, and
+// the host reports the error.  The cooperative launch keeps all blocks
+// resident, so the barriers complete in normal operation.
+#include <string.h>
+
+#include "host.h"
+#include "hop.cuh"
+
+namespace cpsb {
+
+constexpr int PCG_NT = 128;
+// Longest barrier wait before it gives up (ns of the global timer): far above a
+// phase of any lattice the loop takes, and above kernels of other streams that
+// may hold SMs while the launch's blocks become resident.
+constexpr unsigned long long PCG_WAIT_NS = 5000000000ull;
+
+__device__ __forceinline__ unsigned long long pcg_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+struct PcgArgs {
+  // the four hops of one iteration (in, out, x, cb, dag, a set per phase):
+  // [0] t1 = D p, [1] t2 = p - kappa^2 D t1 with |t2|^2, [2] t1 = D^dag t2,
+  // [3] A p = t2 - kappa^2 D^dag t1 consumed by the residual update
+  DslashArgs ph[4];
+  SpinorPtr r, p, x;
+  CgState *S;
+  double *partial;  // [nrhs][gridDim.x] block partials
+  unsigned *bar;    // [0] arrivals, [1] generation
+  int *err;         // set when a barrier wait ran out
+};
+
+// Grid barrier with a bounded wait; false (in every thread) when this block's
+// wait ran out or another block has already reported one.
+__device__ __forceinline__ bool pcg_sync(const PcgArgs &P) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = P.bar + 1;
+    volatile int *err = P.err;
+    const unsigned g0 = *gen;
+    __threadfence();
+    ok = 1;
+    if (atomicAdd(P.bar, 1u) == gridDim.x - 1) {
+      atomicExch(P.bar, 0u);
+      __threadfence();
+      atomicAdd(P.bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = pcg_now();
+      while (*gen == g0) {
+        if (*err || pcg_now() - t0 > PCG_WAIT_NS) {
+          atomicExch(P.err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// One hop over every unit of the lattice (the FP64 branch of hop_kernel with one
+// right-hand side per thread at a time).  MODE 0: out = D in; 1: out = x + a D in
+// with |out|^2 into nrm; 2: A p = x + a D in, then r -= alpha A p, x_sol += alpha p
+// and |r|^2 into nrm.
+template <bool LC, bool DAG, int MODE>
+__device__ __forceinline__ void pcg_hop(const DslashArgs &A, const PcgArgs &P, unsigned char *dsh, double *nrm,
+                                        const int *skip, const double *alpha) {
+  constexpr int NT = PCG_NT;
+  const Geom &g = A.g;
+  const int C0 = g.cs[0];
+  const int TX = NT / C0;
+  const HopShm L = hop_shm(TX, NT, g.nrhs, true, LC);
+  const int sp = threadIdx.x % C0;
+  const int xl = threadIdx.x / C0;
+  const int ntiles = (g.n4cb + TX - 1) / TX;
+  const int nunits = ntiles * g.ncls;
+  const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
+  for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+    const int k = unit % g.ncls, tile = unit / g.ncls;
+    const int par_out = A.five_d ? ((1 - A.cb + k) & 1) : 1 - A.cb;
+    __syncthreads();  // the previous unit is done with the tables
+    load_unit<P64, LC>(A, tile, k, par_out, TX, NT, dsh);
+    __syncthreads();
+    const int xs = tile * TX + xl;
+    const int C = g.cs[k];
+    if (xl >= TX || xs >= g.n4cb || sp >= C) continue;
+    HopCtx hc;
+    entry_ctx<P64, LC>(hc, A, dsh, L, xl, xs, k, sp, par_out);
+    const unsigned own = (k ? (unsigned)g.kb1 : 0u) + (unsigned)xs * (unsigned)C + (unsigned)sp;
+    for (int q = 0; q < g.nrhs; q++) {
+      if (skip[q]) continue;
+      const unsigned rb = (unsigned)q * per;
+      const unsigned i = rb + own;
+      Spinor<double> acc = hop_entry_64<P64, LC, DAG, 1, true>(A, hc, rb);
+      if (MODE == 0) {
+        store_spinor<P64>(A.out, i, acc);
+        continue;
+      }
+      const double a = A.a;
+      const Spinor<double> xv = unpack64(load_raw64_l2(A.x, i));
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc.c[s2][r] = xv.c[s2][r] + cscale(a, acc.c[s2][r]);
+      if (MODE == 1) {
+        store_spinor<P64>(A.out, i, acc);
+        nrm[q * NT + threadIdx.x] += norm2(acc);
+        continue;
+      }
+      const double al = alpha[q];
+      Spinor<double> rv = unpack64(load_raw64_l2(P.r, i));
+      const Spinor<double> pv = unpack64(load_raw64_l2(P.p, i));
+      Spinor<double> sv = unpack64(load_raw64_l2(P.x, i));
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) sv.c[s2][r] = cscale(al, pv.c[s2][r]) + sv.c[s2][r];
+      store_spinor<P64>(P.x, i, sv);
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) rv.c[s2][r] = rv.c[s2][r] - cscale(al, acc.c[s2][r]);
+      store_spinor<P64>(P.r, i, rv);
+      nrm[q * NT + threadIdx.x] += norm2(rv);
+    }
+  }
+}
+
+// Per-right-hand-side sums of nrm over the grid, left in out[] of every block
+// (the block partials summed in block order, the same order in every block).
+__device__ __forceinline__ bool pcg_reduce(const PcgArgs &P, int nrhs, double *nrm, double *red, double *out) {
+  constexpr int NT = PCG_NT;
+  for (int q = 0; q < nrhs; q++) {
+    const double bs = block_sum<NT>(nrm[q * NT + threadIdx.x], red);
+    nrm[q * NT + threadIdx.x] = 0;
+    if (threadIdx.x == 0) P.partial[q * gridDim.x + blockIdx.x] = bs;
+  }
+  if (!pcg_sync(P)) return false;
+  for (int q = 0; q < nrhs; q++) {
+    const double t = ordered_sum<NT>(P.partial + q * gridDim.x, gridDim.x, red);
+    if (threadIdx.x == 0) out[q] = t;
+    __syncthreads();
+  }
+  return true;
+}
+
+template <bool LC>
+__global__ void __launch_bounds__(PCG_NT, 1) pcg_kernel(PcgArgs P) {
+  constexpr int NT = PCG_NT;
+  extern __shared__ __align__(16) unsigned char dsh[];
+  __shared__ CgState S;
+  __shared__ double red[NT / 32];
+  __shared__ double sums[MAX_RHS], alpha[MAX_RHS];
+  __shared__ int skip[MAX_RHS];
+  const Geom &g = P.ph[0].g;
+  const int nrhs = g.nrhs;
+  const int C0 = g.cs[0];
+  const HopShm L = hop_shm(NT / C0, NT, nrhs, true, LC);
+  double *nrm = (double *)(dsh + L.norm);
+  if (threadIdx.x == 0) S = *P.S;
+  for (int q = 0; q < nrhs; q++) nrm[q * NT + threadIdx.x] = 0;
+  __syncthreads();
+  const long per = (long)g.n4cb * g.ls;
+  for (int guard = 0; guard <= S.max_iter + 1; guard++) {
+    bool all = true;
+    for (int q = 0; q < nrhs; q++) all = all && S.halt_done[q];
+    if (all) break;
+    if (threadIdx.x < nrhs) skip[threadIdx.x] = S.halt[threadIdx.x];
+    __syncthreads();
+    // t1 = D p
+    pcg_hop<LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
+    if (!pcg_sync(P)) break;
+    // t2 = MatPc p, d = |t2|^2
+    pcg_hop<LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
+    if (!pcg_reduce(P, nrhs, nrm, red, sums)) break;
+    if (threadIdx.x < nrhs && !skip[threadIdx.x]) S.d[threadIdx.x] = sums[threadIdx.x];
+    __syncthreads();
+    // t1 = D^dag t2
+    pcg_hop<LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
+    if (!pcg_sync(P)) break;
+    // A p = MatPcDag t2: r -= alpha A p, x += alpha p, |r|^2
+    if (threadIdx.x < nrhs) {
+      const int q = threadIdx.x;
+      alpha[q] = S.rr[q] / (S.d[q] + S.shift * S.pp[q]);
+    }
+    __syncthreads();
+    pcg_hop<LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
+    if (!pcg_reduce(P, nrhs, nrm, red, sums)) break;
+    if (threadIdx.x == 0)
+      for (int q = 0; q < nrhs; q++)
+        if (!skip[q]) cg_advance(&S, q, sums[q]);
+    __syncthreads();
+    // p = r + beta p for the right-hand sides still iterating (cg_xp_update, blas.cu)
+    for (int q = 0; q < nrhs; q++) {
+      if (S.halt_done[q] || S.halt[q]) continue;
+      const double b = S.beta[q];
+      for (long j = (long)blockIdx.x * NT + threadIdx.x; j < per; j += (long)gridDim.x * NT) {
+        const unsigned i = (unsigned)(q * per + j);
+        Spinor<double> pv = unpack64(load_raw64_l2(P.p, i));
+        const Spinor<double> rv = unpack64(load_raw64_l2(P.r, i));
+#pragma unroll
+        for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+          for (int r = 0; r < 3; r++) pv.c[s2][r] = cscale(b, pv.c[s2][r]) + rv.c[s2][r];
+        store_spinor<P64>(P.p, i, pv);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int q = 0; q < nrhs; q++) S.halt_done[q] = S.halt[q];
+    if (!pcg_sync(P)) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *P.S = S;
+}
+
+// Largest grid of a persistent solve on this device: all blocks resident.
+static int pcg_max_blocks(const void *fn, size_t shm) {
+  int dev = 0, nsm = 0, per_sm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_NT, shm) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nsm * per_sm;
+}
+
+int persistent_cg_mode() {
+  const char *e = getenv("CPSB_PERSISTENT_CG");
+  return e ? atoi(e) : 1;
+}
+
+// Runs the iterations of an FP64 CG solve whose state (r, p, x, CgState) the
+// caller has set up.  Returns cudaErrorNotSupported, launching nothing, where
+// the persistent form does not apply (the caller then runs its own loop).
+cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorPtr t1, SpinorPtr t2, SpinorPtr r,
+                                 SpinorPtr p, SpinorPtr x, CgState *S, double *partial, size_t partial_slots,
+                                 unsigned *bar_err, cudaStream_t st) {
+  const Geom &g = base.g;
+  const int C0 = g.cs[0];
+  if (C0 < 1 || C0 > PCG_NT) return cudaErrorNotSupported;
+  const int TX = PCG_NT / C0;
+  const bool lc = TX <= 32;
+  const HopShm L = hop_shm(TX, PCG_NT, g.nrhs, true, lc);
+  if (L.total > 48 * 1024) return cudaErrorNotSupported;
+  const void *fn = lc ? (const void *)pcg_kernel<true> : (const void *)pcg_kernel<false>;
+  const int units = ((g.n4cb + TX - 1) / TX) * g.ncls;
+  const int grid = std::min(units, pcg_max_blocks(fn, L.total));
+  if (grid < 1 || (size_t)grid * g.nrhs > partial_slots) return cudaErrorNotSupported;
+  PcgArgs P;
+  memset(&P, 0, sizeof(P));
+  for (int k = 0; k < 4; k++) {
+    P.ph[k] = base;
+    P.ph[k].rg = 1;
+    P.ph[k].rgroup = g.nrhs;
+    P.ph[k].torder = 0;
+    P.ph[k].skip = nullptr;
+    memset(&P.ph[k].red, 0, sizeof(Reduce));
+    P.ph[k].cg = nullptr;
+  }
+  P.ph[0].in = p, P.ph[0].out = t1, P.ph[0].cb = 1, P.ph[0].dag = 0, P.ph[0].a = 1.0;
+  P.ph[1].in = t1, P.ph[1].out = t2, P.ph[1].x = p, P.ph[1].cb = 0, P.ph[1].dag = 0, P.ph[1].a = mkappa2;
+  P.ph[2].in = t2, P.ph[2].out = t1, P.ph[2].cb = 1, P.ph[2].dag = 1, P.ph[2].a = 1.0;
+  P.ph[3].in = t1, P.ph[3].x = t2, P.ph[3].cb = 0, P.ph[3].dag = 1, P.ph[3].a = mkappa2;
+  P.r = r;
+  P.p = p;
+  P.x = x;
+  P.S = S;
+  P.partial = partial;
+  P.bar = bar_err;
+  P.err = (int *)(bar_err + 2);
+  cudaError_t e = cudaMemsetAsync(bar_err, 0, 4 * sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  void *args[] = {&P};
+  e = cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(PCG_NT), args, L.total, st);
+  count_launch();
+  return e;
+}
+
+}  // namespace cpsb

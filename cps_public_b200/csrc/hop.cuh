@@ -120,6 +120,19 @@ template <> __device__ __forceinline__ Raw<P64> load_raw<P64>(const SpinorPtr &f
   for (int k = 0; k < 12; k++) r.c[k] = __ldg(b + 8 * k);
   return r;
 }
+// The same through L2 only (ld.global.cg): for kernels that read a field that
+// other blocks of the same launch wrote (the read-only path may hold stale lines).
+__device__ __forceinline__ Raw<P64> load_raw64_l2(const SpinorPtr &f, unsigned i) {
+  const double2 *b = entry_ptr<12, double2>(f.data, i);
+  Raw<P64> r;
+#pragma unroll
+  for (int k = 0; k < 12; k++) r.c[k] = __ldcg(b + 8 * k);
+  return r;
+}
+template <bool L2ONLY> __device__ __forceinline__ Raw<P64> load_raw64(const SpinorPtr &f, unsigned i) {
+  if constexpr (L2ONLY) return load_raw64_l2(f, i);
+  else return load_raw<P64>(f, i);
+}
 template <> __device__ __forceinline__ Raw<P32> load_raw<P32>(const SpinorPtr &f, unsigned i) {
   const float4 *b = entry_ptr<6, float4>(f.data, i);
   Raw<P32> r;
@@ -413,6 +426,29 @@ __device__ __forceinline__ SpX2 merge_x2(const AccX2 &a) {
   return o;
 }
 
+// The recurrence scalars and the halting decision of one right-hand side once
+// the new |r|^2 = c is known (cg_r_update of blas.cu; inv_cg.C:329-364).
+__device__ __forceinline__ void cg_advance(CgState *S, int q, double c) {
+  const double rprev = S->rr[q];
+  const double d = S->d[q] + S->shift * S->pp[q];
+  S->alpha[q] = rprev / d;
+  S->rr_prev[q] = rprev;
+  S->rr[q] = c;
+  S->beta[q] = c / rprev;
+  S->iters[q] += 1;
+  int reason = HALT_NONE;
+  const double rn = sqrt(c);
+  if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
+  else if (c <= S->stp[q]) reason = HALT_CONVERGED;
+  else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
+  else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
+  if (rn > S->maxr[q]) S->maxr[q] = rn;
+  if (reason) {
+    S->halt[q] = 1;
+    S->reason[q] = reason;
+  }
+}
+
 // ---------------------------------------------------------------- the kernel
 // Shared-memory link table of a unit: for tile column xl and link j (0-3 the
 // forward links at x, 4-7 the backward links at x - mu) the 9 elements, row
@@ -512,8 +548,9 @@ struct HopCtx {
 
 // The hop of one FP64 entry (right-hand side at entry offset rb): the 8
 // neighbours with links from the table (LC) or global memory, and with A.hop5
-// the 5th-direction neighbours; no scaling.
-template <int P, bool LC, bool DAG, int DEPTH>
+// the 5th-direction neighbours; no scaling.  L2ONLY: spinor loads bypass the
+// read-only cache (the input was written earlier in the same launch).
+template <int P, bool LC, bool DAG, int DEPTH, bool L2ONLY = false>
 __device__ __forceinline__ Spinor<double> hop_entry_64(const DslashArgs &A, const HopCtx &hc, unsigned rb) {
   constexpr float sdag = DAG ? -1.f : 1.f;
   const void *lk = hc.lk;
@@ -523,15 +560,15 @@ __device__ __forceinline__ Spinor<double> hop_entry_64(const DslashArgs &A, cons
   zero(acc);
   // DEPTH: neighbours whose loads are in flight ahead of the one computed
   Raw<P64> nxt;
-  if (DEPTH >= 1) nxt = load_raw<P64>(A.in, rb + (unsigned)hc.nb[0]);
+  if (DEPTH >= 1) nxt = load_raw64<L2ONLY>(A.in, rb + (unsigned)hc.nb[0]);
 #pragma unroll
   for (int j = 0; j < 8; j++) {
     Raw<P64> cur;
     if (DEPTH >= 1) {
       cur = nxt;
-      if (j < 7) nxt = load_raw<P64>(A.in, rb + (unsigned)hc.nb[j + 1]);
+      if (j < 7) nxt = load_raw64<L2ONLY>(A.in, rb + (unsigned)hc.nb[j + 1]);
     } else {
-      cur = load_raw<P64>(A.in, rb + (unsigned)hc.nb[j]);
+      cur = load_raw64<L2ONLY>(A.in, rb + (unsigned)hc.nb[j]);
     }
     const int mu = j & 3;
     const double sg = j < 4 ? -(double)sdag : (double)sdag;
@@ -557,8 +594,8 @@ __device__ __forceinline__ Spinor<double> hop_entry_64(const DslashArgs &A, cons
     double2 vm[6], vp[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-      vm[q] = __ldg(bm + 8 * (um + q));
-      vp[q] = __ldg(bp + 8 * (up + q));
+      vm[q] = L2ONLY ? __ldcg(bm + 8 * (um + q)) : __ldg(bm + 8 * (um + q));
+      vp[q] = L2ONLY ? __ldcg(bp + 8 * (up + q)) : __ldg(bp + 8 * (up + q));
     }
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -873,28 +910,8 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           if (!CGR) {
             A.red.result[q] = t;
           } else {
-            // the recurrence scalars and the halting decision of cg_r_update (blas.cu)
-            CgState *S = A.cg;
-            const double c = t;
-            const double rprev = S->rr[q];
-            const double d = S->d[q] + S->shift * S->pp[q];
-            S->alpha[q] = rprev / d;
-            S->rr_prev[q] = rprev;
-            S->rr[q] = c;
-            S->beta[q] = c / rprev;
-            S->iters[q] += 1;
-            int reason = HALT_NONE;
-            const double rn = sqrt(c);
-            if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
-            else if (c <= S->stp[q]) reason = HALT_CONVERGED;
-            else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
-            else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
-            if (rn > S->maxr[q]) S->maxr[q] = rn;
-            if (reason) {
-              S->halt[q] = 1;
-              S->reason[q] = reason;
-            }
-            if (A.red.result) A.red.result[q] = c;
+            cg_advance(A.cg, q, t);
+            if (A.red.result) A.red.result[q] = t;
           }
         }
         __syncthreads();

@@ -192,6 +192,7 @@ struct CgSolver {
   unsigned long long graph_nodes = 0;  // kernels per batch (per loop body)
   DevBuf loop;                        // LoopCtl
   LoopCtl *hloop = nullptr;           // pinned: [0] to the device, [1] read back
+  DevBuf pcg_partial, pcg_bar;        // FP64 persistent loop: block partials; barrier words + error flag
   std::mutex busy;
 
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
@@ -204,6 +205,9 @@ struct CgSolver {
  private:
   void launch_batch(int k, cudaStream_t st);
   void run_batches(int batch, cudaStream_t st, const bool *done, bool any);
+  // FP64 solves on small lattices: every iteration in one cooperative kernel
+  // (cg_persistent.cu).  Returns false, launching nothing, where it does not apply.
+  bool run_persistent(cudaStream_t st);
   void true_residual(double *rr_out, const double *bnorm, cudaStream_t st, const int *skip_h = nullptr,
                      const int *skip_d = nullptr);
 };
@@ -225,6 +229,16 @@ cudaError_t launch_ms_loop_cond(cudaGraphConditionalHandle h, const MsBatch *B, 
                                 cudaStream_t st);
 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
+
+// The persistent FP64 CG loop (cg_persistent.cu).  CPSB_PERSISTENT_CG in the
+// environment: 0 off, 1 (default) for fields of at most PCG_AUTO_SITES entries,
+// 2 for any size that fits one cooperative launch.
+constexpr long PCG_AUTO_SITES = 1L << 17;
+constexpr size_t PCG_PARTIAL_SLOTS = (size_t)MAX_RHS * 148 * 16;
+int persistent_cg_mode();
+cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorPtr t1, SpinorPtr t2, SpinorPtr r,
+                                 SpinorPtr p, SpinorPtr x, CgState *S, double *partial, size_t partial_slots,
+                                 unsigned *bar_err, cudaStream_t st);
 
 // refiner: the solver for the per-shift refinement of reduced-precision
 // Krylov runs, one right-hand side per source vector (nullptr: the library's

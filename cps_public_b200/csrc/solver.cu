@@ -53,6 +53,8 @@ CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g)
     rS.create(P64, n);  // r, p, Ap of the FP64 recurrence
     pS.create(P64, n);
     ApS.create(P64, n);
+    pcg_partial.alloc(sizeof(double) * PCG_PARTIAL_SLOTS);
+    pcg_bar.alloc(4 * sizeof(unsigned));
   }
   state.alloc(sizeof(CgState));
   CK(cudaMallocHost((void **)&hstate, sizeof(CgState)));
@@ -170,6 +172,36 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
   }
 }
 
+bool CgSolver::run_persistent(cudaStream_t st) {
+  const int mode = persistent_cg_mode();
+  if (opS || shift != 0.0 || mode == 0 || !op64->can_fuse_cg_r()) return false;
+  if (mode == 1 && geom.nsites > PCG_AUTO_SITES) return false;
+  Operator &op = *op64;
+  DslashArgs A;
+  memset(&A, 0, sizeof(A));
+  A.g = op.geom;
+  A.U = G->ptr(P64);
+  A.five_d = p.action == CPSB_DWF;
+  A.hop5 = p.action == CPSB_DWF;
+  A.hop5_fact = 2.0 * p.a5_inv;
+  A.hop5_wall = -2.0 * p.mass * p.a5_inv;
+  A.bc_t_sign = 1.0;  // FP64 links carry the boundary sign
+  const cudaError_t e =
+      launch_persistent_cg(A, -op.kappa * op.kappa, op.t1.ptr(), op.t2.ptr(), rS.ptr(), pS.ptr(), x64.ptr(),
+                           (CgState *)state.p, (double *)pcg_partial.p, PCG_PARTIAL_SLOTS, (unsigned *)pcg_bar.p, st);
+  if (e == cudaErrorNotSupported) {
+    cudaGetLastError();
+    return false;
+  }
+  CK(e);
+  unsigned flags[4];
+  CK(cudaMemcpyAsync(hstate, state.p, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(flags, pcg_bar.p, sizeof(flags), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (flags[2]) throw Error{CPSB_ERR_CUDA, "persistent CG: a grid barrier wait ran out"};
+  return true;
+}
+
 // rr_out[q] = |b - (A + shift) x64|^2 (FP64), leaves r64 = b - (A + shift) x64,
 // for every right-hand side q not masked by skip_h (host) / skip_d (the same
 // mask on the device); masked entries of rr_out and r64 are left as they were.
@@ -271,7 +303,7 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
     bool all = true;
     for (int q = 0; q < nrhs; q++) all = all && done[q];
     if (all) break;
-    run_batches(batch, st, done, opS != nullptr);
+    if (!run_persistent(st)) run_batches(batch, st, done, opS != nullptr);
     CgState h = *hstate;
     if (!opS) {
       for (int q = 0; q < nrhs; q++) done[q] = true;
