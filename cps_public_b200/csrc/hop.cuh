@@ -213,52 +213,6 @@ template <> __device__ __forceinline__ HfX2 load_pair<P16>(const SpinorPtr &f, u
   return h;
 }
 
-// The same split into the loads and the decode, so the loads can be issued
-// ahead of the arithmetic that consumes them.
-template <int P> struct RawPair;
-template <> struct RawPair<P32> { float4 c[3]; };
-template <> struct RawPair<P16> { uint4 v; uint2 m; float nrm; };
-template <int P> __device__ __forceinline__ RawPair<P> load_pair_raw(const SpinorPtr &f, unsigned i, int p);
-template <> __device__ __forceinline__ RawPair<P32> load_pair_raw<P32>(const SpinorPtr &f, unsigned i, int p) {
-  const float4 *b = entry_ptr<6, float4>(f.data, i) + 24 * p;
-  RawPair<P32> r;
-#pragma unroll
-  for (int c = 0; c < 3; c++) r.c[c] = __ldg(b + 8 * c);
-  return r;
-}
-template <> __device__ __forceinline__ RawPair<P16> load_pair_raw<P16>(const SpinorPtr &f, unsigned i, int p) {
-  const uint4 *b = entry_ptr<3, uint4>(f.data, i);
-  RawPair<P16> r;
-  r.v = __ldg(b + (p ? 16 : 0));
-  r.m = __ldg((const uint2 *)(b + 8) + p);
-  r.nrm = __ldg(f.norm + i);
-  return r;
-}
-__device__ __forceinline__ HfX2 decode_pair(const RawPair<P32> &r, int, float *nrm) {
-  HfX2 h;
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    h.re[c] = f2(r.c[c].x, r.c[c].y);
-    h.im[c] = f2(r.c[c].z, r.c[c].w);
-  }
-  *nrm = 1.0f;
-  return h;
-}
-__device__ __forceinline__ HfX2 decode_pair(const RawPair<P16> &r, int p, float *nrm) {
-  HfX2 h;
-  if (p == 0) {
-    h.re[0] = dec16x2(r.v.x); h.im[0] = dec16x2(r.v.y);
-    h.re[1] = dec16x2(r.v.z); h.im[1] = dec16x2(r.v.w);
-    h.re[2] = dec16x2(r.m.x); h.im[2] = dec16x2(r.m.y);
-  } else {
-    h.re[0] = dec16x2(r.m.x); h.im[0] = dec16x2(r.m.y);
-    h.re[1] = dec16x2(r.v.x); h.im[1] = dec16x2(r.v.y);
-    h.re[2] = dec16x2(r.v.z); h.im[2] = dec16x2(r.v.w);
-  }
-  *nrm = r.nrm;
-  return h;
-}
-
 // Stores an entry and returns |stored value|^2 (for 16-bit storage the norm of
 // the rounded value that a later load returns; the squares are summed in FP32
 // and the quantum's square applied in FP64, since it can lie below FP32 range).
@@ -659,23 +613,15 @@ __device__ __forceinline__ Spinor<double> hop_entry_64(const DslashArgs &A, cons
   return acc;
 }
 
-// The same for FP32 / 16-bit storage in packed FP32x2 arithmetic.  EARLY:
-// the 5th-direction pair loads are issued with the 7th 4-D neighbour and the
-// entry of epi (the xpay input, when given) with the 8th, once no further
-// neighbour loads are in flight, instead of after the 4-D hop; *epi_raw
-// receives that entry.
-template <int P, bool LC, bool DAG, int DEPTH, bool EARLY = false>
-__device__ __forceinline__ SpX2 hop_entry_x2(const DslashArgs &A, const HopCtx &hc, unsigned rb,
-                                             const SpinorPtr *epi = nullptr, unsigned iepi = 0,
-                                             Raw<P> *epi_raw = nullptr) {
+// The same for FP32 / 16-bit storage in packed FP32x2 arithmetic.
+template <int P, bool LC, bool DAG, int DEPTH>
+__device__ __forceinline__ SpX2 hop_entry_x2(const DslashArgs &A, const HopCtx &hc, unsigned rb) {
   constexpr float sdag = DAG ? -1.f : 1.f;
   const void *lk = hc.lk;
   const int par_out = hc.par_out, x = hc.x;
   const float4 *l32 = (const float4 *)lk;
   AccX2 acc;
   zero_x2(acc);
-  const int pm = DAG ? 1 : 0;  // chirality pair taken from slice s-1 (s+1 gives the other)
-  RawPair<P> r5m, r5p;
   // DEPTH (1 or 2): neighbours whose loads are in flight ahead of the one computed
   Raw<P> nxt, nx2;
   nxt = load_raw<P>(A.in, rb + (unsigned)hc.nb[0]);
@@ -689,11 +635,6 @@ __device__ __forceinline__ SpX2 hop_entry_x2(const DslashArgs &A, const HopCtx &
     } else if (j < 7) {
       nxt = load_raw<P>(A.in, rb + (unsigned)hc.nb[j + 1]);
     }
-    if (EARLY && j == 6 && A.hop5) {
-      r5m = load_pair_raw<P>(A.in, rb + hc.e5m, pm);
-      r5p = load_pair_raw<P>(A.in, rb + hc.e5p, 1 - pm);
-    }
-    if (EARLY && j == 7 && epi) *epi_raw = load_raw<P>(*epi, iepi);
     float nrm;
     const float sg = j < 4 ? -sdag : sdag;
     // FP32: unpack, then project; 16-bit: project on the integers (iproject)
@@ -726,15 +667,10 @@ __device__ __forceinline__ SpX2 hop_entry_x2(const DslashArgs &A, const HopCtx &
   if (A.hop5) {
     // upper pair from s-1 and lower from s+1 at dag 0 (swapped at dag 1),
     // scaled by 2 a5_inv or, across the walls, -2 m_f a5_inv
+    const int pm = DAG ? 1 : 0;
     float nm, np;
-    HfX2 vm, vp;
-    if (EARLY) {
-      vm = decode_pair(r5m, pm, &nm);
-      vp = decode_pair(r5p, 1 - pm, &np);
-    } else {
-      vm = load_pair<P>(A.in, rb + hc.e5m, pm, &nm);
-      vp = load_pair<P>(A.in, rb + hc.e5p, 1 - pm, &np);
-    }
+    const HfX2 vm = load_pair<P>(A.in, rb + hc.e5m, pm, &nm);
+    const HfX2 vp = load_pair<P>(A.in, rb + hc.e5p, 1 - pm, &np);
     const float2 cm = f2b((float)hc.f5m * nm), cp = f2b((float)hc.f5p * np);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -794,7 +730,7 @@ __device__ __forceinline__ void entry_ctx(HopCtx &hc, const DslashArgs &A, const
 // their neighbour columns are read while they are in L2.
 // CGR: 0 none, 1 the fused residual update r -= alpha A p, 2 the same for the
 // shifted operator, r -= alpha (A p + shift p).
-template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, int CGR, bool DAG, int DEPTH, bool EARLY = false>
+template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, int CGR, bool DAG, int DEPTH>
 __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const Geom &g = A.g;
   extern __shared__ __align__(16) unsigned char dsh[];
@@ -891,12 +827,11 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         }
       } else {
         // ------------------------------------------------ FP32 / 16-bit, packed
-        Raw<P> xraw;
-        SpX2 o = hop_entry_x2<P, LC, DAG, DEPTH, EARLY>(A, hc, rb, XPAY ? &A.x : nullptr, i, &xraw);
+        SpX2 o = hop_entry_x2<P, LC, DAG, DEPTH>(A, hc, rb);
         const float2 a2 = f2b((float)A.a);
         if (XPAY) {
           float xn;
-          const SpX2 xv = unpack(EARLY ? xraw : load_raw<P>(A.x, i), &xn);
+          const SpX2 xv = unpack(load_raw<P>(A.x, i), &xn);
 #pragma unroll
           for (int p = 0; p < 2; p++)
 #pragma unroll
@@ -1018,7 +953,7 @@ static int resident_blocks(const void *fn, int nt, size_t shm) {
 // table (LC), right-hand-side grouping (GRP: as many right-hand sides per warp
 // as divide it, else one).  The fused residual update (A.cg) needs the xpay
 // form.
-template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH, bool EARLY = false>
+template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH>
 static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st, int rgroup, int torder) {
   const int C0 = A.g.cs[0];
   if (C0 < 1 || C0 > NT) return cudaErrorNotSupported;
@@ -1049,12 +984,12 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
   cudaError_t e = cudaSuccess;
 #define CPSB_HOP(XP, NR, CG, D)                                                            \
   {                                                                                        \
-    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH, EARLY>;      \
+    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH>;             \
     static bool done = false;                                                              \
     e = opt_in(fn, done);                                                                  \
     if (e != cudaSuccess) return e;                                                        \
     const long nb = std::min(units, (long)resident_blocks(fn, NT, L.total));                \
-    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH, EARLY><<<(unsigned)nb, NT, L.total, st>>>(A); \
+    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH><<<(unsigned)nb, NT, L.total, st>>>(A);      \
   }
 #define CPSB_HOP_D(XP, NR, CG)          \
   if (A.dag) CPSB_HOP(XP, NR, CG, true) \
@@ -1087,13 +1022,6 @@ static cudaError_t hop_launch_p(const DslashArgs &A, int xpay, int norm, int var
     case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 7: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st, 4, 0);
-    // shapes 2 and 0 with the 5th-direction and xpay loads issued early (FP32 / 16-bit)
-    case 8:
-      if constexpr (P == P64) return cudaErrorNotSupported;
-      else return hop_launch_v<P, 256, 2, true, false, 2, true>(A, xpay, norm, st, 0, 0);
-    case 9:
-      if constexpr (P == P64) return cudaErrorNotSupported;
-      else return hop_launch_v<P, 128, 4, true, false, 2, true>(A, xpay, norm, st, 0, 0);
     default: return cudaErrorNotSupported;
   }
 }
