@@ -26,7 +26,10 @@
 
 namespace cpsb {
 
-constexpr int PCG_NT = 128;
+// Threads per block: 128, or 32 for single-slice columns (Wilson), so that a
+// unit is 32 columns whose link table fits shared memory and a small lattice
+// still spreads over many SMs.
+constexpr int PCG_NT_MAX = 128;
 // Longest barrier wait before it gives up (ns of the global timer): far above a
 // phase of any lattice the loop takes, and above kernels of other streams that
 // may hold SMs while the launch's blocks become resident.
@@ -73,7 +76,6 @@ __device__ __forceinline__ bool pcg_sync(const PcgArgs &P) {
           ok = 0;
           break;
         }
-        __nanosleep(128);
       }
     }
     __threadfence();
@@ -86,10 +88,9 @@ __device__ __forceinline__ bool pcg_sync(const PcgArgs &P) {
 // right-hand side per thread at a time).  MODE 0: out = D in; 1: out = x + a D in
 // with |out|^2 into nrm; 2: A p = x + a D in, then r -= alpha A p, x_sol += alpha p
 // and |r|^2 into nrm.
-template <bool LC, bool DAG, int MODE>
+template <int NT, bool LC, bool DAG, int MODE>
 __device__ __forceinline__ void pcg_hop(const DslashArgs &A, const PcgArgs &P, unsigned char *dsh, double *nrm,
                                         const int *skip, const double *alpha) {
-  constexpr int NT = PCG_NT;
   const Geom &g = A.g;
   const int C0 = g.cs[0];
   const int TX = NT / C0;
@@ -152,8 +153,8 @@ __device__ __forceinline__ void pcg_hop(const DslashArgs &A, const PcgArgs &P, u
 
 // Per-right-hand-side sums of nrm over the grid, left in out[] of every block
 // (the block partials summed in block order, the same order in every block).
+template <int NT>
 __device__ __forceinline__ bool pcg_reduce(const PcgArgs &P, int nrhs, double *nrm, double *red, double *out) {
-  constexpr int NT = PCG_NT;
   for (int q = 0; q < nrhs; q++) {
     const double bs = block_sum<NT>(nrm[q * NT + threadIdx.x], red);
     nrm[q * NT + threadIdx.x] = 0;
@@ -168,9 +169,8 @@ __device__ __forceinline__ bool pcg_reduce(const PcgArgs &P, int nrhs, double *n
   return true;
 }
 
-template <bool LC>
-__global__ void __launch_bounds__(PCG_NT, 1) pcg_kernel(PcgArgs P) {
-  constexpr int NT = PCG_NT;
+template <int NT, bool LC>
+__global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ CgState S;
   __shared__ double red[NT / 32];
@@ -192,15 +192,15 @@ __global__ void __launch_bounds__(PCG_NT, 1) pcg_kernel(PcgArgs P) {
     if (threadIdx.x < nrhs) skip[threadIdx.x] = S.halt[threadIdx.x];
     __syncthreads();
     // t1 = D p
-    pcg_hop<LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
+    pcg_hop<NT, LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // t2 = MatPc p, d = |t2|^2
-    pcg_hop<LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
-    if (!pcg_reduce(P, nrhs, nrm, red, sums)) break;
+    pcg_hop<NT, LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
+    if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x < nrhs && !skip[threadIdx.x]) S.d[threadIdx.x] = sums[threadIdx.x];
     __syncthreads();
     // t1 = D^dag t2
-    pcg_hop<LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
+    pcg_hop<NT, LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // A p = MatPcDag t2: r -= alpha A p, x += alpha p, |r|^2
     if (threadIdx.x < nrhs) {
@@ -208,8 +208,8 @@ __global__ void __launch_bounds__(PCG_NT, 1) pcg_kernel(PcgArgs P) {
       alpha[q] = S.rr[q] / (S.d[q] + S.shift * S.pp[q]);
     }
     __syncthreads();
-    pcg_hop<LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
-    if (!pcg_reduce(P, nrhs, nrm, red, sums)) break;
+    pcg_hop<NT, LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
+    if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x == 0)
       for (int q = 0; q < nrhs; q++)
         if (!skip[q]) cg_advance(&S, q, sums[q]);
@@ -238,12 +238,12 @@ __global__ void __launch_bounds__(PCG_NT, 1) pcg_kernel(PcgArgs P) {
 }
 
 // Largest grid of a persistent solve on this device: all blocks resident.
-static int pcg_max_blocks(const void *fn, size_t shm) {
+static int pcg_max_blocks(const void *fn, int nt, size_t shm) {
   int dev = 0, nsm = 0, per_sm = 0, coop = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_NT, shm) != cudaSuccess) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, shm) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -263,14 +263,16 @@ cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorP
                                  unsigned *bar_err, cudaStream_t st) {
   const Geom &g = base.g;
   const int C0 = g.cs[0];
-  if (C0 < 1 || C0 > PCG_NT) return cudaErrorNotSupported;
-  const int TX = PCG_NT / C0;
+  if (C0 < 1 || C0 > PCG_NT_MAX) return cudaErrorNotSupported;
+  const int nt = C0 == 1 ? 32 : PCG_NT_MAX;
+  const int TX = nt / C0;
   const bool lc = TX <= 32;
-  const HopShm L = hop_shm(TX, PCG_NT, g.nrhs, true, lc);
+  const HopShm L = hop_shm(TX, nt, g.nrhs, true, lc);
   if (L.total > 48 * 1024) return cudaErrorNotSupported;
-  const void *fn = lc ? (const void *)pcg_kernel<true> : (const void *)pcg_kernel<false>;
+  const void *fn = nt == 32 ? (const void *)pcg_kernel<32, true>
+                            : lc ? (const void *)pcg_kernel<PCG_NT_MAX, true> : (const void *)pcg_kernel<PCG_NT_MAX, false>;
   const int units = ((g.n4cb + TX - 1) / TX) * g.ncls;
-  const int grid = std::min(units, pcg_max_blocks(fn, L.total));
+  const int grid = std::min(units, pcg_max_blocks(fn, nt, L.total));
   if (grid < 1 || (size_t)grid * g.nrhs > partial_slots) return cudaErrorNotSupported;
   PcgArgs P;
   memset(&P, 0, sizeof(P));
@@ -297,7 +299,7 @@ cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorP
   cudaError_t e = cudaMemsetAsync(bar_err, 0, 4 * sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
   void *args[] = {&P};
-  e = cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(PCG_NT), args, L.total, st);
+  e = cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(nt), args, L.total, st);
   count_launch();
   return e;
 }
