@@ -15,6 +15,11 @@
 // writes the state back when the loop ends.  Fields written inside the launch
 // are read through L2 (ld.global.cg), never through the read-only cache.
 //
+// Measured on B200 it is slower than the device-side graph loop of solver.cu
+// (Wilson 8^4 FP64: 345 against 408 solves/s; DWF 8^4 x Ls 16: 11.3 against
+// 10.5 ms per solve): the five grid barriers of an iteration cost more than
+// the kernel boundaries of a graph, so it runs only when asked for.
+//
 // Grid barriers spin on a generation counter with a time limit: a wait that
 // runs out sets the error flag, every other block leaves at its next wait, and
 // the host reports the error.  The cooperative launch keeps all blocks
@@ -252,7 +257,7 @@ static int pcg_max_blocks(const void *fn, int nt, size_t shm) {
 
 int persistent_cg_mode() {
   const char *e = getenv("CPSB_PERSISTENT_CG");
-  return e ? atoi(e) : 1;
+  return e ? atoi(e) : 0;
 }
 
 // Runs the iterations of an FP64 CG solve whose state (r, p, x, CgState) the

@@ -5,10 +5,8 @@ Both run DiracOp::InvCg's recurrence (inv_cg.C:293-364); they differ only in
 the number of blocks whose partial sums make up each dot product, so their
 iteration counts agree within one and their solutions within 1e-9 relative
 (the bound the FP64 solver keeps against CPS itself).  CPSB_PERSISTENT_CG
-selects the loop: 0 launch-per-step, 1 (default) persistent for fields of at
-most 2^17 entries, 2 persistent at any size.  The golden CPS cases that run
-through the default loop (Wilson 8^4, DWF 8^4 x Ls 16) are in
-test_gpu_parity.py.
+selects the loop: 0 (default) launch-per-step, 1 persistent for fields of at
+most 2^17 entries, 2 persistent at any size.
 """
 import ctypes as C
 import os
@@ -56,7 +54,7 @@ def _compare(op, srcs, mode=1):
     # the whole iteration loop is one launch: the set-up and the true residuals
     # are a handful of kernels per right-hand side, against several per
     # iteration step by step
-    assert nb <= 8 + 4 * len(srcs) and 10 * nb < na, (na, nb)
+    assert nb <= 16 + 4 * len(srcs) and 10 * nb < na, (na, nb)
     return ra, rb
 
 
