@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, Sp
   const long per = (long)g.n4cb * g.ls;
   double acc = 0;
   if (!S->halt[rhs]) {
-    const double sigma = S->sig[rhs];
+    const double sigma = S->shift;
     const double alpha = S->rr[rhs] / (S->d[rhs] + sigma * S->pp[rhs]);
     const T a = (T)alpha, ts = (T)sigma;
     for (long j = (long)blockIdx.x * NT + threadIdx.x; j < per; j += (long)gridDim.x * NT) {
@@ -246,7 +246,21 @@ __global__ void __launch_bounds__(NT) cg_r_update_kernel(Geom g, SpinorPtr r, Sp
     for (int q = 0; q < g.nrhs; q++) {
       double c = ordered_sum<NT>(red.partial + q * gridDim.x, gridDim.x, sh);
       if (threadIdx.x == 0 && !S->halt[q]) {
-        cg_advance(S, q, c);
+        const double rprev = S->rr[q];
+        const double d = S->d[q] + S->shift * S->pp[q];
+        S->alpha[q] = rprev / d;
+        S->rr_prev[q] = rprev;
+        S->rr[q] = c;
+        S->beta[q] = c / rprev;
+        S->iters[q] += 1;
+        int reason = HALT_NONE;
+        const double rn = sqrt(c);
+        if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
+        else if (c <= S->stp[q]) reason = HALT_CONVERGED;
+        else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
+        else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
+        if (rn > S->maxr[q]) S->maxr[q] = rn;
+        if (reason) { S->halt[q] = 1; S->reason[q] = reason; }
         if (red.result) red.result[q] = c;
       }
       __syncthreads();

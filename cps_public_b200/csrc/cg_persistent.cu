@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
     // A p = MatPcDag t2: r -= alpha A p, x += alpha p, |r|^2
     if (threadIdx.x < nrhs) {
       const int q = threadIdx.x;
-      alpha[q] = S.rr[q] / (S.d[q] + S.sig[q] * S.pp[q]);
+      alpha[q] = S.rr[q] / (S.d[q] + S.shift * S.pp[q]);
     }
     __syncthreads();
     pcg_hop<NT, LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);

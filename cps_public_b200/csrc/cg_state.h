@@ -21,9 +21,8 @@ struct CgState {
   double stp[MAX_RHS];       // stop when rr <= stp  (stop_rsd^2 |b|^2)
   double maxr[MAX_RHS];      // largest |r| since the last reliable update
   double pp[MAX_RHS];        // |p|^2 (needed for the shifted operator A + sigma)
-  double sig[MAX_RHS];       // shift sigma_q of (A + sigma_q): <p,(A+sigma_q)p> = d + sigma_q pp
   double delta;              // reliable-update threshold (0: pure CG)
-  double shift;              // nonzero when any sig[q] is: the updates then read p and form |p|^2
+  double shift;              // constant shift sigma of (A + sigma): <p,(A+sigma)p> = d + sigma pp
   int halt[MAX_RHS];         // set by the r-update: this RHS pauses for the host
   int halt_done[MAX_RHS];    // set after the x/p update of the halting iteration
   int reason[MAX_RHS];
@@ -31,33 +30,6 @@ struct CgState {
   int max_iter;              // CPS max_num_iter: at most max_num_iter-1 iterations
   int nrhs;
 };
-
-#ifdef __CUDACC__
-// The recurrence scalars and the halting decision of one right-hand side once
-// the new |r|^2 = c is known (inv_cg.C:329-364): shared by the residual-update
-// kernel (blas.cu), the hop with the fused residual update (hop.cuh) and the
-// persistent loop (cg_persistent.cu).
-__device__ __forceinline__ void cg_advance(CgState *S, int q, double c) {
-  const double rprev = S->rr[q];
-  const double d = S->d[q] + S->sig[q] * S->pp[q];
-  S->alpha[q] = rprev / d;
-  S->rr_prev[q] = rprev;
-  S->rr[q] = c;
-  S->beta[q] = c / rprev;
-  S->iters[q] += 1;
-  int reason = HALT_NONE;
-  const double rn = sqrt(c);
-  if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
-  else if (c <= S->stp[q]) reason = HALT_CONVERGED;
-  else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
-  else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
-  if (rn > S->maxr[q]) S->maxr[q] = rn;
-  if (reason) {
-    S->halt[q] = 1;
-    S->reason[q] = reason;
-  }
-}
-#endif
 
 }  // namespace cpsb
 

@@ -426,6 +426,29 @@ __device__ __forceinline__ SpX2 merge_x2(const AccX2 &a) {
   return o;
 }
 
+// The recurrence scalars and the halting decision of one right-hand side once
+// the new |r|^2 = c is known (cg_r_update of blas.cu; inv_cg.C:329-364).
+__device__ __forceinline__ void cg_advance(CgState *S, int q, double c) {
+  const double rprev = S->rr[q];
+  const double d = S->d[q] + S->shift * S->pp[q];
+  S->alpha[q] = rprev / d;
+  S->rr_prev[q] = rprev;
+  S->rr[q] = c;
+  S->beta[q] = c / rprev;
+  S->iters[q] += 1;
+  int reason = HALT_NONE;
+  const double rn = sqrt(c);
+  if (!(d != 0.0) || !isfinite(c)) reason = HALT_BREAKDOWN;
+  else if (c <= S->stp[q]) reason = HALT_CONVERGED;
+  else if (S->iters[q] >= S->max_iter - 1) reason = HALT_MAXITER;
+  else if (S->delta > 0 && rn < S->delta * S->maxr[q]) reason = HALT_RELIABLE;
+  if (rn > S->maxr[q]) S->maxr[q] = rn;
+  if (reason) {
+    S->halt[q] = 1;
+    S->reason[q] = reason;
+  }
+}
+
 // ---------------------------------------------------------------- the kernel
 // Shared-memory link table of a unit: for tile column xl and link j (0-3 the
 // forward links at x, 4-7 the backward links at x - mu) the 9 elements, row
@@ -717,7 +740,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   __shared__ double cg_alpha[MAX_RHS];
   if (CGR && threadIdx.x < g.nrhs) {
     const CgState *S = A.cg;
-    cg_alpha[threadIdx.x] = S->rr[threadIdx.x] / (S->d[threadIdx.x] + S->sig[threadIdx.x] * S->pp[threadIdx.x]);
+    cg_alpha[threadIdx.x] = S->rr[threadIdx.x] / (S->d[threadIdx.x] + S->shift * S->pp[threadIdx.x]);
   }
   const int C0 = g.cs[0];
   const int RG = A.rg;
@@ -776,7 +799,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           if (CGR == 2 || A.cg_x.data) {
             const Spinor<double> pv = unpack64(load_raw<P64>(A.cg_p, i));
             if (CGR == 2) {
-              const double sigma = A.cg->sig[rhs];
+              const double sigma = A.cg->shift;
 #pragma unroll
               for (int s2 = 0; s2 < 4; s2++)
 #pragma unroll
@@ -839,7 +862,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           SpX2 pv;
           double sigma = 0.0;
           if (CGR == 2 || A.cg_x.data) pv = unpack(load_raw<P>(A.cg_p, i), &pn);
-          if (CGR == 2) sigma = A.cg->sig[rhs];
+          if (CGR == 2) sigma = A.cg->shift;
           if (A.cg_x.data) {
             // x += alpha p in FP32 (the solution half of cg_xp_update, blas.cu)
             float xn;

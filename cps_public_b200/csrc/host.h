@@ -184,8 +184,7 @@ struct CgSolver {
   DevBuf scal;                        // misc per-RHS scalars
   double *hscal = nullptr;            // pinned: |b|^2 read back without its own synchronisation
   RedSlot red_d, red_r, red_p, red_misc;
-  double shift = 0;                   // nonzero when a right-hand side of the solve in progress is shifted
-  double sig[MAX_RHS] = {};           // per-right-hand-side shifts sigma_q of the solve in progress
+  double shift = 0;                   // sigma of the solve in progress
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;
   bool graph_shifted = false;
@@ -199,10 +198,9 @@ struct CgSolver {
   CgSolver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
   ~CgSolver();
   // Solves with x64 (initial guess) and b64 already packed; fills res[nrhs].
-  // stop_q: per-right-hand-side stop_rsd (nullptr: a.stop_rsd for all);
-  // sigma_q: per-right-hand-side shifts of (A + sigma_q) (nullptr: sigma for all).
+  // stop_q: per-right-hand-side stop_rsd (nullptr: a.stop_rsd for all).
   int solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma = 0.0,
-            const double *stop_q = nullptr, const double *sigma_q = nullptr);
+            const double *stop_q = nullptr);
 
  private:
   void launch_batch(int k, cudaStream_t st);

@@ -279,26 +279,6 @@ Scal2 scal_all(double a, double b) {
 // vector q on entry, its reported residual on return; res[q]: the report of
 // vector q (iters: CPS's iteration count of its Krylov phase plus, with
 // refinement, the refinement iterations).
-// Whether a refinement solver of nb right-hand sides of n1 entries each (all
-// shifts of all vectors at once) fits the free device memory with a margin.
-static bool batched_refinement_fits(Gauge *G, const cpsb_dirac_params &p, int prec, int nb, long n1) {
-  if (nb > MAX_RHS) return false;
-  const char *e = getenv("CPSB_BATCHED_REFINE");
-  if (e && atoi(e) == 0) return false;
-  const long N = nb * n1;
-  const bool m5 = p.action == CPSB_MOBIUS || p.action == CPSB_ZMOBIUS;
-  // x, b, r in FP64; r, p, Ap, the operator's temporaries and the iterate sum
-  // in the sloppy precision; the FP64 operator of one right-hand side
-  const size_t need = 3 * field_bytes(P64, N) + (5 + (m5 ? 1 : 0)) * field_bytes(prec, N) + field_bytes(P32, N) +
-                      (2 + (m5 ? 1 : 0)) * field_bytes(P64, n1) + 8 * 18 * 8 * (size_t)G->n4cb;
-  size_t free_b = 0, total_b = 0;
-  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return need + need / 8 + ((size_t)1 << 30) < free_b;
-}
-
 int multishift_multi(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a, int nvec, Field &chi,
                      std::vector<Field> &x, const double *shift, int nshift, double *rsd, int type,
                      const double *alpha, cpsb_solve_result *res, cudaStream_t st, CgSolver *refiner) {
@@ -466,53 +446,6 @@ int multishift_multi(Gauge *G, const cpsb_dirac_params &p, const cpsb_cg_arg &a,
         rsd[q * nshift + s] = ms_rsd[q * nshift + s];
         if (!h.s[q].conv[s] && status[q] >= 0) status[q] = CPSB_NOT_CONVERGED;
       }
-  } else if (!refiner && batched_refinement_fits(G, p, prec, nvec * nshift, n1)) {
-    // Refine every shift with mixed-precision CG on (A + shift_s) to its own
-    // tolerance, checked with the FP64 true residual, all shifts and vectors as
-    // the right-hand sides of one solve (right-hand side s*nvec + q: vector q,
-    // shift s): every hop serves all of them, and each right-hand side carries
-    // its own shift and stop_rsd and drops out once it has converged.
-    const int nb = nvec * nshift;
-    pv.clear();  // the Krylov phase's vectors make room for the solver
-    r.data.alloc(0);
-    r.norm.alloc(0);
-    Ap.data.alloc(0);
-    Ap.norm.alloc(0);
-    std::unique_ptr<CgSolver> cg(new CgSolver(G, p, prec, nb));
-    double stop_q[MAX_RHS], sig_q[MAX_RHS];
-    for (int s = 0; s < nshift; s++) {
-      CK(launch_convert(P64, cg->b64.view(s * n), P64, chi.ptr(), n, st));
-      CK(launch_convert(P64, cg->x64.view(s * n), px, psi[s].ptr(), n, st));
-      for (int q = 0; q < nvec; q++) {
-        stop_q[s * nvec + q] = rsd[q * nshift + s];
-        sig_q[s * nvec + q] = shift[s];
-      }
-    }
-    cpsb_solve_result rs[MAX_RHS];
-    const int rc = cg->solve(a, rs, st, 0.0, stop_q, sig_q);
-    (void)rc;
-    for (int s = 0; s < nshift; s++) {
-      for (int q = 0; q < nvec; q++) {
-        const cpsb_solve_result &o = rs[s * nvec + q];
-        total_iters[q] += o.iters - 1;
-        nupd[q] += o.reliable_updates;
-        rsd[q * nshift + s] = o.true_rsd;
-        if (o.status < 0) status[q] = o.status;
-        else if (o.status == CPSB_NOT_CONVERGED && status[q] == CPSB_OK) status[q] = CPSB_NOT_CONVERGED;
-      }
-      const SpinorPtr xs = cg->x64.view(s * n);
-      if (type == 1) {
-        Reduce none;
-        memset(&none, 0, sizeof(none));
-        const double al = alpha ? alpha[s] : 1.0;
-        if (s == 0) CK(launch_axpby(P64, x[0].ptr(), P64, xs, P64, SpinorPtr{}, g, scal_all(al, 0.0), nullptr, none, 0,
-                                    st));
-        else CK(launch_axpby(P64, x[0].ptr(), P64, x[0].ptr(), P64, xs, g, scal_all(1.0, al), nullptr, none, 0, st));
-      } else {
-        CK(cudaMemcpyAsync(x[s].data.p, xs.data, x[s].data.bytes, cudaMemcpyDeviceToDevice, st));
-      }
-    }
-    CK(cudaStreamSynchronize(st));  // the solver's fields are freed at the end of this block
   } else {
     // Refine every shift with mixed-precision CG on (A + shift_s) to its own
     // tolerance, checked with the FP64 true residual: one solve over all

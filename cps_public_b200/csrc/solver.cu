@@ -221,9 +221,8 @@ void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t s
   if (shift != 0.0) {
     Reduce none;
     memset(&none, 0, sizeof(none));
-    Scal2 sg = sc2(nrhs, 1.0, 0.0);
-    for (int q = 0; q < nrhs; q++) sg.b[q] = sig[q];
-    CK(launch_axpby(P64, r64.ptr(), P64, r64.ptr(), P64, x64.ptr(), geom, sg, skip_d, none, 0, st));
+    CK(launch_axpby(P64, r64.ptr(), P64, r64.ptr(), P64, x64.ptr(), geom, sc2(nrhs, 1.0, shift), skip_d,
+                    none, 0, st));
   }
   CK(launch_axpby(P64, r64.ptr(), P64, b64.ptr(), P64, r64.ptr(), geom, sc2(nrhs, 1.0, -1.0), skip_d, rm, 1,
                   st));
@@ -235,14 +234,10 @@ void CgSolver::true_residual(double *rr_out, const double *bnorm, cudaStream_t s
 }
 
 int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t st, double sigma,
-                    const double *stop_q, const double *sigma_q) {
+                    const double *stop_q) {
   auto stop = [&](int q) { return stop_q ? stop_q[q] : a.stop_rsd; };
   auto t0 = std::chrono::steady_clock::now();
-  shift = 0.0;
-  for (int q = 0; q < MAX_RHS; q++) {
-    sig[q] = q < nrhs ? (sigma_q ? sigma_q[q] : sigma) : 0.0;
-    if (sig[q] != 0.0) shift = sig[q];
-  }
+  shift = sigma;
   const Geom &gg = geom;
   double bnorm[MAX_RHS], rr[MAX_RHS];
   double *dres = (double *)scal.p;
@@ -260,7 +255,6 @@ int CgSolver::solve(const cpsb_cg_arg &a, cpsb_solve_result *res, cudaStream_t s
   const double delta = sloppy == P64 ? 0.0 : (a.reliable_delta > 0 ? a.reliable_delta : 0.1);
   hs.delta = delta;
   hs.shift = shift;
-  for (int q = 0; q < MAX_RHS; q++) hs.sig[q] = sig[q];
   hs.max_iter = a.max_num_iter;
   hs.nrhs = nrhs;
   int nupd[MAX_RHS] = {0};
