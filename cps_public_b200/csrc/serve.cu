@@ -53,7 +53,7 @@ static size_t solve_footprint(const cpsb_dirac_params &p, long n, int sloppy, in
   if (sloppy == P64) {
     b += field_bytes(P64, N) * (3 + op_tmp);             // r, p, Ap; temporaries of the FP64 operator
   } else {
-    b += field_bytes(P64, N) * op_tmp;                   // FP64 operator (true residuals)
+    b += field_bytes(P64, n) * op_tmp;                   // one-RHS FP64 operator (true residuals)
     b += field_bytes(sloppy, N) * (3 + op_tmp) + field_bytes(P32, N);  // r, p, Ap, temporaries; x
   }
   return b + (size_t)(8u << 20);                         // reduction slots, state, graph

@@ -28,11 +28,10 @@
 namespace cpsb {
 
 CgSolver::CgSolver(Gauge *g, const cpsb_dirac_params &pp, int sl, int nr) : G(g), p(pp), sloppy(sl), nrhs(nr) {
-  // The FP64 operator serves the FP64 recurrence or, for mixed precision, only
-  // the true residuals; either way it spans all right-hand sides, so the true
-  // residuals of the right-hand sides that pause together share each launch
-  // (the others are masked out).
-  op64.reset(new Operator(G, p, P64, nr));
+  // The FP64 operator serves the FP64 recurrence (all right-hand sides at once)
+  // or, for mixed precision, only the true residuals, which it forms one
+  // right-hand side at a time so that its temporaries are one vector each.
+  op64.reset(new Operator(G, p, P64, sl == P64 ? nr : 1));
   geom = op64->geom;
   geom.nrhs = nr;
   geom.nsites = op64->geom.nsites / op64->geom.nrhs * nr;
