@@ -54,7 +54,6 @@
 #include <map>
 #include <mutex>
 #include <tuple>
-#include <cuda_pipeline.h>
 #include "cpsb_device.cuh"
 #include "cg_state.h"
 #include "cpsb_kernels.h"
@@ -459,69 +458,19 @@ __device__ __forceinline__ void cg_advance(CgState *S, int q, double c) {
 constexpr int LSTR = 73;
 
 // Dynamic shared memory of a launch: links (LC shapes only), neighbour column
-// offsets and checkerboard indices, norm slots, and (epi bytes per thread) the
-// slots that the epilogue operands of the entry in flight are copied into.
+// offsets and checkerboard indices, norm slots.
 struct HopShm {
-  size_t links, nbo, xn, norm, epi, total;
+  size_t links, nbo, xn, norm, total;
 };
-__host__ __device__ inline HopShm hop_shm(int TX, int NT, int nrhs, bool red, bool lc, size_t epi = 0) {
+__host__ __device__ inline HopShm hop_shm(int TX, int NT, int nrhs, bool red, bool lc) {
   HopShm s;
   s.links = 0;
   s.nbo = lc ? (size_t)TX * LSTR * 16 : 0;
   s.xn = s.nbo + (size_t)TX * 8 * sizeof(int);
   s.norm = s.xn + (size_t)TX * 8 * sizeof(int);
   s.norm = (s.norm + 15) & ~(size_t)15;
-  s.epi = (s.norm + (red ? (size_t)NT * nrhs * sizeof(double) : 0) + 15) & ~(size_t)15;
-  s.total = s.epi + (size_t)NT * epi;
+  s.total = s.norm + (red ? (size_t)NT * nrhs * sizeof(double) : 0);
   return s;
-}
-
-// Epilogue operands of a 16-bit entry copied to shared memory asynchronously
-// (cp.async) when the entry's hop starts, so that their loads overlap the hop's
-// arithmetic instead of following it: the xpay input (chunks 0-2, norm 0) and,
-// with the fused CG update, r (chunks 3-5, norm 1), p (chunks 6-8, norm 2) and
-// the FP32 iterate sum x (chunks 9-14).  Chunk-major slots: chunk c of thread t
-// at 16 (c NT + t), so a warp's copies and reads hit consecutive banks.
-constexpr size_t EPI16_BYTES = 15 * 16 + 3 * 4;
-
-template <int NT, int CGR>
-__device__ __forceinline__ void epi16_issue(const DslashArgs &A, unsigned i, unsigned char *E) {
-  const int t = threadIdx.x;
-  unsigned char *nb = E + (size_t)15 * NT * 16;
-  auto cp3 = [&](int c0, int n, const SpinorPtr &f) {
-    const uint4 *b = entry_ptr<3, uint4>(f.data, i);
-#pragma unroll
-    for (int k = 0; k < 3; k++) __pipeline_memcpy_async(E + ((size_t)(c0 + k) * NT + t) * 16, b + 8 * k, 16);
-    __pipeline_memcpy_async(nb + ((size_t)n * NT + t) * 4, f.norm + i, 4);
-  };
-  cp3(0, 0, A.x);
-  if (CGR) {
-    cp3(3, 1, A.cg_r);
-    if (CGR == 2 || A.cg_x.data) cp3(6, 2, A.cg_p);
-    if (A.cg_x.data) {
-      const float4 *b = entry_ptr<6, float4>(A.cg_x.data, i);
-#pragma unroll
-      for (int k = 0; k < 6; k++) __pipeline_memcpy_async(E + ((size_t)(9 + k) * NT + t) * 16, b + 8 * k, 16);
-    }
-  }
-  __pipeline_commit();
-}
-template <int NT>
-__device__ __forceinline__ Raw<P16> epi16_raw(const unsigned char *E, int c0, int n) {
-  const int t = threadIdx.x;
-  Raw<P16> r;
-#pragma unroll
-  for (int k = 0; k < 3; k++) r.c[k] = *(const uint4 *)(E + ((size_t)(c0 + k) * NT + t) * 16);
-  r.nrm = *(const float *)(E + (size_t)15 * NT * 16 + ((size_t)n * NT + t) * 4);
-  return r;
-}
-template <int NT>
-__device__ __forceinline__ Raw<P32> epi16_x32(const unsigned char *E) {
-  const int t = threadIdx.x;
-  Raw<P32> r;
-#pragma unroll
-  for (int k = 0; k < 6; k++) r.c[k] = *(const float4 *)(E + ((size_t)(9 + k) * NT + t) * 16);
-  return r;
 }
 
 // Fills the unit's neighbour tables -- for column xl and neighbour j the
@@ -781,10 +730,8 @@ __device__ __forceinline__ void entry_ctx(HopCtx &hc, const DslashArgs &A, const
 // their neighbour columns are read while they are in L2.
 // CGR: 0 none, 1 the fused residual update r -= alpha A p, 2 the same for the
 // shifted operator, r -= alpha (A p + shift p).
-template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, int CGR, bool DAG, int DEPTH, bool EPI = false>
+template <int P, int NT, int MINB, bool LC, bool XPAY, bool NORM, int CGR, bool DAG, int DEPTH>
 __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
-  // EPI: the epilogue operands travel to shared memory during the hop (16-bit, xpay forms)
-  static_assert(!EPI || (P == P16 && XPAY), "asynchronous epilogue operands: 16-bit xpay hops only");
   const Geom &g = A.g;
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ double red[NT / 32];
@@ -798,9 +745,8 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   const int C0 = g.cs[0];
   const int RG = A.rg;
   const int TX = NT / (C0 * RG);
-  const HopShm L = hop_shm(TX, NT, g.nrhs, NORM || CGR, LC, EPI ? EPI16_BYTES : 0);
+  const HopShm L = hop_shm(TX, NT, g.nrhs, NORM || CGR, LC);
   double *nrm_sh = (double *)(dsh + L.norm);
-  unsigned char *epi_sh = dsh + L.epi;
   if (NORM || CGR)
     for (int q = 0; q < g.nrhs; q++) nrm_sh[q * NT + threadIdx.x] = 0;
   const int sp = threadIdx.x % C0;                 // slice index of the thread within its column
@@ -881,15 +827,11 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
         }
       } else {
         // ------------------------------------------------ FP32 / 16-bit, packed
-        if constexpr (EPI) epi16_issue<NT, CGR>(A, i, epi_sh);
         SpX2 o = hop_entry_x2<P, LC, DAG, DEPTH>(A, hc, rb);
-        if constexpr (EPI) __pipeline_wait_prior(0);
         const float2 a2 = f2b((float)A.a);
         if (XPAY) {
           float xn;
-          SpX2 xv;
-          if constexpr (EPI) xv = unpack(epi16_raw<NT>(epi_sh, 0, 0), &xn);
-          else xv = unpack(load_raw<P>(A.x, i), &xn);
+          const SpX2 xv = unpack(load_raw<P>(A.x, i), &xn);
 #pragma unroll
           for (int p = 0; p < 2; p++)
 #pragma unroll
@@ -915,23 +857,16 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
           // r -= alpha (A p + shift p), A p = o in registers (cg_r_update of blas.cu)
           const float alpha = (float)cg_alpha[rhs];
           float rn;
-          SpX2 rv;
-          if constexpr (EPI) rv = unpack(epi16_raw<NT>(epi_sh, 3, 1), &rn);
-          else rv = unpack(load_raw<P>(A.cg_r, i), &rn);
+          SpX2 rv = unpack(load_raw<P>(A.cg_r, i), &rn);
           float pn = 0.f;
           SpX2 pv;
           double sigma = 0.0;
-          if (CGR == 2 || A.cg_x.data) {
-            if constexpr (EPI) pv = unpack(epi16_raw<NT>(epi_sh, 6, 2), &pn);
-            else pv = unpack(load_raw<P>(A.cg_p, i), &pn);
-          }
+          if (CGR == 2 || A.cg_x.data) pv = unpack(load_raw<P>(A.cg_p, i), &pn);
           if (CGR == 2) sigma = A.cg->shift;
           if (A.cg_x.data) {
             // x += alpha p in FP32 (the solution half of cg_xp_update, blas.cu)
             float xn;
-            SpX2 xv;
-            if constexpr (EPI) xv = unpack(epi16_x32<NT>(epi_sh), &xn);
-            else xv = unpack(load_raw<P32>(A.cg_x, i), &xn);
+            SpX2 xv = unpack(load_raw<P32>(A.cg_x, i), &xn);
             const float2 ap = f2b(alpha * pn);
 #pragma unroll
             for (int p = 0; p < 2; p++)
@@ -1018,9 +953,8 @@ static int resident_blocks(const void *fn, int nt, size_t shm) {
 // table (LC), right-hand-side grouping (GRP: as many right-hand sides per warp
 // as divide it, else one).  The fused residual update (A.cg) needs the xpay
 // form.
-template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH, bool EPI = false>
+template <int P, int NT, int MINB, bool LC, bool GRP, int DEPTH>
 static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t st, int rgroup, int torder) {
-  if (EPI && (P != P16 || !xpay)) return cudaErrorNotSupported;
   const int C0 = A.g.cs[0];
   if (C0 < 1 || C0 > NT) return cudaErrorNotSupported;
   int rg = 1;
@@ -1037,7 +971,7 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
   if (TX < 1 || (LC && TX > 32)) return cudaErrorNotSupported;  // link tables of more than 32 columns: use !LC
   const bool cgr = A.cg != nullptr;
   if (cgr && !xpay) return cudaErrorInvalidValue;
-  const HopShm L = hop_shm(TX, NT, A.g.nrhs, norm || cgr, LC, EPI ? EPI16_BYTES : 0);
+  const HopShm L = hop_shm(TX, NT, A.g.nrhs, norm || cgr, LC);
   if (L.total > 200 * 1024) return cudaErrorNotSupported;
   const long units = (long)((A.g.n4cb + TX - 1) / TX) * A.g.ncls * ((A.g.nrhs + A.rgroup - 1) / A.rgroup);
   // the opt-in above the 48 KB default is set once per instantiation
@@ -1050,13 +984,12 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
   cudaError_t e = cudaSuccess;
 #define CPSB_HOP(XP, NR, CG, D)                                                            \
   {                                                                                        \
-    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH, EPI && XP && P == P16>; \
+    const void *fn = (const void *)hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH>;             \
     static bool done = false;                                                              \
     e = opt_in(fn, done);                                                                  \
     if (e != cudaSuccess) return e;                                                        \
     const long nb = std::min(units, (long)resident_blocks(fn, NT, L.total));                \
-    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH, EPI && XP && P == P16>                    \
-        <<<(unsigned)nb, NT, L.total, st>>>(A);                                            \
+    hop_kernel<P, NT, MINB, LC, XP, NR, CG, D, DEPTH><<<(unsigned)nb, NT, L.total, st>>>(A);      \
   }
 #define CPSB_HOP_D(XP, NR, CG)          \
   if (A.dag) CPSB_HOP(XP, NR, CG, true) \
@@ -1089,14 +1022,6 @@ static cudaError_t hop_launch_p(const DslashArgs &A, int xpay, int norm, int var
     case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 7: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st, 4, 0);
-    // shapes 2 and 0 with the epilogue operands copied to shared memory during the
-    // hop (16-bit xpay forms, including the fused CG update)
-    case 8:
-      if constexpr (P != P16) return cudaErrorNotSupported;
-      else return hop_launch_v<P, 256, 2, true, false, 2, true>(A, xpay, norm, st, 0, 0);
-    case 9:
-      if constexpr (P != P16) return cudaErrorNotSupported;
-      else return hop_launch_v<P, 128, 4, true, false, 2, true>(A, xpay, norm, st, 0, 0);
     default: return cudaErrorNotSupported;
   }
 }
