@@ -4,7 +4,8 @@ The autotuner picks one launch shape per operator shape, so the parity tests
 exercise only the winners; here each shape is pinned in a fresh process
 (CPSB_TUNE_FORCE) and Dslash / MatPcDagMatPc are compared with the oracle for
 Wilson, DWF and Mobius at FP64 (tolerance 1e-13), FP32 (2e-6 per hop) and
-16-bit storage (5e-4 per hop), on two non-cubic
+16-bit storage (5e-4 per hop), and a 16-bit mixed CG (Wilson, DWF; its last
+hop carries the CG update) against the oracle's FP64 solve, on two non-cubic
 antiperiodic lattices, 4x6x4x8 and 8x8x4x6 (columns of 1, 4 and 8 entries;
 tiles that end inside a lattice row).  A shape that does not fit an operator
 (link tables need columns of at least NT/32 entries) falls back to the tuned
@@ -47,6 +48,15 @@ def _child():
             m, dot = op.MatPcDagMatPcPrec(src, prec)
             rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
             out[f"{dims}/{action}/{prec}"] = [rel(d0, rd), rel(d1, rdd), rel(m, rm), abs(dot - rdot) / rdot]
+        if action != "mobius":
+            # the fused CG update in the last hop (16-bit mixed CG, two right-hand sides)
+            src2 = fields.random_source(n, 43)
+            xs, rs = op.InvCgMulti([src, src2], stop_rsd=1e-10, max_num_iter=5000, precision=cb.F16)
+            worst = 0.0
+            for x, b in zip(xs, (src, src2)):
+                xr, _, _ = ref.invcg(b, 1e-10, 5000)
+                worst = max(worst, float(np.linalg.norm(x - xr) / np.linalg.norm(xr)))
+            out[f"{dims}/{action}/cg16"] = [max(r.true_rsd for r in rs), worst, min(r.status for r in rs)]
     print(json.dumps(out))
 
 
@@ -58,6 +68,10 @@ def test_launch_shape_matches_oracle(variant):
     assert p.returncode == 0, p.stderr[-3000:]
     res = json.loads(p.stdout.strip().splitlines()[-1])
     for key, errs in res.items():
+        if key.endswith("/cg16"):
+            # mixed solve: FP64 true residual met, solution within 1e-8 of the oracle's FP64 solve
+            assert errs[2] == 0 and errs[0] <= 1e-10 and errs[1] < 1e-8, (key, errs)
+            continue
         prec = int(key.split("/")[2])
         tol = TOL[prec]
         assert errs[0] < tol and errs[1] < tol, (key, errs)
