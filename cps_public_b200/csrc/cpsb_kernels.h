@@ -58,7 +58,7 @@ int grid_blocks(long sites_per_rhs, int nt);
 // variant: launch shape 0..NUM_DSLASH_VARIANTS-1 of hop.cuh, chosen by the
 // autotuner; a launcher returns cudaErrorNotSupported for shapes that do not
 // fit the operator.
-constexpr int NUM_DSLASH_VARIANTS = 8;
+constexpr int NUM_DSLASH_VARIANTS = 9;
 cudaError_t launch_dslash(int prec, const DslashArgs &A, int xpay, int norm, int variant, cudaStream_t st);
 
 // ---------------------------------------------------------------- BLAS

@@ -920,6 +920,175 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
   }
 }
 
+// ---------------------------------------------------------------- direction-parallel FP64 hop
+// For lattices too small to fill the GPU with one thread per entry (Wilson 8^4:
+// 2048 entries per checkerboard), eight consecutive lanes share an entry: lane
+// d takes neighbour d (0-3 forward, 4-7 backward) -- one spinor and one link
+// load each, all eight in flight at once instead of one after another -- and
+// lanes 0 and 1 add the two 5th-direction terms.  The eight partial spinors are
+// summed by a three-step butterfly of warp shuffles, which leaves the same sum
+// in every lane, and lane 0 runs the epilogue of hop_kernel (xpay, norm, the
+// fused CG update).  Every warp runs the same number of rounds, so the
+// shuffles always have all 32 lanes.
+template <int NT, bool XPAY, bool NORM, int CGR, bool DAG>
+__global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
+  const Geom &g = A.g;
+  extern __shared__ __align__(16) unsigned char dsh[];
+  __shared__ double red[NT / 32];
+  __shared__ double cg_alpha[MAX_RHS];
+  double *nrm_sh = (double *)dsh;
+  if (CGR && threadIdx.x < g.nrhs) {
+    const CgState *S = A.cg;
+    cg_alpha[threadIdx.x] = S->rr[threadIdx.x] / (S->d[threadIdx.x] + S->shift * S->pp[threadIdx.x]);
+  }
+  if (NORM || CGR)
+    for (int q = 0; q < g.nrhs; q++) nrm_sh[q * NT + threadIdx.x] = 0;
+  __syncthreads();
+  constexpr double sdag = DAG ? -1.0 : 1.0;
+  const int d = threadIdx.x & 7;
+  const int lane = threadIdx.x & 31;
+  const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
+  const long total = (long)per * g.nrhs;
+  const long wstride = (long)gridDim.x * (NT / 32) * 4;
+  for (long e0 = ((long)blockIdx.x * (NT / 32) + threadIdx.x / 32) * 4; e0 < total; e0 += wstride) {
+    const long e = e0 + (lane >> 3);
+    const int q = e < total ? (int)(e / per) : 0;
+    const bool valid = e < total && !(A.skip && A.skip[q]);
+    Spinor<double> acc;
+    zero(acc);
+    unsigned i = 0;
+    if (valid) {
+      const unsigned own = (unsigned)(e - (long)q * per);
+      const int k = (g.ncls == 2 && own >= (unsigned)g.kb1) ? 1 : 0;
+      const int C = g.cs[k];
+      const unsigned rem = own - (k ? (unsigned)g.kb1 : 0u);
+      const int x = (int)(rem / (unsigned)C);
+      const int sp = (int)(rem - (unsigned)x * (unsigned)C);
+      const int s = g.ncls == 2 ? k + 2 * sp : sp;
+      const int par_out = A.five_d ? ((1 - A.cb + k) & 1) : 1 - A.cb;
+      const unsigned rb = (unsigned)q * per;
+      i = rb + own;
+      const int mu = d & 3;
+      const double sg = d < 4 ? -sdag : sdag;
+      Coord c = decode(g, x, par_out);
+      auto step = [&](int v, int n) { return d < 4 ? (v + 1 == n ? 0 : v + 1) : (v == 0 ? n - 1 : v - 1); };
+      switch (mu) {
+        case 0: c.x = step(c.x, g.lx); break;
+        case 1: c.y = step(c.y, g.ly); break;
+        case 2: c.z = step(c.z, g.lz); break;
+        default: c.t = step(c.t, g.lt); break;
+      }
+      const int xn = cbindex(g, c.x, c.y, c.z, c.t);
+      const unsigned ni = rb + (k ? (unsigned)g.kb1 : 0u) + (unsigned)xn * (unsigned)C + (unsigned)sp;
+      const Raw<P64> nr = load_raw<P64>(A.in, ni);
+      const Link<double> l = d < 4 ? load_link<P64>(A.U, par_out, mu, x) : load_link<P64>(A.U, 1 - par_out, mu, xn);
+      const Half<double> h = project(unpack64(nr), mu, sg);
+      switch (mu) {  // accum_reconstruct with a compile-time direction
+        case 0: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 0, sg); break;
+        case 1: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 1, sg); break;
+        case 2: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 2, sg); break;
+        default: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 3, sg); break;
+      }
+      if (A.hop5 && d < 2) {
+        // dwf_dslash_5_plus: lane 0 the term from slice s-1, lane 1 the one from s+1;
+        // upper (lower) chirality from s-1 (s+1) at dag 0, swapped at dag 1
+        const bool minus = d == 0;
+        const int sn = minus ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
+        const double f = minus ? (s == 0 ? A.hop5_wall : A.hop5_fact) : (s == g.ls - 1 ? A.hop5_wall : A.hop5_fact);
+        const double2 *b = entry_ptr<12, const double2>(A.in.data, rb + site_entry(g, sn, x));
+        if (minus != DAG) {  // adds to the upper chirality (spins 0, 1)
+#pragma unroll
+          for (int qq = 0; qq < 6; qq++) {
+            const double2 v = __ldg(b + 8 * qq);
+            acc.c[qq / 3][qq % 3] = acc.c[qq / 3][qq % 3] + cscale(f, mk(v.x, v.y));
+          }
+        } else {             // to the lower chirality (spins 2, 3)
+#pragma unroll
+          for (int qq = 0; qq < 6; qq++) {
+            const double2 v = __ldg(b + 8 * (6 + qq));
+            acc.c[2 + qq / 3][qq % 3] = acc.c[2 + qq / 3][qq % 3] + cscale(f, mk(v.x, v.y));
+          }
+        }
+      }
+    }
+    // sum of the eight partial spinors of the entry, the same bits in every lane
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          acc.c[a][r].re += __shfl_xor_sync(0xffffffffu, acc.c[a][r].re, o);
+          acc.c[a][r].im += __shfl_xor_sync(0xffffffffu, acc.c[a][r].im, o);
+        }
+    if (!valid || d != 0) continue;
+    const double a = A.a;
+    if (XPAY) {
+      const Spinor<double> xv = unpack64(load_raw<P64>(A.x, i));
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc.c[s2][r] = xv.c[s2][r] + cscale(a, acc.c[s2][r]);
+    } else if (a != 1.0) {
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc.c[s2][r] = cscale(a, acc.c[s2][r]);
+    }
+    if (CGR) {
+      const double alpha = cg_alpha[q];
+      Spinor<double> rv = unpack64(load_raw<P64>(A.cg_r, i));
+      if (CGR == 2 || A.cg_x.data) {
+        const Spinor<double> pv = unpack64(load_raw<P64>(A.cg_p, i));
+        if (CGR == 2) {
+          const double sigma = A.cg->shift;
+#pragma unroll
+          for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) acc.c[s2][r] = acc.c[s2][r] + cscale(sigma, pv.c[s2][r]);
+        }
+        if (A.cg_x.data) {
+          Spinor<double> xv = unpack64(load_raw<P64>(A.cg_x, i));
+#pragma unroll
+          for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) xv.c[s2][r] = cscale(alpha, pv.c[s2][r]) + xv.c[s2][r];
+          store_spinor<P64>(A.cg_x, i, xv);
+        }
+      }
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) rv.c[s2][r] = rv.c[s2][r] - cscale(alpha, acc.c[s2][r]);
+      store_spinor<P64>(A.cg_r, i, rv);
+      nrm_sh[q * NT + threadIdx.x] += norm2(rv);
+    } else {
+      store_spinor<P64>(A.out, i, acc);
+      if (NORM) nrm_sh[q * NT + threadIdx.x] += norm2(acc);
+    }
+  }
+  if (NORM || CGR) {
+    for (int q = 0; q < g.nrhs; q++) {
+      const double bs = block_sum<NT>(nrm_sh[q * NT + threadIdx.x], red);
+      if (threadIdx.x == 0) A.red.partial[q * gridDim.x + blockIdx.x] = bs;
+    }
+    if (last_block(A.red.ticket, gridDim.x)) {
+      for (int q = 0; q < g.nrhs; q++) {
+        const double t = ordered_sum<NT>(A.red.partial + q * gridDim.x, gridDim.x, red);
+        if (threadIdx.x == 0 && !(A.skip && A.skip[q])) {
+          if (!CGR) {
+            A.red.result[q] = t;
+          } else {
+            cg_advance(A.cg, q, t);
+            if (A.red.result) A.red.result[q] = t;
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
 // Blocks of a kernel that fit on the device at once with this dynamic shared
 // memory (at least 1, at most the 148*16 partial slots of a reduction).
 static int resident_blocks(const void *fn, int nt, size_t shm) {
@@ -1005,6 +1174,37 @@ static cudaError_t hop_launch_v(DslashArgs A, int xpay, int norm, cudaStream_t s
   return launched();
 }
 
+// The direction-parallel FP64 hop: eight lanes per entry, the grid no larger
+// than the blocks resident at once.
+template <int NT>
+static cudaError_t hop8_launch(const DslashArgs &A, int xpay, int norm, cudaStream_t st) {
+  const bool cgr = A.cg != nullptr;
+  if (cgr && !xpay) return cudaErrorInvalidValue;
+  const size_t shm = (norm || cgr) ? (size_t)NT * A.g.nrhs * sizeof(double) : 0;
+  const long entries = (long)A.g.n4cb * A.g.ls * A.g.nrhs;
+  const long want = (entries + NT / 8 - 1) / (NT / 8);
+  cudaError_t e = cudaSuccess;
+#define CPSB_HOP8(XP, NR, CG, D)                                                   \
+  {                                                                                \
+    const void *fn = (const void *)hop8_kernel<NT, XP, NR, CG, D>;                 \
+    const long nb = std::min(want, (long)resident_blocks(fn, NT, shm));            \
+    hop8_kernel<NT, XP, NR, CG, D><<<(unsigned)nb, NT, shm, st>>>(A);              \
+  }
+#define CPSB_HOP8_D(XP, NR, CG)          \
+  if (A.dag) CPSB_HOP8(XP, NR, CG, true) \
+  else CPSB_HOP8(XP, NR, CG, false)
+  if (cgr && A.cg_shift) CPSB_HOP8_D(true, false, 2)
+  else if (cgr) CPSB_HOP8_D(true, false, 1)
+  else if (xpay && norm) CPSB_HOP8_D(true, true, 0)
+  else if (xpay) CPSB_HOP8_D(true, false, 0)
+  else if (norm) CPSB_HOP8_D(false, true, 0)
+  else CPSB_HOP8_D(false, false, 0)
+#undef CPSB_HOP8_D
+#undef CPSB_HOP8
+  (void)e;
+  return launched();
+}
+
 // Launch shapes the autotuner chooses from: (threads, min blocks per SM, link
 // table, right-hand-side grouping).  Shapes with link tables need columns of at
 // least NT/32 entries (DWF, Mobius); shape 4 serves short columns (Wilson).
@@ -1022,6 +1222,10 @@ static cudaError_t hop_launch_p(const DslashArgs &A, int xpay, int norm, int var
     case 5: return hop_launch_v<P, 128, P == P64 ? 3 : 5, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 6: return hop_launch_v<P, 128, P == P64 ? 4 : 6, true, false, P == P64 ? 0 : 1>(A, xpay, norm, st, 0, 0);
     case 7: return hop_launch_v<P, 256, P == P64 ? 1 : 2, true, true, P == P64 ? 1 : 2>(A, xpay, norm, st, 4, 0);
+    // FP64: eight lanes per entry, one neighbour each (small lattices)
+    case 8:
+      if constexpr (P == P64) return hop8_launch<128>(A, xpay, norm, st);
+      else return cudaErrorNotSupported;
     default: return cudaErrorNotSupported;
   }
 }

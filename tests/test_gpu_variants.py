@@ -60,7 +60,7 @@ def _child():
     print(json.dumps(out))
 
 
-@pytest.mark.parametrize("variant", list(range(8)))
+@pytest.mark.parametrize("variant", list(range(9)))
 def test_launch_shape_matches_oracle(variant):
     env = dict(os.environ, CPSB_TUNE_FORCE=str(variant))
     p = subprocess.run([sys.executable, "-c", "import tests.test_gpu_variants as t; t._child()"], cwd=ROOT, env=env,
