@@ -392,13 +392,15 @@ def run_configs(no_cpu=False):
                           sample="one timed multishift solve per arm after a 30-iteration warm-up")
     gauges = serve_bench.make_gauges()
     sat = serve_bench.run(requests=12, rate=20.0, slots=4, precision="f32", seed=4, gauges=gauges)
+    light = serve_bench.run(requests=6, rate=0.2, slots=4, precision="f32", seed=6, gauges=gauges)
     alone = serve_bench.run(requests=4, rate=20.0, slots=4, precision="f32", seed=5, gauges=gauges,
                             one_at_a_time=True)
-    for d in (sat, alone):
+    for d in (sat, light, alone):
         d.pop("per_request", None)
-    cfg["config4"] = {"poisson_20_per_s": sat, "one_at_a_time": alone,
-                      "sample": "12 Poisson arrivals at 20/s (saturated: one GPU serves ~0.3 requests/s of this mix) "
-                                "and 4 requests submitted one at a time (latency = service time, no queueing)"}
+    cfg["config4"] = {"poisson_20_per_s": sat, "poisson_0.2_per_s": light, "one_at_a_time": alone,
+                      "sample": "12 Poisson arrivals at 20/s (saturated: one GPU serves ~0.3-0.6 requests/s of this "
+                                "mix), 6 Poisson arrivals at 0.2/s (below capacity), and 4 requests submitted one at "
+                                "a time (latency = service time, no queueing)"}
     del gauges
     cfg["seconds"] = time.perf_counter() - t0
     return cfg
