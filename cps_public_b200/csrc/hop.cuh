@@ -925,10 +925,11 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
 // 2048 entries per checkerboard), eight consecutive lanes share an entry: lane
 // d takes neighbour d (0-3 forward, 4-7 backward) -- one spinor and one link
 // load each, all eight in flight at once instead of one after another -- and
-// lanes 0 and 1 add the two 5th-direction terms.  The eight partial spinors are
-// summed by a three-step butterfly of warp shuffles, which leaves the same sum
-// in every lane, and lane 0 runs the epilogue of hop_kernel (xpay, norm, the
-// fused CG update).  Every warp runs the same number of rounds, so the
+// lanes 0 and 1 load the two 5th-direction terms.  Lane 0 then gathers the
+// eight partial spinors by warp shuffles and sums them in direction order,
+// adds the 5th-direction terms last and runs the epilogue of hop_kernel: the
+// same operations in the same order as hop_entry_64, so every launch shape
+// gives the same bits.  Every warp runs the same number of rounds, so the
 // shuffles always have all 32 lanes.
 template <int NT, bool XPAY, bool NORM, int CGR, bool DAG>
 __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
@@ -956,7 +957,11 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
     const bool valid = e < total && !(A.skip && A.skip[q]);
     Spinor<double> acc;
     zero(acc);
+    double2 v5[6];  // lane 0: the pair from slice s-1, lane 1: from s+1
+#pragma unroll
+    for (int qq = 0; qq < 6; qq++) v5[qq] = make_double2(0.0, 0.0);
     unsigned i = 0;
+    double f5m = 0.0, f5p = 0.0;
     if (valid) {
       const unsigned own = (unsigned)(e - (long)q * per);
       const int k = (g.ncls == 2 && own >= (unsigned)g.kb1) ? 1 : 0;
@@ -981,6 +986,16 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
       const int xn = cbindex(g, c.x, c.y, c.z, c.t);
       const unsigned ni = rb + (k ? (unsigned)g.kb1 : 0u) + (unsigned)xn * (unsigned)C + (unsigned)sp;
       const Raw<P64> nr = load_raw<P64>(A.in, ni);
+      if (A.hop5 && d < 2) {
+        // dwf_dslash_5_plus: upper (lower) chirality from s-1 (s+1) at dag 0, swapped at dag 1
+        const int sn = d == 0 ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
+        const int chunk0 = (d == 0) != DAG ? 0 : 6;
+        const double2 *b = entry_ptr<12, const double2>(A.in.data, rb + site_entry(g, sn, x));
+#pragma unroll
+        for (int qq = 0; qq < 6; qq++) v5[qq] = __ldg(b + 8 * (chunk0 + qq));
+        f5m = s == 0 ? A.hop5_wall : A.hop5_fact;
+        f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
+      }
       const Link<double> l = d < 4 ? load_link<P64>(A.U, par_out, mu, x) : load_link<P64>(A.U, 1 - par_out, mu, xn);
       const Half<double> h = project(unpack64(nr), mu, sg);
       switch (mu) {  // accum_reconstruct with a compile-time direction
@@ -989,39 +1004,38 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
         case 2: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 2, sg); break;
         default: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 3, sg); break;
       }
-      if (A.hop5 && d < 2) {
-        // dwf_dslash_5_plus: lane 0 the term from slice s-1, lane 1 the one from s+1;
-        // upper (lower) chirality from s-1 (s+1) at dag 0, swapped at dag 1
-        const bool minus = d == 0;
-        const int sn = minus ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
-        const double f = minus ? (s == 0 ? A.hop5_wall : A.hop5_fact) : (s == g.ls - 1 ? A.hop5_wall : A.hop5_fact);
-        const double2 *b = entry_ptr<12, const double2>(A.in.data, rb + site_entry(g, sn, x));
-        if (minus != DAG) {  // adds to the upper chirality (spins 0, 1)
-#pragma unroll
-          for (int qq = 0; qq < 6; qq++) {
-            const double2 v = __ldg(b + 8 * qq);
-            acc.c[qq / 3][qq % 3] = acc.c[qq / 3][qq % 3] + cscale(f, mk(v.x, v.y));
-          }
-        } else {             // to the lower chirality (spins 2, 3)
-#pragma unroll
-          for (int qq = 0; qq < 6; qq++) {
-            const double2 v = __ldg(b + 8 * (6 + qq));
-            acc.c[2 + qq / 3][qq % 3] = acc.c[2 + qq / 3][qq % 3] + cscale(f, mk(v.x, v.y));
-          }
-        }
-      }
     }
-    // sum of the eight partial spinors of the entry, the same bits in every lane
+    // lane 0 sums the eight partial spinors in direction order, as hop_entry_64
+    const int base = lane & ~7;
 #pragma unroll
-    for (int o = 1; o < 8; o <<= 1)
+    for (int j = 1; j < 8; j++)
 #pragma unroll
       for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-          acc.c[a][r].re += __shfl_xor_sync(0xffffffffu, acc.c[a][r].re, o);
-          acc.c[a][r].im += __shfl_xor_sync(0xffffffffu, acc.c[a][r].im, o);
+          const double re = __shfl_sync(0xffffffffu, acc.c[a][r].re, base + j);
+          const double im = __shfl_sync(0xffffffffu, acc.c[a][r].im, base + j);
+          acc.c[a][r] = acc.c[a][r] + mk(re, im);
         }
+    double2 vp[6];  // lane 1's pair, for lane 0
+#pragma unroll
+    for (int qq = 0; qq < 6; qq++)
+      vp[qq] = make_double2(__shfl_sync(0xffffffffu, v5[qq].x, base + 1), __shfl_sync(0xffffffffu, v5[qq].y, base + 1));
     if (!valid || d != 0) continue;
+    if (A.hop5) {
+#pragma unroll
+      for (int qq = 0; qq < 6; qq++) {
+        const cplx<double> lo = cscale(f5m, mk(v5[qq].x, v5[qq].y)), hi = cscale(f5p, mk(vp[qq].x, vp[qq].y));
+        cplx<double> &u = acc.c[qq / 3][qq % 3], &w = acc.c[2 + qq / 3][qq % 3];
+        if (!DAG) {
+          u = u + lo;
+          w = w + hi;
+        } else {
+          w = w + lo;
+          u = u + hi;
+        }
+      }
+    }
     const double a = A.a;
     if (XPAY) {
       const Spinor<double> xv = unpack64(load_raw<P64>(A.x, i));

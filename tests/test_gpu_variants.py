@@ -11,6 +11,7 @@ tiles that end inside a lattice row).  A shape that does not fit an operator
 (link tables need columns of at least NT/32 entries) falls back to the tuned
 one.
 """
+import hashlib
 import json
 import os
 import subprocess
@@ -48,6 +49,10 @@ def _child():
             m, dot = op.MatPcDagMatPcPrec(src, prec)
             rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
             out[f"{dims}/{action}/{prec}"] = [rel(d0, rd), rel(d1, rdd), rel(m, rm), abs(dot - rdot) / rdot]
+            h = hashlib.sha256()
+            for arr in (d0, d1, m, np.array([dot])):
+                h.update(np.ascontiguousarray(arr).tobytes())
+            out[f"{dims}/{action}/{prec}/sha"] = h.hexdigest()
         if action != "mobius":
             # the fused CG update in the last hop (16-bit mixed CG, two right-hand sides)
             src2 = fields.random_source(n, 43)
@@ -68,6 +73,8 @@ def test_launch_shape_matches_oracle(variant):
     assert p.returncode == 0, p.stderr[-3000:]
     res = json.loads(p.stdout.strip().splitlines()[-1])
     for key, errs in res.items():
+        if key.endswith("/sha"):
+            continue
         if key.endswith("/cg16"):
             # mixed solve: FP64 true residual met, solution within 1e-8 of the oracle's FP64 solve
             assert errs[2] == 0 and errs[0] <= 1e-10 and errs[1] < 1e-8, (key, errs)
@@ -76,3 +83,25 @@ def test_launch_shape_matches_oracle(variant):
         tol = TOL[prec]
         assert errs[0] < tol and errs[1] < tol, (key, errs)
         assert errs[2] < 4 * tol and errs[3] < 4 * tol, (key, errs)
+
+
+def _run_child(variant):
+    env = dict(os.environ, CPSB_TUNE_FORCE=str(variant))
+    p = subprocess.run([sys.executable, "-c", "import tests.test_gpu_variants as t; t._child()"], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
+def test_fp64_launch_shapes_give_identical_bits():
+    """The autotuner may pick any launch shape, so every FP64 shape must
+    compute the same bits: the one-thread-per-entry shapes (1: link table,
+    4: links from global memory) and the direction-parallel shape 8, whose
+    lane 0 sums the eight neighbours' contributions in the same order.  Dslash
+    (both checkerboards / daggers), MatPcDagMatPc and its dot, compared by
+    SHA-256 for Wilson, DWF and Mobius on both lattices."""
+    runs = {v: _run_child(v) for v in (1, 4, 8)}
+    keys = [k for k in runs[8] if k.endswith("/0/sha")]
+    assert len(keys) == 6
+    for k in keys:
+        assert runs[1][k] == runs[4][k] == runs[8][k], k
