@@ -1006,6 +1006,7 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
       }
     }
     // lane 0 sums the eight partial spinors in direction order, as hop_entry_64
+    // (only lane 0 accumulates: the other lanes keep their own partial to send)
     const int base = lane & ~7;
 #pragma unroll
     for (int j = 1; j < 8; j++)
@@ -1015,7 +1016,7 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
         for (int r = 0; r < 3; r++) {
           const double re = __shfl_sync(0xffffffffu, acc.c[a][r].re, base + j);
           const double im = __shfl_sync(0xffffffffu, acc.c[a][r].im, base + j);
-          acc.c[a][r] = acc.c[a][r] + mk(re, im);
+          if (d == 0) acc.c[a][r] = acc.c[a][r] + mk(re, im);
         }
     double2 vp[6];  // lane 1's pair, for lane 0
 #pragma unroll
