@@ -949,12 +949,13 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
   const int d = threadIdx.x & 7;
   const int lane = threadIdx.x & 31;
   const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
-  const long total = (long)per * g.nrhs;
   const long wstride = (long)gridDim.x * (NT / 32) * 4;
-  for (long e0 = ((long)blockIdx.x * (NT / 32) + threadIdx.x / 32) * 4; e0 < total; e0 += wstride) {
+  // right-hand sides one after another, each spread over the grid the same way
+  // whatever their number (so a right-hand side's reductions do not depend on it)
+  for (int q = 0; q < g.nrhs; q++)
+  for (long e0 = ((long)blockIdx.x * (NT / 32) + threadIdx.x / 32) * 4; e0 < (long)per; e0 += wstride) {
     const long e = e0 + (lane >> 3);
-    const int q = e < total ? (int)(e / per) : 0;
-    const bool valid = e < total && !(A.skip && A.skip[q]);
+    const bool valid = e < (long)per && !(A.skip && A.skip[q]);
     Spinor<double> acc;
     zero(acc);
     double2 v5[6];  // lane 0: the pair from slice s-1, lane 1: from s+1
@@ -963,7 +964,7 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
     unsigned i = 0;
     double f5m = 0.0, f5p = 0.0;
     if (valid) {
-      const unsigned own = (unsigned)(e - (long)q * per);
+      const unsigned own = (unsigned)e;
       const int k = (g.ncls == 2 && own >= (unsigned)g.kb1) ? 1 : 0;
       const int C = g.cs[k];
       const unsigned rem = own - (k ? (unsigned)g.kb1 : 0u);
@@ -1196,7 +1197,7 @@ static cudaError_t hop8_launch(const DslashArgs &A, int xpay, int norm, cudaStre
   const bool cgr = A.cg != nullptr;
   if (cgr && !xpay) return cudaErrorInvalidValue;
   const size_t shm = (norm || cgr) ? (size_t)NT * A.g.nrhs * sizeof(double) : 0;
-  const long entries = (long)A.g.n4cb * A.g.ls * A.g.nrhs;
+  const long entries = (long)A.g.n4cb * A.g.ls;  // of one right-hand side
   const long want = (entries + NT / 8 - 1) / (NT / 8);
   cudaError_t e = cudaSuccess;
 #define CPSB_HOP8(XP, NR, CG, D)                                                   \

