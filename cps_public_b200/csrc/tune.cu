@@ -6,8 +6,9 @@
 // events and the fastest is kept for the rest of the process.  Launches met
 // during a capture before tuning use variant 0.  CPSB_TUNE=0 disables tuning;
 // CPSB_TUNE_VERBOSE=1 prints each decision; CPSB_TUNE_FORCE=v pins variant v
-// (for profiling) wherever it fits.  The tuned kernels recompute the
-// same output, so tuning has no effect on results.
+// (for profiling) wherever it fits.  Every launch shape computes the same
+// operator output bit for bit; the fused norms and dot products are summed over
+// each shape's blocks in its own way, so they agree to rounding.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
