@@ -926,7 +926,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_kernel(DslashArgs A) {
 // d takes neighbour d (0-3 forward, 4-7 backward) -- one spinor and one link
 // load each, all eight in flight at once instead of one after another -- and
 // lanes 0 and 1 load the two 5th-direction terms.  Lane 0 then gathers the
-// eight partial spinors by warp shuffles and sums them in direction order,
+// eight partial spinors through shared memory and sums them in direction order,
 // adds the 5th-direction terms last and runs the epilogue of hop_kernel: the
 // same operations in the same order as hop_entry_64, so every launch shape
 // gives the same bits.  Every warp runs the same number of rounds, so the
@@ -937,7 +937,8 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ double red[NT / 32];
   __shared__ double cg_alpha[MAX_RHS];
-  double *nrm_sh = (double *)dsh;
+  double2 *gsh = (double2 *)dsh;                        // 12 x NT partial-spinor slots
+  double *nrm_sh = (double *)(dsh + (size_t)12 * NT * sizeof(double2));
   if (CGR && threadIdx.x < g.nrhs) {
     const CgState *S = A.cg;
     cg_alpha[threadIdx.x] = S->rr[threadIdx.x] / (S->d[threadIdx.x] + S->shift * S->pp[threadIdx.x]);
@@ -1006,19 +1007,26 @@ __global__ void __launch_bounds__(NT) hop8_kernel(DslashArgs A) {
         default: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 3, sg); break;
       }
     }
-    // lane 0 sums the eight partial spinors in direction order, as hop_entry_64
-    // (only lane 0 accumulates: the other lanes keep their own partial to send)
+    // lane 0 sums the eight partial spinors in direction order, as hop_entry_64,
+    // reading them from shared memory (component-major slots: conflict-free)
     const int base = lane & ~7;
 #pragma unroll
-    for (int j = 1; j < 8; j++)
+    for (int a = 0; a < 4; a++)
 #pragma unroll
-      for (int a = 0; a < 4; a++)
+      for (int r = 0; r < 3; r++) gsh[(3 * a + r) * NT + threadIdx.x] = make_double2(acc.c[a][r].re, acc.c[a][r].im);
+    __syncwarp();
+    if (d == 0) {
 #pragma unroll
-        for (int r = 0; r < 3; r++) {
-          const double re = __shfl_sync(0xffffffffu, acc.c[a][r].re, base + j);
-          const double im = __shfl_sync(0xffffffffu, acc.c[a][r].im, base + j);
-          if (d == 0) acc.c[a][r] = acc.c[a][r] + mk(re, im);
-        }
+      for (int j = 1; j < 8; j++)
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            const double2 v = gsh[(3 * a + r) * NT + threadIdx.x + j];
+            acc.c[a][r] = acc.c[a][r] + mk(v.x, v.y);
+          }
+    }
+    __syncwarp();  // the slots are written again in the next round
     double2 vp[6];  // lane 1's pair, for lane 0
 #pragma unroll
     for (int qq = 0; qq < 6; qq++)
@@ -1196,7 +1204,7 @@ template <int NT>
 static cudaError_t hop8_launch(const DslashArgs &A, int xpay, int norm, cudaStream_t st) {
   const bool cgr = A.cg != nullptr;
   if (cgr && !xpay) return cudaErrorInvalidValue;
-  const size_t shm = (norm || cgr) ? (size_t)NT * A.g.nrhs * sizeof(double) : 0;
+  const size_t shm = (size_t)12 * NT * sizeof(double2) + ((norm || cgr) ? (size_t)NT * A.g.nrhs * sizeof(double) : 0);
   const long entries = (long)A.g.n4cb * A.g.ls;  // of one right-hand side
   const long want = (entries + NT / 8 - 1) / (NT / 8);
   cudaError_t e = cudaSuccess;
