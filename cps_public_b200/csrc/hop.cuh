@@ -1207,7 +1207,6 @@ static cudaError_t hop8_launch(const DslashArgs &A, int xpay, int norm, cudaStre
   const size_t shm = (size_t)12 * NT * sizeof(double2) + ((norm || cgr) ? (size_t)NT * A.g.nrhs * sizeof(double) : 0);
   const long entries = (long)A.g.n4cb * A.g.ls;  // of one right-hand side
   const long want = (entries + NT / 8 - 1) / (NT / 8);
-  cudaError_t e = cudaSuccess;
 #define CPSB_HOP8(XP, NR, CG, D)                                                   \
   {                                                                                \
     const void *fn = (const void *)hop8_kernel<NT, XP, NR, CG, D>;                 \
@@ -1225,7 +1224,6 @@ static cudaError_t hop8_launch(const DslashArgs &A, int xpay, int norm, cudaStre
   else CPSB_HOP8_D(false, false, 0)
 #undef CPSB_HOP8_D
 #undef CPSB_HOP8
-  (void)e;
   return launched();
 }
 
