@@ -8,6 +8,11 @@ workload with CUDA events over many launches and reports algorithmic GB/s
 vectors, CUDA events over --reps applications), e.g. the Mobius operator with
 its fused hop + M5 kernels:
   python -m cps_public_b200.dslash_bench --op mdagm --action mobius --prec f16 --nrhs 12
+
+--op cg runs one InvCg on nrhs seeded sources, stopped after --reps
+iterations (a short launch sequence of every CG kernel, for a profiler), e.g.
+the 16-bit mixed solve's hop with the fused CG update:
+  python -m cps_public_b200.dslash_bench --op cg --dims 16,16,16,16 --prec f16 --nrhs 12 --reps 12
 """
 from __future__ import annotations
 
@@ -31,7 +36,7 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--action", default="dwf")
-    ap.add_argument("--op", default="hop", choices=["hop", "mdagm"])
+    ap.add_argument("--op", default="hop", choices=["hop", "mdagm", "cg"])
     a = ap.parse_args()
     dims = tuple(int(x) for x in a.dims.split(","))
     init(0)
@@ -44,6 +49,13 @@ def main():
     except Exception:
         pass
     lib = _lib.load()
+    if a.op == "cg":
+        srcs = [fields.random_source(op.n // 24, 100 + q) for q in range(a.nrhs)]
+        for name in a.prec.split(","):
+            _, rs = op.InvCgMulti(srcs, stop_rsd=1e-10, max_num_iter=a.reps, precision=PRECS[name])
+            print(json.dumps({"op": "cg", "action": a.action, "prec": name, "dims": dims, "ls": a.ls,
+                              "nrhs": a.nrhs, "iters": [r.iters for r in rs], "status": [r.status for r in rs]}))
+        return
     if a.op == "mdagm":
         import torch
         dev = torch.device("cuda", 0)
