@@ -35,6 +35,9 @@ namespace cpsb {
 // unit is 32 columns whose link table fits shared memory and a small lattice
 // still spreads over many SMs.
 constexpr int PCG_NT_MAX = 128;
+// Fields (all right-hand sides) of at most this many entries use the
+// direction-parallel hop phases.
+constexpr long PCG_DP_SITES = 1L << 14;
 // Longest barrier wait before it gives up (ns of the global timer): far above a
 // phase of any lattice the loop takes, and above kernels of other streams that
 // may hold SMs while the launch's blocks become resident.
@@ -156,6 +159,144 @@ __device__ __forceinline__ void pcg_hop(const DslashArgs &A, const PcgArgs &P, u
   }
 }
 
+// The same phase with eight lanes per entry (hop8_kernel of hop.cuh): lane d
+// loads neighbour d and its link, lanes 0 and 1 the 5th-direction terms, lane
+// 0 sums the partial spinors in direction order through the shared-memory
+// slots gsh (12 x NT double2) and runs the epilogue; all loads through L2.
+template <int NT, bool DAG, int MODE>
+__device__ __forceinline__ void pcg8_hop(const DslashArgs &A, const PcgArgs &P, double2 *gsh, double *nrm,
+                                         const int *skip, const double *alpha) {
+  const Geom &g = A.g;
+  constexpr double sdag = DAG ? -1.0 : 1.0;
+  const int d = threadIdx.x & 7;
+  const int lane = threadIdx.x & 31;
+  const unsigned per = (unsigned)g.n4cb * (unsigned)g.ls;
+  const long wstride = (long)gridDim.x * (NT / 32) * 4;
+  for (int q = 0; q < g.nrhs; q++) {
+    if (skip[q]) continue;
+    for (long e0 = ((long)blockIdx.x * (NT / 32) + threadIdx.x / 32) * 4; e0 < (long)per; e0 += wstride) {
+      const long e = e0 + (lane >> 3);
+      const bool valid = e < (long)per;
+      Spinor<double> acc;
+      zero(acc);
+      double2 v5[6];
+#pragma unroll
+      for (int qq = 0; qq < 6; qq++) v5[qq] = make_double2(0.0, 0.0);
+      unsigned i = 0;
+      double f5m = 0.0, f5p = 0.0;
+      if (valid) {
+        const unsigned own = (unsigned)e;
+        const int k = (g.ncls == 2 && own >= (unsigned)g.kb1) ? 1 : 0;
+        const int C = g.cs[k];
+        const unsigned rem = own - (k ? (unsigned)g.kb1 : 0u);
+        const int x = (int)(rem / (unsigned)C);
+        const int sp = (int)(rem - (unsigned)x * (unsigned)C);
+        const int s = g.ncls == 2 ? k + 2 * sp : sp;
+        const int par_out = A.five_d ? ((1 - A.cb + k) & 1) : 1 - A.cb;
+        const unsigned rb = (unsigned)q * per;
+        i = rb + own;
+        const int mu = d & 3;
+        const double sg = d < 4 ? -sdag : sdag;
+        Coord c = decode(g, x, par_out);
+        auto step = [&](int v, int n) { return d < 4 ? (v + 1 == n ? 0 : v + 1) : (v == 0 ? n - 1 : v - 1); };
+        switch (mu) {
+          case 0: c.x = step(c.x, g.lx); break;
+          case 1: c.y = step(c.y, g.ly); break;
+          case 2: c.z = step(c.z, g.lz); break;
+          default: c.t = step(c.t, g.lt); break;
+        }
+        const int xn = cbindex(g, c.x, c.y, c.z, c.t);
+        const unsigned ni = rb + (k ? (unsigned)g.kb1 : 0u) + (unsigned)xn * (unsigned)C + (unsigned)sp;
+        const Raw<P64> nr = load_raw64_l2(A.in, ni);
+        if (A.hop5 && d < 2) {
+          const int sn = d == 0 ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
+          const int chunk0 = (d == 0) != DAG ? 0 : 6;
+          const double2 *b = entry_ptr<12, const double2>(A.in.data, rb + site_entry(g, sn, x));
+#pragma unroll
+          for (int qq = 0; qq < 6; qq++) v5[qq] = __ldcg(b + 8 * (chunk0 + qq));
+          f5m = s == 0 ? A.hop5_wall : A.hop5_fact;
+          f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
+        }
+        const Link<double> l = d < 4 ? load_link<P64>(A.U, par_out, mu, x) : load_link<P64>(A.U, 1 - par_out, mu, xn);
+        const Half<double> h = project(unpack64(nr), mu, sg);
+        switch (mu) {
+          case 0: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 0, sg); break;
+          case 1: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 1, sg); break;
+          case 2: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 2, sg); break;
+          default: accum_reconstruct(acc, d < 4 ? umul(l, h) : umul_dag(l, h), 3, sg); break;
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) gsh[(3 * a + r) * NT + threadIdx.x] = make_double2(acc.c[a][r].re, acc.c[a][r].im);
+      __syncwarp();
+      if (d == 0) {
+#pragma unroll
+        for (int j = 1; j < 8; j++)
+#pragma unroll
+          for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+              const double2 v = gsh[(3 * a + r) * NT + threadIdx.x + j];
+              acc.c[a][r] = acc.c[a][r] + mk(v.x, v.y);
+            }
+      }
+      __syncwarp();
+      const int base = lane & ~7;
+      double2 vp[6];
+#pragma unroll
+      for (int qq = 0; qq < 6; qq++)
+        vp[qq] = make_double2(__shfl_sync(0xffffffffu, v5[qq].x, base + 1), __shfl_sync(0xffffffffu, v5[qq].y, base + 1));
+      if (!valid || d != 0) continue;
+      if (A.hop5) {
+#pragma unroll
+        for (int qq = 0; qq < 6; qq++) {
+          const cplx<double> lo = cscale(f5m, mk(v5[qq].x, v5[qq].y)), hi = cscale(f5p, mk(vp[qq].x, vp[qq].y));
+          cplx<double> &u = acc.c[qq / 3][qq % 3], &w = acc.c[2 + qq / 3][qq % 3];
+          if (!DAG) {
+            u = u + lo;
+            w = w + hi;
+          } else {
+            w = w + lo;
+            u = u + hi;
+          }
+        }
+      }
+      if (MODE == 0) {
+        store_spinor<P64>(A.out, i, acc);
+        continue;
+      }
+      const double a = A.a;
+      const Spinor<double> xv = unpack64(load_raw64_l2(A.x, i));
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc.c[s2][r] = xv.c[s2][r] + cscale(a, acc.c[s2][r]);
+      if (MODE == 1) {
+        store_spinor<P64>(A.out, i, acc);
+        nrm[q * NT + threadIdx.x] += norm2(acc);
+        continue;
+      }
+      const double al = alpha[q];
+      Spinor<double> rv = unpack64(load_raw64_l2(P.r, i));
+      const Spinor<double> pv = unpack64(load_raw64_l2(P.p, i));
+      Spinor<double> sv = unpack64(load_raw64_l2(P.x, i));
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) sv.c[s2][r] = cscale(al, pv.c[s2][r]) + sv.c[s2][r];
+      store_spinor<P64>(P.x, i, sv);
+#pragma unroll
+      for (int s2 = 0; s2 < 4; s2++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) rv.c[s2][r] = rv.c[s2][r] - cscale(al, acc.c[s2][r]);
+      store_spinor<P64>(P.r, i, rv);
+      nrm[q * NT + threadIdx.x] += norm2(rv);
+    }
+  }
+}
+
 // Per-right-hand-side sums of nrm over the grid, left in out[] of every block
 // (the block partials summed in block order, the same order in every block).
 template <int NT>
@@ -174,7 +315,8 @@ __device__ __forceinline__ bool pcg_reduce(const PcgArgs &P, int nrhs, double *n
   return true;
 }
 
-template <int NT, bool LC>
+// DP: the hop phases with eight lanes per entry (pcg8_hop), for the smallest lattices.
+template <int NT, bool LC, bool DP>
 __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ CgState S;
@@ -185,7 +327,8 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
   const int nrhs = g.nrhs;
   const int C0 = g.cs[0];
   const HopShm L = hop_shm(NT / C0, NT, nrhs, true, LC);
-  double *nrm = (double *)(dsh + L.norm);
+  double2 *gsh = (double2 *)dsh;  // DP: 12 x NT partial-spinor slots
+  double *nrm = (double *)(dsh + (DP ? (size_t)12 * NT * sizeof(double2) : L.norm));
   if (threadIdx.x == 0) S = *P.S;
   for (int q = 0; q < nrhs; q++) nrm[q * NT + threadIdx.x] = 0;
   __syncthreads();
@@ -197,15 +340,18 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
     if (threadIdx.x < nrhs) skip[threadIdx.x] = S.halt[threadIdx.x];
     __syncthreads();
     // t1 = D p
-    pcg_hop<NT, LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, false, 0>(P.ph[0], P, gsh, nrm, skip, alpha);
+    else pcg_hop<NT, LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // t2 = MatPc p, d = |t2|^2
-    pcg_hop<NT, LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, false, 1>(P.ph[1], P, gsh, nrm, skip, alpha);
+    else pcg_hop<NT, LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
     if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x < nrhs && !skip[threadIdx.x]) S.d[threadIdx.x] = sums[threadIdx.x];
     __syncthreads();
     // t1 = D^dag t2
-    pcg_hop<NT, LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, true, 0>(P.ph[2], P, gsh, nrm, skip, alpha);
+    else pcg_hop<NT, LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // A p = MatPcDag t2: r -= alpha A p, x += alpha p, |r|^2
     if (threadIdx.x < nrhs) {
@@ -213,7 +359,8 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
       alpha[q] = S.rr[q] / (S.d[q] + S.shift * S.pp[q]);
     }
     __syncthreads();
-    pcg_hop<NT, LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, true, 2>(P.ph[3], P, gsh, nrm, skip, alpha);
+    else pcg_hop<NT, LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
     if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x == 0)
       for (int q = 0; q < nrhs; q++)
@@ -269,15 +416,21 @@ cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorP
   const Geom &g = base.g;
   const int C0 = g.cs[0];
   if (C0 < 1 || C0 > PCG_NT_MAX) return cudaErrorNotSupported;
-  const int nt = C0 == 1 ? 32 : PCG_NT_MAX;
+  const long per = (long)g.n4cb * g.ls;
+  // eight lanes per entry where even that leaves blocks for every SM to spare
+  const bool dp = per * g.nrhs <= PCG_DP_SITES;
+  const int nt = dp ? PCG_NT_MAX : C0 == 1 ? 32 : PCG_NT_MAX;
   const int TX = nt / C0;
   const bool lc = TX <= 32;
-  const HopShm L = hop_shm(TX, nt, g.nrhs, true, lc);
-  if (L.total > 48 * 1024) return cudaErrorNotSupported;
-  const void *fn = nt == 32 ? (const void *)pcg_kernel<32, true>
-                            : lc ? (const void *)pcg_kernel<PCG_NT_MAX, true> : (const void *)pcg_kernel<PCG_NT_MAX, false>;
-  const int units = ((g.n4cb + TX - 1) / TX) * g.ncls;
-  const int grid = std::min(units, pcg_max_blocks(fn, nt, L.total));
+  const size_t shm = dp ? (size_t)12 * nt * sizeof(double2) + (size_t)nt * g.nrhs * sizeof(double)
+                        : hop_shm(TX, nt, g.nrhs, true, lc).total;
+  if (shm > 48 * 1024) return cudaErrorNotSupported;
+  const void *fn = dp ? (const void *)pcg_kernel<PCG_NT_MAX, false, true>
+                      : nt == 32 ? (const void *)pcg_kernel<32, true, false>
+                      : lc ? (const void *)pcg_kernel<PCG_NT_MAX, true, false>
+                           : (const void *)pcg_kernel<PCG_NT_MAX, false, false>;
+  const long units = dp ? (per + nt / 8 - 1) / (nt / 8) : (long)((g.n4cb + TX - 1) / TX) * g.ncls;
+  const int grid = (int)std::min(units, (long)pcg_max_blocks(fn, nt, shm));
   if (grid < 1 || (size_t)grid * g.nrhs > partial_slots) return cudaErrorNotSupported;
   PcgArgs P;
   memset(&P, 0, sizeof(P));
@@ -304,7 +457,7 @@ cudaError_t launch_persistent_cg(const DslashArgs &base, double mkappa2, SpinorP
   cudaError_t e = cudaMemsetAsync(bar_err, 0, 4 * sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
   void *args[] = {&P};
-  e = cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(nt), args, L.total, st);
+  e = cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(nt), args, shm, st);
   count_launch();
   return e;
 }
