@@ -163,9 +163,20 @@ __device__ __forceinline__ void pcg_hop(const DslashArgs &A, const PcgArgs &P, u
 // loads neighbour d and its link, lanes 0 and 1 the 5th-direction terms, lane
 // 0 sums the partial spinors in direction order through the shared-memory
 // slots gsh (12 x NT double2) and runs the epilogue; all loads through L2.
-template <int NT, bool DAG, int MODE>
+// PUPD folds the direction update p = r + beta p of the previous iteration in:
+// MODE 0 forms each neighbour's r + beta p from r and the old p as it loads
+// them, and MODE 1 forms its own entry's, stores it as the new p and uses it as
+// the xpay input (one fused multiply-add per real in both, so the two agree).
+__device__ __forceinline__ Raw<P64> p_next(const Raw<P64> &r, const Raw<P64> &p, double b) {
+  Raw<P64> o;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.c[k] = make_double2(__fma_rn(b, p.c[k].x, r.c[k].x), __fma_rn(b, p.c[k].y, r.c[k].y));
+  return o;
+}
+
+template <int NT, bool DAG, int MODE, bool PUPD>
 __device__ __forceinline__ void pcg8_hop(const DslashArgs &A, const PcgArgs &P, double2 *gsh, double *nrm,
-                                         const int *skip, const double *alpha) {
+                                         const int *skip, const double *alpha, const double *beta) {
   const Geom &g = A.g;
   constexpr double sdag = DAG ? -1.0 : 1.0;
   const int d = threadIdx.x & 7;
@@ -207,13 +218,24 @@ __device__ __forceinline__ void pcg8_hop(const DslashArgs &A, const PcgArgs &P, 
         }
         const int xn = cbindex(g, c.x, c.y, c.z, c.t);
         const unsigned ni = rb + (k ? (unsigned)g.kb1 : 0u) + (unsigned)xn * (unsigned)C + (unsigned)sp;
-        const Raw<P64> nr = load_raw64_l2(A.in, ni);
+        Raw<P64> nr = load_raw64_l2(A.in, ni);
+        if (PUPD && MODE == 0) nr = p_next(load_raw64_l2(P.r, ni), nr, beta[q]);
         if (A.hop5 && d < 2) {
           const int sn = d == 0 ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
           const int chunk0 = (d == 0) != DAG ? 0 : 6;
-          const double2 *b = entry_ptr<12, const double2>(A.in.data, rb + site_entry(g, sn, x));
+          const unsigned i5 = rb + site_entry(g, sn, x);
+          const double2 *b = entry_ptr<12, const double2>(A.in.data, i5);
+          if (PUPD && MODE == 0) {
+            const double2 *br = entry_ptr<12, const double2>(P.r.data, i5);
 #pragma unroll
-          for (int qq = 0; qq < 6; qq++) v5[qq] = __ldcg(b + 8 * (chunk0 + qq));
+            for (int qq = 0; qq < 6; qq++) {
+              const double2 pv = __ldcg(b + 8 * (chunk0 + qq)), rv = __ldcg(br + 8 * (chunk0 + qq));
+              v5[qq] = make_double2(__fma_rn(beta[q], pv.x, rv.x), __fma_rn(beta[q], pv.y, rv.y));
+            }
+          } else {
+#pragma unroll
+            for (int qq = 0; qq < 6; qq++) v5[qq] = __ldcg(b + 8 * (chunk0 + qq));
+          }
           f5m = s == 0 ? A.hop5_wall : A.hop5_fact;
           f5p = s == g.ls - 1 ? A.hop5_wall : A.hop5_fact;
         }
@@ -268,7 +290,14 @@ __device__ __forceinline__ void pcg8_hop(const DslashArgs &A, const PcgArgs &P, 
         continue;
       }
       const double a = A.a;
-      const Spinor<double> xv = unpack64(load_raw64_l2(A.x, i));
+      Spinor<double> xv;
+      if (PUPD && MODE == 1) {
+        // the new direction p = r + beta p at this entry: stored, and the xpay input
+        xv = unpack64(p_next(load_raw64_l2(P.r, i), load_raw64_l2(A.x, i), beta[q]));
+        store_spinor<P64>(A.x, i, xv);
+      } else {
+        xv = unpack64(load_raw64_l2(A.x, i));
+      }
 #pragma unroll
       for (int s2 = 0; s2 < 4; s2++)
 #pragma unroll
@@ -321,7 +350,7 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
   extern __shared__ __align__(16) unsigned char dsh[];
   __shared__ CgState S;
   __shared__ double red[NT / 32];
-  __shared__ double sums[MAX_RHS], alpha[MAX_RHS];
+  __shared__ double sums[MAX_RHS], alpha[MAX_RHS], beta[MAX_RHS];
   __shared__ int skip[MAX_RHS];
   const Geom &g = P.ph[0].g;
   const int nrhs = g.nrhs;
@@ -337,20 +366,25 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
     bool all = true;
     for (int q = 0; q < nrhs; q++) all = all && S.halt_done[q];
     if (all) break;
-    if (threadIdx.x < nrhs) skip[threadIdx.x] = S.halt[threadIdx.x];
+    if (threadIdx.x < nrhs) {
+      skip[threadIdx.x] = S.halt[threadIdx.x];
+      // DP: the direction update of the previous iteration rides on this one's
+      // first two hops (p = r on entry: beta 0 in the first iteration)
+      beta[threadIdx.x] = guard == 0 ? 0.0 : S.beta[threadIdx.x];
+    }
     __syncthreads();
     // t1 = D p
-    if constexpr (DP) pcg8_hop<NT, false, 0>(P.ph[0], P, gsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, false, 0, true>(P.ph[0], P, gsh, nrm, skip, alpha, beta);
     else pcg_hop<NT, LC, false, 0>(P.ph[0], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // t2 = MatPc p, d = |t2|^2
-    if constexpr (DP) pcg8_hop<NT, false, 1>(P.ph[1], P, gsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, false, 1, true>(P.ph[1], P, gsh, nrm, skip, alpha, beta);
     else pcg_hop<NT, LC, false, 1>(P.ph[1], P, dsh, nrm, skip, alpha);
     if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x < nrhs && !skip[threadIdx.x]) S.d[threadIdx.x] = sums[threadIdx.x];
     __syncthreads();
     // t1 = D^dag t2
-    if constexpr (DP) pcg8_hop<NT, true, 0>(P.ph[2], P, gsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, true, 0, false>(P.ph[2], P, gsh, nrm, skip, alpha, beta);
     else pcg_hop<NT, LC, true, 0>(P.ph[2], P, dsh, nrm, skip, alpha);
     if (!pcg_sync(P)) break;
     // A p = MatPcDag t2: r -= alpha A p, x += alpha p, |r|^2
@@ -359,13 +393,21 @@ __global__ void __launch_bounds__(NT, 1) pcg_kernel(PcgArgs P) {
       alpha[q] = S.rr[q] / (S.d[q] + S.shift * S.pp[q]);
     }
     __syncthreads();
-    if constexpr (DP) pcg8_hop<NT, true, 2>(P.ph[3], P, gsh, nrm, skip, alpha);
+    if constexpr (DP) pcg8_hop<NT, true, 2, false>(P.ph[3], P, gsh, nrm, skip, alpha, beta);
     else pcg_hop<NT, LC, true, 2>(P.ph[3], P, dsh, nrm, skip, alpha);
     if (!pcg_reduce<NT>(P, nrhs, nrm, red, sums)) break;
     if (threadIdx.x == 0)
       for (int q = 0; q < nrhs; q++)
         if (!skip[q]) cg_advance(&S, q, sums[q]);
     __syncthreads();
+    if constexpr (DP) {
+      // p is updated by the next iteration's first two hops; a right-hand side
+      // that halted here is skipped from then on
+      if (threadIdx.x == 0)
+        for (int q = 0; q < nrhs; q++) S.halt_done[q] = S.halt[q];
+      __syncthreads();
+      continue;
+    }
     // p = r + beta p for the right-hand sides still iterating (cg_xp_update, blas.cu)
     for (int q = 0; q < nrhs; q++) {
       if (S.halt_done[q] || S.halt[q]) continue;
