@@ -15,10 +15,14 @@
 // writes the state back when the loop ends.  Fields written inside the launch
 // are read through L2 (ld.global.cg), never through the read-only cache.
 //
-// Measured on B200 it is slower than the device-side graph loop of solver.cu
-// (Wilson 8^4 FP64: 345 against 408 solves/s; DWF 8^4 x Ls 16: 11.3 against
-// 10.5 ms per solve): the five grid barriers of an iteration cost more than
-// the kernel boundaries of a graph, so it runs only when asked for.
+// Two forms.  On fields of at most PCG_DP_SITES entries (all right-hand sides)
+// the hops run with eight lanes per entry and the direction update rides on the
+// next iteration's first two hops, so an iteration is four hops and four grid
+// barriers; measured on B200 this beats the device-side graph loop of
+// solver.cu (Wilson 8^4 FP64: 506 against 482 solves/s) and is the default
+// there.  Larger fields run the column hop of hop_kernel plus a p-update phase
+// (five barriers), which is slower than the graph loop (DWF 8^4 x Ls 16: 11.3
+// against 10.3 ms per solve) and runs only when asked for.
 //
 // Grid barriers spin on a generation counter with a time limit: a wait that
 // runs out sets the error flag, every other block leaves at its next wait, and
@@ -36,8 +40,8 @@ namespace cpsb {
 // still spreads over many SMs.
 constexpr int PCG_NT_MAX = 128;
 // Fields (all right-hand sides) of at most this many entries use the
-// direction-parallel hop phases.
-constexpr long PCG_DP_SITES = 1L << 14;
+// direction-parallel hop phases (the same bound as the automatic mode).
+constexpr long PCG_DP_SITES = PCG_AUTO_SITES;
 // Longest barrier wait before it gives up (ns of the global timer): far above a
 // phase of any lattice the loop takes, and above kernels of other streams that
 // may hold SMs while the launch's blocks become resident.
@@ -446,7 +450,7 @@ static int pcg_max_blocks(const void *fn, int nt, size_t shm) {
 
 int persistent_cg_mode() {
   const char *e = getenv("CPSB_PERSISTENT_CG");
-  return e ? atoi(e) : 0;
+  return e ? atoi(e) : 1;
 }
 
 // Runs the iterations of an FP64 CG solve whose state (r, p, x, CgState) the

@@ -5,8 +5,10 @@ Both run DiracOp::InvCg's recurrence (inv_cg.C:293-364); they differ only in
 the number of blocks whose partial sums make up each dot product, so their
 iteration counts agree within one and their solutions within 1e-9 relative
 (the bound the FP64 solver keeps against CPS itself).  CPSB_PERSISTENT_CG
-selects the loop: 0 (default) launch-per-step, 1 persistent for fields of at
-most 2^17 entries, 2 persistent at any size.
+selects the loop: 0 launch-per-step, 1 (default) persistent for fields of at
+most 2^14 entries (eight lanes per entry, the direction update folded into the
+next iteration's hops), 2 persistent at any size (larger fields: one thread per
+entry and a separate direction-update phase).
 """
 import ctypes as C
 import os
@@ -92,7 +94,8 @@ def test_persistent_dwf_multi_rhs_with_zero_source():
 
 def test_persistent_forced_at_larger_size():
     """Mode 2 on DWF 8^4 x Ls 16 with 8 right-hand sides (262144 entries, above
-    the automatic limit): blocks stride over several work units per phase."""
+    the automatic limit): the one-thread-per-entry form, blocks striding over
+    several work units per phase."""
     import cps_public_b200 as cb
     from cps_public_b200 import fields
     cb.init(0)
