@@ -19,10 +19,12 @@
 // the hops run with eight lanes per entry and the direction update rides on the
 // next iteration's first two hops, so an iteration is four hops and four grid
 // barriers; measured on B200 this beats the device-side graph loop of
-// solver.cu (Wilson 8^4 FP64: 506 against 482 solves/s) and is the default
-// there.  Larger fields run the column hop of hop_kernel plus a p-update phase
-// (five barriers), which is slower than the graph loop (DWF 8^4 x Ls 16: 11.3
-// against 10.3 ms per solve) and runs only when asked for.
+// solver.cu for Wilson (8^4 FP64: 506 against 482 solves/s) and is the default
+// there.  It does not suit DWF, whose columns of slices share each link (DWF
+// 8^4 x Ls 16 with this form: 39 against 10.4 ms per solve).  Larger fields run
+// the column hop of hop_kernel plus a p-update phase (five barriers), which is
+// slower than the graph loop (DWF 8^4 x Ls 16: 11.3 against 10.3 ms per solve);
+// both run for DWF and for larger fields only when asked for.
 //
 // Grid barriers spin on a generation counter with a time limit: a wait that
 // runs out sets the error flag, every other block leaves at its next wait, and

@@ -231,9 +231,9 @@ cudaError_t launch_ms_loop_cond(cudaGraphConditionalHandle h, const MsBatch *B, 
 CgSolver *get_solver(Gauge *G, const cpsb_dirac_params &p, int sloppy, int nrhs);
 
 // The persistent FP64 CG loop (cg_persistent.cu).  CPSB_PERSISTENT_CG in the
-// environment: 0 off, 1 (default) for fields of at most PCG_AUTO_SITES entries
-// (its direction-parallel form, faster than the graph loop there), 2 for any
-// size that fits one cooperative launch.
+// environment: 0 off, 1 (default) for Wilson fields of at most PCG_AUTO_SITES
+// entries (its direction-parallel form, faster than the graph loop there), 2
+// for any action and any size that fits one cooperative launch.
 constexpr long PCG_AUTO_SITES = 1L << 14;
 constexpr size_t PCG_PARTIAL_SLOTS = (size_t)MAX_RHS * 148 * 16;
 int persistent_cg_mode();

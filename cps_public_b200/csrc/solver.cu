@@ -175,7 +175,9 @@ void CgSolver::run_batches(int batch, cudaStream_t st, const bool *done, bool an
 bool CgSolver::run_persistent(cudaStream_t st) {
   const int mode = persistent_cg_mode();
   if (opS || shift != 0.0 || mode == 0 || !op64->can_fuse_cg_r()) return false;
-  if (mode == 1 && geom.nsites > PCG_AUTO_SITES) return false;
+  // automatic: Wilson fields small enough for the direction-parallel form (for
+  // DWF, whose columns of slices share each link, the graph loop is faster)
+  if (mode == 1 && (geom.nsites > PCG_AUTO_SITES || p.action != CPSB_WILSON)) return false;
   Operator &op = *op64;
   DslashArgs A;
   memset(&A, 0, sizeof(A));

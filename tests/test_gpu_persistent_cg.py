@@ -5,10 +5,11 @@ Both run DiracOp::InvCg's recurrence (inv_cg.C:293-364); they differ only in
 the number of blocks whose partial sums make up each dot product, so their
 iteration counts agree within one and their solutions within 1e-9 relative
 (the bound the FP64 solver keeps against CPS itself).  CPSB_PERSISTENT_CG
-selects the loop: 0 launch-per-step, 1 (default) persistent for fields of at
-most 2^14 entries (eight lanes per entry, the direction update folded into the
-next iteration's hops), 2 persistent at any size (larger fields: one thread per
-entry and a separate direction-update phase).
+selects the loop: 0 launch-per-step, 1 (default) persistent for Wilson fields
+of at most 2^14 entries, 2 persistent for any action and size.  Fields of at
+most 2^14 entries run eight lanes per entry with the direction update folded
+into the next iteration's hops; larger ones one thread per entry with a
+separate direction-update phase.
 """
 import ctypes as C
 import os
@@ -88,7 +89,7 @@ def test_persistent_dwf_multi_rhs_with_zero_source():
             fields.random_source(n, 74)]
     for mass in (0.05, 0.3):
         op = cb.DiracOp(g, "dwf", mass=mass, ls=ls)
-        ra, rb = _compare(op, srcs)
+        ra, rb = _compare(op, srcs, mode=2)  # the direction-parallel form with the 5th-direction hop
         assert rb[1].iters == ra[1].iters
 
 
